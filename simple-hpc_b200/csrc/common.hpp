@@ -1,0 +1,89 @@
+// common.hpp — shared host/device definitions of the B200 SIMPLE solver.
+#pragma once
+
+#include "../../include/sgpu.h"
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#define SGPU_HD __host__ __device__
+#else
+#define SGPU_HD
+#endif
+
+namespace sgpu {
+
+// ---- errors ----
+
+// Exception carrying an sgpu status code; converted to a return value at the C ABI.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void set_last_error(const std::string& msg);
+int fail(int code, const std::string& msg); // sets the message, returns code
+
+void params_defaults(sgpu_params_t& p);
+void params_finalize(sgpu_params_t& p);
+void params_from_config(const std::string& text, sgpu_params_t& p);
+
+#ifdef __CUDACC__
+#define SGPU_CUDA(x)                                                                          \
+    do {                                                                                      \
+        cudaError_t e_ = (x);                                                                 \
+        if (e_ != cudaSuccess)                                                                \
+            throw ::sgpu::Error(e_ == cudaErrorMemoryAllocation ? SGPU_E_NOMEM : SGPU_E_CUDA, \
+                                std::string("GPU error: ") + cudaGetErrorString(e_) +         \
+                                    " in " #x);                                               \
+    } while (0)
+#define SGPU_LAUNCH() SGPU_CUDA(cudaGetLastError())
+#endif
+
+// ---- device layout ----
+//
+// Every full-grid field is stored row-major with a padded row pitch: element (i, j) of the
+// reference's nrows x ncols Field2D is at [i * pitch + j]. The pitch is a multiple of 32 doubles, so
+// each row starts on a 256-byte boundary; the padding columns are never read as cells.
+struct Grid {
+    int nrows = 0, ncols = 0, pitch = 0;
+    std::size_t elems() const { return static_cast<std::size_t>(nrows) * pitch; }
+    std::size_t bytes() const { return elems() * sizeof(double); }
+};
+
+inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+// Inclusive cell range [i0, i1] x [j0, j1] of a kernel, in global (i, j) indices.
+struct Range {
+    int i0, i1, j0, j1;
+    SGPU_HD int rows() const { return i1 >= i0 ? i1 - i0 + 1 : 0; }
+    SGPU_HD int cols() const { return j1 >= j0 ? j1 - j0 + 1 : 0; }
+};
+
+// What the kernels read from the parameters. The diffusive coefficients depend only on whether a
+// cell is in the boundary band, so the host evaluates both variants once (with the expressions of
+// diffusive_coefficients, src/coefficients.cpp:41-63; IEEE-exact, no contraction) and the kernels
+// add them to the per-cell convective part.
+struct DevParams {
+    int NX, NY, H, Hx, Hy, nrows, ncols, pitch;
+    int ncol;  // momentum colours: 5, or 2 for UDS + order 2 (momentum_u.cpp:70-72)
+    int uds;   // convection_scheme == UDS
+    int order; // diffusion_order
+    double dx, dy, nu, au, av, ap;
+    double dband[9]; // diffusive coefficients in the boundary band (and for order 2)
+    double dint[9];  // diffusive coefficients elsewhere (order 4)
+};
+
+// Multigrid level view (the reference's MGView, include/simple/multigrid.hpp:59-66): element
+// (I, J), 0 <= I < nx, 0 <= J < ny, of each array is ptr[I * stride + J]; the pointers address
+// interior cell (0, 0) and every neighbour of an interior cell lies inside the allocation.
+struct LevelView {
+    int nx, ny, stride;
+    double *AE, *AW, *AN, *AS, *AP, *b, *x, *r;
+};
+
+} // namespace sgpu

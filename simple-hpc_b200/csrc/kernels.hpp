@@ -1,0 +1,97 @@
+// kernels.hpp — host-side launchers of the FP64 kernels (one translation unit per family).
+#pragma once
+
+#include "common.hpp"
+
+#include <cuda_runtime.h>
+
+namespace sgpu {
+
+// ---- ordered sums (reduce.cu) ----
+//
+// K planes of nr x nc values (plane m at vals + m * plane_stride, row r at + r * ld) are summed in
+// the reference's fixed order: each row left to right from 0.0, then the rows top to bottom from
+// 0.0 (CellSums, src/decomp.cpp:176-205; det_sum, src/multigrid.cpp:18-34). out[m] receives plane
+// m's sum. rows (K * nr doubles) and counter (one unsigned int, zero between calls) are scratch. If
+// skip is non-null and *skip != 0 the launch does nothing (a finished iterative solve).
+struct SumScratch {
+    double* rows = nullptr;
+    unsigned int* counter = nullptr;
+    int max_rows = 0, max_k = 0;
+};
+void launch_ordered_sum(const double* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
+                        double* out, const SumScratch& s, const int* skip, cudaStream_t st);
+
+// ---- momentum and pressure phases, reference-shaped (phases.cu) ----
+struct Coef9Ptr {
+    double* a[9]; // AE AW AN AS AEE AWW ANN ASS AP
+};
+struct PressurePtr {
+    double *AEP, *AWP, *ANP, *ASP, *APP, *b, *pc;
+};
+
+void launch_assemble_u(const DevParams& p, const double* u, const double* v, Coef9Ptr cu,
+                       cudaStream_t st);
+void launch_assemble_v(const DevParams& p, const double* u, const double* v, Coef9Ptr cv,
+                       cudaStream_t st);
+void launch_bc_u(const DevParams& p, double* u, cudaStream_t st);
+void launch_bc_v(const DevParams& p, double* v, cudaStream_t st);
+// |R| of every residual cell into cells (compact rows of the residual range).
+void launch_residual_u_cells(const DevParams& p, Coef9Ptr cu, const double* u, const double* pf,
+                             double* cells, cudaStream_t st);
+void launch_residual_v_cells(const DevParams& p, Coef9Ptr cv, const double* v, const double* pf,
+                             double* cells, cudaStream_t st);
+// One colour pass of the multicolour sweep (in place).
+void launch_sweep_u_colour(const DevParams& p, Coef9Ptr cu, double* u, const double* pf, int colour,
+                           cudaStream_t st);
+void launch_sweep_v_colour(const DevParams& p, Coef9Ptr cv, double* v, const double* pf, int colour,
+                           cudaStream_t st);
+// One Jacobi pass src -> dst.
+void launch_sweep_u_jacobi(const DevParams& p, Coef9Ptr cu, const double* src, double* dst,
+                           const double* pf, cudaStream_t st);
+void launch_sweep_v_jacobi(const DevParams& p, Coef9Ptr cv, const double* src, double* dst,
+                           const double* pf, cudaStream_t st);
+// assemble_p: links, wall zeros, APP, b and |b| into cells[0..), b into cells + plane (if two).
+void launch_assemble_p(const DevParams& p, const double* APU, const double* APV, const double* u,
+                       const double* v, PressurePtr w, double* cells_absb, double* cells_b,
+                       cudaStream_t st);
+void launch_pc_redblack(const DevParams& p, PressurePtr w, int colour, cudaStream_t st);
+void launch_pc_jacobi(const DevParams& p, PressurePtr w, const double* src, double* dst,
+                      cudaStream_t st);
+void launch_correct(const DevParams& p, PressurePtr w, const double* APU, const double* APV,
+                    double* u, double* v, double* pf, cudaStream_t st);
+// dst[i] = src[i] over n doubles.
+void launch_copy(const double* src, double* dst, std::size_t n, cudaStream_t st);
+
+// ---- multigrid (mg.cu) ----
+void launch_mg_build(const LevelView& F, const LevelView& C, cudaStream_t st);
+void launch_mg_smooth_colour(const LevelView& L, int colour, cudaStream_t st);
+void launch_mg_residual(const LevelView& L, cudaStream_t st);
+void launch_mg_restrict(const LevelView& F, const LevelView& C, cudaStream_t st);
+void launch_mg_prolong(const LevelView& C, const LevelView& F, double omega, cudaStream_t st);
+// x[I, J] -= *sum / (nx * ny) over the level interior (the mean removal after an ordered sum).
+void launch_mg_sub_mean(const LevelView& L, double* x, const double* sum, cudaStream_t st);
+// Coarsest-level solve in one CTA (coarse_solve, multigrid.cpp:120-140); *sweeps_out gets the count.
+void launch_mg_coarse(const LevelView& L, double* rowbuf, int* sweeps_out, cudaStream_t st);
+
+// ---- conjugate gradient (cg.cu) ----
+struct CgScalars {
+    double rz, nb, mz, alpha, beta, rel, mb;
+    int k, done, maxit;
+    double tol, n;
+};
+struct CgPtr {
+    double *r, *z, *d, *q;
+};
+void launch_cg_init(const DevParams& p, PressurePtr w, CgPtr cg, CgScalars* sc, double* cells,
+                    std::size_t plane, cudaStream_t st);
+void launch_cg_scalars(int stage, CgScalars* sc, const double* sums, cudaStream_t st);
+void launch_cg_dinit(const DevParams& p, CgPtr cg, const CgScalars* sc, cudaStream_t st);
+void launch_cg_dq(const DevParams& p, PressurePtr w, CgPtr cg, const CgScalars* sc, double* cells,
+                  cudaStream_t st);
+void launch_cg_update(const DevParams& p, PressurePtr w, CgPtr cg, const CgScalars* sc,
+                      double* cells, std::size_t plane, cudaStream_t st);
+void launch_cg_dir(const DevParams& p, CgPtr cg, const CgScalars* sc, cudaStream_t st);
+void launch_cg_copy_x(const DevParams& p, const double* x, double* cells, cudaStream_t st);
+
+} // namespace sgpu

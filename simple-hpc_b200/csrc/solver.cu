@@ -1,0 +1,746 @@
+// solver.cu — device state, phase orchestration and the C ABI (include/sgpu.h).
+//
+// Replaces the reference's HipSolver (src/hip/solver_hip.hip:326-550). Differences by design:
+//  - every State array lives on the device for the whole run (as in the reference), with a padded
+//    row pitch (Grid) instead of the host's packed rows;
+//  - residual sums use the reference CPU's fixed order (reduce.cu), so res_u, res_v, res_p and the
+//    stopping iteration are bit-identical to the serial code, not just close;
+//  - momentum_solver jacobi and pressure_solver jacobi, cg and mg run on the GPU too (the reference
+//    GPU backend accepts gs_multicolour + gs_redblack only, solver_hip.hip:373-377);
+//  - one CUDA stream per handle; an outer iteration ends with one device->host copy of the three
+//    residuals instead of a device synchronisation per phase.
+#include "kernels.hpp"
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace sgpu {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+// Host evaluation of diffusive_coefficients (src/coefficients.cpp:41-63) for the two cell kinds.
+static void diffusive_host(const sgpu_params_t& p, bool band_or_order2, double out[9]) {
+    const double dx = p.dx, dy = p.dy, nu = p.nu;
+    if (band_or_order2) {
+        out[0] = dy * nu / dx;
+        out[1] = dy * nu / dx;
+        out[2] = dx * nu / dy;
+        out[3] = dx * nu / dy;
+        out[4] = out[5] = out[6] = out[7] = 0.0;
+        out[8] = -nu * (-2 * dx / dy - 2 * dy / dx);
+    } else {
+        out[0] = 4.0 / 3 * dy * nu / dx;
+        out[1] = 4.0 / 3 * dy * nu / dx;
+        out[2] = 4.0 / 3 * dx * nu / dy;
+        out[3] = 4.0 / 3 * dx * nu / dy;
+        out[4] = -1.0 / 12 * dy * nu / dx;
+        out[5] = -1.0 / 12 * dy * nu / dx;
+        out[6] = -1.0 / 12 * dx * nu / dy;
+        out[7] = -1.0 / 12 * dx * nu / dy;
+        out[8] = -nu * (-2.5 * dx / dy - 2.5 * dy / dx);
+    }
+}
+
+struct Solver {
+    sgpu_params_t prm{};
+    DevParams dp{};
+    Grid g;
+    cudaStream_t st = nullptr;
+    std::vector<void*> allocs;
+    std::size_t bytes = 0;
+
+    double *u = nullptr, *v = nullptr, *pf = nullptr;
+    Coef9Ptr cu{}, cv{};
+    PressurePtr w{};
+    double* scratch = nullptr; // Jacobi previous iterate (u, v and p')
+    CgPtr cg{};
+    CgScalars* cgs = nullptr;
+    double* cells = nullptr; // 4 planes of NX x NY per-cell values for the ordered sums
+    std::size_t plane = 0;
+    double* sums = nullptr;  // 32 device doubles: results of ordered sums
+    double* res_dev = nullptr; // res_u, res_v, res_p of the current iteration
+    SumScratch ss;
+    int* stats = nullptr;      // device ints: [0] coarse sweeps
+    double* host_res = nullptr; // pinned: 3 residuals
+
+    // multigrid
+    std::vector<LevelView> lv;
+    double* mg_r0 = nullptr;
+    double* coarse_rowbuf = nullptr;
+
+    int ncol = 5;
+    int last_cg_iterations = 0, last_vcycles = 0, last_coarse_sweeps = 0;
+    double last_rel = 0.0;
+    bool cg_stats_pending = false;
+
+    template <class T> T* dalloc(std::size_t count) {
+        void* p = nullptr;
+        const std::size_t nb = count * sizeof(T);
+        SGPU_CUDA(cudaMalloc(&p, nb > 0 ? nb : 1));
+        allocs.push_back(p);
+        bytes += nb;
+        SGPU_CUDA(cudaMemsetAsync(p, 0, nb > 0 ? nb : 1, st));
+        return static_cast<T*>(p);
+    }
+    double* field() { return dalloc<double>(g.elems()); }
+
+    Solver(const sgpu_params_t& p, const double* hu, const double* hv, const double* hp);
+    ~Solver();
+
+    void upload(double* dst, const double* host) {
+        SGPU_CUDA(cudaMemcpy2DAsync(dst, sizeof(double) * g.pitch, host, sizeof(double) * g.ncols,
+                                    sizeof(double) * g.ncols, g.nrows, cudaMemcpyHostToDevice, st));
+    }
+    void download(const double* src, double* host) {
+        SGPU_CUDA(cudaMemcpy2DAsync(host, sizeof(double) * g.ncols, src, sizeof(double) * g.pitch,
+                                    sizeof(double) * g.ncols, g.nrows, cudaMemcpyDeviceToHost, st));
+        SGPU_CUDA(cudaStreamSynchronize(st));
+    }
+    double* field_ptr(int id) {
+        if (id == SGPU_F_U) return u;
+        if (id == SGPU_F_V) return v;
+        if (id == SGPU_F_P) return pf;
+        if (id >= SGPU_F_CU_AE && id <= SGPU_F_CU_AP) return cu.a[id - SGPU_F_CU_AE];
+        if (id >= SGPU_F_CV_AE && id <= SGPU_F_CV_AP) return cv.a[id - SGPU_F_CV_AE];
+        switch (id) {
+        case SGPU_F_AEP: return w.AEP;
+        case SGPU_F_AWP: return w.AWP;
+        case SGPU_F_ANP: return w.ANP;
+        case SGPU_F_ASP: return w.ASP;
+        case SGPU_F_APP: return w.APP;
+        case SGPU_F_B: return w.b;
+        case SGPU_F_PC: return w.pc;
+        default: return nullptr;
+        }
+    }
+    double* at(double* f, int i, int j) const {
+        return f + static_cast<std::size_t>(i) * g.pitch + j;
+    }
+
+    // ---- phases (enqueue only) ----
+    void assemble_u() { launch_assemble_u(dp, u, v, cu, st); }
+    void bc_u() { launch_bc_u(dp, u, st); }
+    void residual_u(double* out) {
+        launch_residual_u_cells(dp, cu, u, pf, cells, st);
+        launch_ordered_sum(cells, 0, prm.NY - 1, prm.NX, prm.NY - 1, 1, out, ss, nullptr, st);
+    }
+    void sweep_u(int n);
+    void assemble_v() { launch_assemble_v(dp, u, v, cv, st); }
+    void bc_v() { launch_bc_v(dp, v, st); }
+    void residual_v(double* out) {
+        launch_residual_v_cells(dp, cv, v, pf, cells, st);
+        launch_ordered_sum(cells, 0, prm.NY, prm.NX - 1, prm.NY, 1, out, ss, nullptr, st);
+    }
+    void sweep_v(int n);
+    void assemble_p(double* out) {
+        launch_assemble_p(dp, cu.a[8], cv.a[8], u, v, w, cells, nullptr, st);
+        launch_ordered_sum(cells, 0, prm.NY, prm.NX, prm.NY, 1, out, ss, nullptr, st);
+    }
+    void solve_p();
+    void correct() { launch_correct(dp, w, cu.a[8], cv.a[8], u, v, pf, st); }
+
+    void solve_redblack();
+    void solve_jacobi();
+    void solve_cg();
+    void solve_mg();
+    void mg_vcycle();
+    void remove_mean0(double* f);
+
+    void outer_iteration_enqueue(double* res3) {
+        assemble_u();
+        bc_u();
+        residual_u(res3 + 0);
+        sweep_u(prm.maxit_inner_u);
+        assemble_v();
+        bc_v();
+        residual_v(res3 + 1);
+        sweep_v(prm.maxit_inner_v);
+        assemble_p(res3 + 2);
+        solve_p();
+        correct();
+    }
+    void sync() { SGPU_CUDA(cudaStreamSynchronize(st)); }
+    double fetch(const double* dev) {
+        SGPU_CUDA(cudaMemcpyAsync(host_res, dev, sizeof(double), cudaMemcpyDeviceToHost, st));
+        sync();
+        return host_res[0];
+    }
+    void finish_stats() {
+        if (prm.pressure_solver == SGPU_P_MG) {
+            int h = 0;
+            SGPU_CUDA(cudaMemcpyAsync(&h, stats, sizeof(int), cudaMemcpyDeviceToHost, st));
+            sync();
+            last_coarse_sweeps = h;
+        }
+    }
+};
+
+Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const double* hp)
+    : prm(p) {
+    // Solver check of the reference GPU backend (solver_hip.hip:373-377), widened to every solver
+    // this backend implements.
+    if (p.momentum_solver == SGPU_MOM_GS_LEX || p.pressure_solver == SGPU_P_GS_LEX)
+        throw Error(SGPU_E_INVALID,
+                    "backend = gpu supports momentum_solver = gs_multicolour or jacobi with "
+                    "pressure_solver = gs_redblack, jacobi, cg or mg (gs_lex is sequential)");
+    if (p.nrows != p.NX + 2 * p.H + 1 || p.ncols != p.NY + 2 * p.H + 1 || p.NX < 1 || p.NY < 1 ||
+        p.H < 2)
+        throw Error(SGPU_E_INVALID, "sgpu_create: parameters are not finalised (call sgpu_params_finalize)");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        (void)cudaGetLastError();
+        throw Error(SGPU_E_NODEVICE, "GPU error: no CUDA device is visible");
+    }
+    SGPU_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    g.nrows = p.nrows;
+    g.ncols = p.ncols;
+    g.pitch = round_up(p.ncols, 32);
+    ncol = (p.convection_scheme == SGPU_UDS && p.diffusion_order == 2) ? 2 : 5;
+
+    dp.NX = p.NX;
+    dp.NY = p.NY;
+    dp.H = p.H;
+    dp.Hx = p.N_halo_x;
+    dp.Hy = p.N_halo_y;
+    dp.nrows = p.nrows;
+    dp.ncols = p.ncols;
+    dp.pitch = g.pitch;
+    dp.ncol = ncol;
+    dp.uds = p.convection_scheme == SGPU_UDS ? 1 : 0;
+    dp.order = p.diffusion_order;
+    dp.dx = p.dx;
+    dp.dy = p.dy;
+    dp.nu = p.nu;
+    dp.au = p.relaxation_factor_u;
+    dp.av = p.relaxation_factor_v;
+    dp.ap = p.relaxation_factor_p;
+    diffusive_host(p, true, dp.dband);
+    diffusive_host(p, false, dp.dint);
+
+    u = field();
+    v = field();
+    pf = field();
+    for (int k = 0; k < 9; ++k) cu.a[k] = field();
+    for (int k = 0; k < 9; ++k) cv.a[k] = field();
+    w.AEP = field();
+    w.AWP = field();
+    w.ANP = field();
+    w.ASP = field();
+    w.APP = field();
+    w.b = field();
+    w.pc = field();
+    if (p.momentum_solver == SGPU_MOM_JACOBI || p.pressure_solver == SGPU_P_JACOBI)
+        scratch = field();
+    plane = static_cast<std::size_t>(p.NX) * p.NY;
+    const int kplanes = p.pressure_solver == SGPU_P_CG ? 4 : 2;
+    cells = dalloc<double>(plane * kplanes);
+    if (p.pressure_solver == SGPU_P_CG) {
+        cg.r = field();
+        cg.z = field();
+        cg.d = field();
+        cg.q = field();
+        cgs = dalloc<CgScalars>(1);
+        CgScalars init{};
+        init.n = static_cast<double>(p.NX) * p.NY;
+        init.tol = p.pressure_tolerance;
+        init.maxit = p.pressure_maxit;
+        SGPU_CUDA(cudaMemcpyAsync(cgs, &init, sizeof init, cudaMemcpyHostToDevice, st));
+    }
+    sums = dalloc<double>(32);
+    res_dev = dalloc<double>(4);
+    stats = dalloc<int>(8);
+    ss.max_rows = p.nrows;
+    ss.max_k = 4;
+    ss.rows = dalloc<double>(static_cast<std::size_t>(ss.max_rows) * ss.max_k);
+    ss.counter = dalloc<unsigned int>(1);
+    SGPU_CUDA(cudaMallocHost(&host_res, sizeof(double) * 8));
+
+    if (p.pressure_solver == SGPU_P_MG) {
+        int dims[128];
+        int nl = 0;
+        sgpu_mg_levels(p.NX, p.NY, &nl, dims);
+        mg_r0 = field();
+        lv.resize(nl);
+        int maxnx = 1;
+        for (int l = 0; l < nl; ++l) {
+            LevelView& L = lv[l];
+            L.nx = dims[2 * l];
+            L.ny = dims[2 * l + 1];
+            if (L.nx > maxnx) maxnx = L.nx;
+            if (l == 0) {
+                // Level 0 aliases the PressureWork arrays (mg_view, multigrid.cpp:193-206).
+                const std::size_t base = static_cast<std::size_t>(p.H) * g.pitch + p.H + 1;
+                L.stride = g.pitch;
+                L.AE = w.AEP + base;
+                L.AW = w.AWP + base;
+                L.AN = w.ANP + base;
+                L.AS = w.ASP + base;
+                L.AP = w.APP + base;
+                L.b = w.b + base;
+                L.x = w.pc + base;
+                L.r = mg_r0 + base;
+            } else {
+                // Coarse levels: (nx + 2) x (ny + 2) with a zero halo (MGWork, multigrid.cpp:176-184).
+                L.stride = L.ny + 2;
+                const std::size_t n = static_cast<std::size_t>(L.nx + 2) * L.stride;
+                const std::size_t base = static_cast<std::size_t>(L.stride) + 1;
+                double* a[8];
+                for (int k = 0; k < 8; ++k) a[k] = dalloc<double>(n) + base;
+                L.AE = a[0];
+                L.AW = a[1];
+                L.AN = a[2];
+                L.AS = a[3];
+                L.AP = a[4];
+                L.b = a[5];
+                L.x = a[6];
+                L.r = a[7];
+            }
+        }
+        coarse_rowbuf = dalloc<double>(static_cast<std::size_t>(maxnx) + 1);
+    }
+
+    if (hu) upload(u, hu);
+    if (hv) upload(v, hv);
+    if (hp) upload(pf, hp);
+    sync();
+}
+
+Solver::~Solver() {
+    if (st) cudaStreamSynchronize(st);
+    for (void* q : allocs) cudaFree(q);
+    if (host_res) cudaFreeHost(host_res);
+    if (st) cudaStreamDestroy(st);
+}
+
+// sweep_u_batch (momentum_u.cpp:162-171).
+void Solver::sweep_u(int n) {
+    if (n <= 0) return;
+    if (prm.momentum_solver == SGPU_MOM_JACOBI) {
+        launch_copy(u, scratch, g.elems(), st);
+        for (int k = 0; k < n; ++k) {
+            const bool to_u = (n - k) % 2 == 1;
+            launch_sweep_u_jacobi(dp, cu, to_u ? scratch : u, to_u ? u : scratch, pf, st);
+        }
+        return;
+    }
+    for (int s = 0; s < n; ++s)
+        for (int c = 0; c < ncol; ++c) launch_sweep_u_colour(dp, cu, u, pf, c, st);
+}
+
+// sweep_v_batch (momentum_v.cpp:164-173).
+void Solver::sweep_v(int n) {
+    if (n <= 0) return;
+    if (prm.momentum_solver == SGPU_MOM_JACOBI) {
+        launch_copy(v, scratch, g.elems(), st);
+        for (int k = 0; k < n; ++k) {
+            const bool to_v = (n - k) % 2 == 1;
+            launch_sweep_v_jacobi(dp, cv, to_v ? scratch : v, to_v ? v : scratch, pf, st);
+        }
+        return;
+    }
+    for (int s = 0; s < n; ++s)
+        for (int c = 0; c < ncol; ++c) launch_sweep_v_colour(dp, cv, v, pf, c, st);
+}
+
+// solve_pc_redblack (pressure.cpp:114-134).
+void Solver::solve_redblack() {
+    SGPU_CUDA(cudaMemsetAsync(w.pc, 0, g.bytes(), st));
+    for (int k = 0; k < prm.maxit_inner_p; ++k)
+        for (int c = 0; c < 2; ++c) launch_pc_redblack(dp, w, c, st);
+}
+
+// solve_pc_jacobi (pressure.cpp:77-112).
+void Solver::solve_jacobi() {
+    SGPU_CUDA(cudaMemsetAsync(w.pc, 0, g.bytes(), st));
+    SGPU_CUDA(cudaMemsetAsync(scratch, 0, g.bytes(), st));
+    const int n = prm.maxit_inner_p;
+    for (int k = 0; k < n; ++k) {
+        const bool to_pc = (n - k) % 2 == 1;
+        launch_pc_jacobi(dp, w, to_pc ? scratch : w.pc, to_pc ? w.pc : scratch, st);
+    }
+}
+
+// solve_pc_cg (pressure.cpp:208-317) with device-resident scalars.
+void Solver::solve_cg() {
+    SGPU_CUDA(cudaMemsetAsync(w.pc, 0, g.bytes(), st));
+    const double* b0 = at(w.b, prm.H, prm.H + 1);
+    launch_ordered_sum(b0, 0, g.pitch, prm.NX, prm.NY, 1, sums, ss, nullptr, st);
+    launch_cg_scalars(0, cgs, sums, st);
+    launch_cg_init(dp, w, cg, cgs, cells, plane, st);
+    launch_ordered_sum(cells, plane, prm.NY, prm.NX, prm.NY, 4, sums, ss, nullptr, st);
+    launch_cg_scalars(1, cgs, sums, st);
+    launch_cg_dinit(dp, cg, cgs, st);
+    const int* done = &cgs->done;
+    // Iterations are enqueued in chunks; between chunks the host reads `done` once.
+    const int chunk = 16;
+    int enqueued = 0;
+    while (enqueued < prm.pressure_maxit) {
+        const int m = std::min(chunk, prm.pressure_maxit - enqueued);
+        for (int it = 0; it < m; ++it) {
+            launch_cg_dq(dp, w, cg, cgs, cells, st);
+            launch_ordered_sum(cells, plane, prm.NY, prm.NX, prm.NY, 1, sums, ss, done, st);
+            launch_cg_scalars(2, cgs, sums, st);
+            launch_cg_update(dp, w, cg, cgs, cells, plane, st);
+            launch_ordered_sum(cells, plane, prm.NY, prm.NX, prm.NY, 4, sums, ss, done, st);
+            launch_cg_scalars(3, cgs, sums, st);
+            launch_cg_dir(dp, cg, cgs, st);
+        }
+        enqueued += m;
+        int h = 0;
+        SGPU_CUDA(cudaMemcpyAsync(&h, done, sizeof(int), cudaMemcpyDeviceToHost, st));
+        sync();
+        if (h) break;
+    }
+    // Remove the mean of the solution (pressure.cpp:311-316).
+    const double* x0 = at(w.pc, prm.H, prm.H + 1);
+    launch_ordered_sum(x0, 0, g.pitch, prm.NX, prm.NY, 1, sums + 8, ss, nullptr, st);
+    LevelView L0{prm.NX, prm.NY, g.pitch, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                 nullptr, nullptr};
+    launch_mg_sub_mean(L0, at(w.pc, prm.H, prm.H + 1), sums + 8, st);
+    cg_stats_pending = true;
+}
+
+// remove_mean0 (multigrid.cpp:327-345) on the p' interior.
+void Solver::remove_mean0(double* f) {
+    double* f0 = at(f, prm.H, prm.H + 1);
+    launch_ordered_sum(f0, 0, g.pitch, prm.NX, prm.NY, 1, sums + 16, ss, nullptr, st);
+    LevelView L0{prm.NX, prm.NY, g.pitch, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                 nullptr, nullptr};
+    launch_mg_sub_mean(L0, f0, sums + 16, st);
+}
+
+// mg_vcycle (multigrid.cpp:299-323).
+void Solver::mg_vcycle() {
+    const int nl = static_cast<int>(lv.size());
+    for (int l = 0; l + 1 < nl; ++l) {
+        for (int s = 0; s < prm.mg_pre; ++s) {
+            launch_mg_smooth_colour(lv[l], 0, st);
+            launch_mg_smooth_colour(lv[l], 1, st);
+        }
+        launch_mg_residual(lv[l], st);
+        launch_mg_restrict(lv[l], lv[l + 1], st);
+    }
+    launch_mg_coarse(lv[nl - 1], coarse_rowbuf, stats, st);
+    for (int l = nl - 2; l >= 0; --l) {
+        launch_mg_prolong(lv[l + 1], lv[l], prm.mg_omega, st);
+        for (int s = 0; s < prm.mg_post; ++s) {
+            launch_mg_smooth_colour(lv[l], 0, st);
+            launch_mg_smooth_colour(lv[l], 1, st);
+        }
+    }
+}
+
+// solve_pc_mg (multigrid.cpp:347-357).
+void Solver::solve_mg() {
+    for (std::size_t l = 1; l < lv.size(); ++l) launch_mg_build(lv[l - 1], lv[l], st);
+    SGPU_CUDA(cudaMemsetAsync(w.pc, 0, g.bytes(), st));
+    remove_mean0(w.b);
+    for (int c = 0; c < prm.mg_cycles; ++c) mg_vcycle();
+    remove_mean0(w.pc);
+    last_vcycles = prm.mg_cycles;
+}
+
+void Solver::solve_p() {
+    switch (prm.pressure_solver) {
+    case SGPU_P_JACOBI: solve_jacobi(); break;
+    case SGPU_P_GS_REDBLACK: solve_redblack(); break;
+    case SGPU_P_CG: solve_cg(); break;
+    case SGPU_P_MG: solve_mg(); break;
+    default: throw Error(SGPU_E_INVALID, "unsupported pressure_solver");
+    }
+}
+
+} // namespace sgpu
+
+struct sgpu_handle {
+    std::unique_ptr<sgpu::Solver> s;
+};
+
+namespace {
+
+template <class F> int guarded(F&& f) {
+    try {
+        f();
+        return SGPU_OK;
+    } catch (const sgpu::Error& e) {
+        return sgpu::fail(e.code, e.what());
+    } catch (const std::bad_alloc&) {
+        return sgpu::fail(SGPU_E_NOMEM, "host allocation failed");
+    } catch (const std::exception& e) {
+        return sgpu::fail(SGPU_E_INVALID, e.what());
+    }
+}
+
+#define SGPU_NEED_HANDLE(h)                                                                  \
+    if (!(h) || !(h)->s) return sgpu::fail(SGPU_E_INVALID, "null sgpu handle")
+
+} // namespace
+
+extern "C" {
+
+const char* sgpu_last_error(void) { return sgpu::g_last_error.c_str(); }
+const char* sgpu_version(void) { return "simple-b200 0.1 (sm_100a)"; }
+
+int sgpu_create(const sgpu_params_t* p, const double* u, const double* v, const double* pf,
+                sgpu_handle** out) {
+    if (!p || !out) return sgpu::fail(SGPU_E_INVALID, "sgpu_create: null argument");
+    *out = nullptr;
+    return guarded([&] {
+        auto h = std::make_unique<sgpu_handle>();
+        h->s = std::make_unique<sgpu::Solver>(*p, u, v, pf);
+        *out = h.release();
+    });
+}
+
+int sgpu_destroy(sgpu_handle* h) {
+    if (!h) return SGPU_OK;
+    const int rc = guarded([&] { h->s.reset(); });
+    delete h;
+    return rc;
+}
+
+int sgpu_assemble_u(sgpu_handle* h) {
+    SGPU_NEED_HANDLE(h);
+    return guarded([&] { h->s->assemble_u(); h->s->sync(); });
+}
+int sgpu_bc_u(sgpu_handle* h) {
+    SGPU_NEED_HANDLE(h);
+    return guarded([&] { h->s->bc_u(); h->s->sync(); });
+}
+int sgpu_residual_u(sgpu_handle* h, double* res) {
+    SGPU_NEED_HANDLE(h);
+    return guarded([&] {
+        h->s->residual_u(h->s->res_dev);
+        const double r = h->s->fetch(h->s->res_dev);
+        if (res) *res = r;
+    });
+}
+int sgpu_sweep_u(sgpu_handle* h, int n) {
+    SGPU_NEED_HANDLE(h);
+    return guarded([&] { h->s->sweep_u(n); h->s->sync(); });
+}
+int sgpu_assemble_v(sgpu_handle* h) {
+    SGPU_NEED_HANDLE(h);
+    return guarded([&] { h->s->assemble_v(); h->s->sync(); });
+}
+int sgpu_bc_v(sgpu_handle* h) {
+    SGPU_NEED_HANDLE(h);
+    return guarded([&] { h->s->bc_v(); h->s->sync(); });
+}
+int sgpu_residual_v(sgpu_handle* h, double* res) {
+    SGPU_NEED_HANDLE(h);
+    return guarded([&] {
+        h->s->residual_v(h->s->res_dev + 1);
+        const double r = h->s->fetch(h->s->res_dev + 1);
+        if (res) *res = r;
+    });
+}
+int sgpu_sweep_v(sgpu_handle* h, int n) {
+    SGPU_NEED_HANDLE(h);
+    return guarded([&] { h->s->sweep_v(n); h->s->sync(); });
+}
+int sgpu_assemble_p(sgpu_handle* h, double* res) {
+    SGPU_NEED_HANDLE(h);
+    return guarded([&] {
+        h->s->assemble_p(h->s->res_dev + 2);
+        const double r = h->s->fetch(h->s->res_dev + 2);
+        if (res) *res = r;
+    });
+}
+int sgpu_solve_p(sgpu_handle* h) {
+    SGPU_NEED_HANDLE(h);
+    return guarded([&] {
+        h->s->solve_p();
+        h->s->sync();
+        h->s->finish_stats();
+    });
+}
+int sgpu_correct(sgpu_handle* h) {
+    SGPU_NEED_HANDLE(h);
+    return guarded([&] { h->s->correct(); h->s->sync(); });
+}
+
+int sgpu_outer_iteration(sgpu_handle* h, double res[3], double* phase_seconds) {
+    SGPU_NEED_HANDLE(h);
+    (void)phase_seconds;
+    return guarded([&] {
+        sgpu::Solver& s = *h->s;
+        s.outer_iteration_enqueue(s.res_dev);
+        SGPU_CUDA(cudaMemcpyAsync(s.host_res, s.res_dev, 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                                  s.st));
+        s.sync();
+        if (res) {
+            res[0] = s.host_res[0];
+            res[1] = s.host_res[1];
+            res[2] = s.host_res[2];
+        }
+    });
+}
+
+int sgpu_run(sgpu_handle* h, int maxit, double* log, int print_every, sgpu_result_t* result) {
+    SGPU_NEED_HANDLE(h);
+    return guarded([&] {
+        sgpu::Solver& s = *h->s;
+        sgpu_result_t out{};
+        const auto t0 = std::chrono::steady_clock::now();
+        double mu = 0.0, mv = 0.0, mp = 0.0;
+        for (int iter = 1; iter <= maxit; ++iter) {
+            s.outer_iteration_enqueue(s.res_dev);
+            SGPU_CUDA(cudaMemcpyAsync(s.host_res, s.res_dev, 3 * sizeof(double),
+                                      cudaMemcpyDeviceToHost, s.st));
+            s.sync();
+            const double ru = s.host_res[0], rv = s.host_res[1], rp = s.host_res[2];
+            if (log) {
+                log[4 * (iter - 1) + 0] = iter;
+                log[4 * (iter - 1) + 1] = ru;
+                log[4 * (iter - 1) + 2] = rv;
+                log[4 * (iter - 1) + 3] = rp;
+            }
+            out.iterations = iter;
+            if (print_every > 0 && (iter == 1 || iter % print_every == 0))
+                std::printf("iter %d  res_u %.6e  res_v %.6e  res_p %.6e\n", iter, ru, rv, rp);
+            // Stopping rule of run_outer_loop (solver.cpp:117-129).
+            double tu = ru, tv = rv, tp = rp;
+            if (s.prm.residual_normalisation == SGPU_NORM_RUNNING_MAX) {
+                mu = mu < ru ? ru : mu;
+                mv = mv < rv ? rv : mv;
+                mp = mp < rp ? rp : mp;
+                tu = mu > 0.0 ? ru / mu : 0.0;
+                tv = mv > 0.0 ? rv / mv : 0.0;
+                tp = mp > 0.0 ? rp / mp : 0.0;
+            }
+            double m = tu;
+            if (m < tv) m = tv;
+            if (m < tp) m = tp;
+            if (m <= s.prm.error_tolerance && iter > 1) {
+                out.converged = 1;
+                break;
+            }
+        }
+        out.seconds =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (result) *result = out;
+    });
+}
+
+int sgpu_download(sgpu_handle* h, int id, double* host) {
+    SGPU_NEED_HANDLE(h);
+    if (!host) return sgpu::fail(SGPU_E_INVALID, "sgpu_download: null buffer");
+    return guarded([&] {
+        double* f = h->s->field_ptr(id);
+        if (!f) throw sgpu::Error(SGPU_E_INVALID, "sgpu_download: unknown field id " + std::to_string(id));
+        h->s->download(f, host);
+    });
+}
+
+int sgpu_upload(sgpu_handle* h, int id, const double* host) {
+    SGPU_NEED_HANDLE(h);
+    if (!host) return sgpu::fail(SGPU_E_INVALID, "sgpu_upload: null buffer");
+    return guarded([&] {
+        double* f = h->s->field_ptr(id);
+        if (!f) throw sgpu::Error(SGPU_E_INVALID, "sgpu_upload: unknown field id " + std::to_string(id));
+        h->s->upload(f, host);
+        h->s->sync();
+    });
+}
+
+int sgpu_memory_bytes(sgpu_handle* h, size_t* bytes) {
+    SGPU_NEED_HANDLE(h);
+    if (bytes) *bytes = h->s->bytes;
+    return SGPU_OK;
+}
+
+int sgpu_mg_levels(int NX, int NY, int* nlevels, int* dims) {
+    if (NX < 1 || NY < 1 || !nlevels) return sgpu::fail(SGPU_E_INVALID, "sgpu_mg_levels: bad arguments");
+    // mg_level_dims (multigrid.cpp:143-151): halve while both are even and the result is >= 4 x 4.
+    int nx = NX, ny = NY, n = 0;
+    if (dims) {
+        dims[0] = nx;
+        dims[1] = ny;
+    }
+    n = 1;
+    while (nx % 2 == 0 && ny % 2 == 0 && nx / 2 >= 4 && ny / 2 >= 4 && n < 64) {
+        nx /= 2;
+        ny /= 2;
+        if (dims) {
+            dims[2 * n] = nx;
+            dims[2 * n + 1] = ny;
+        }
+        ++n;
+    }
+    *nlevels = n;
+    return SGPU_OK;
+}
+
+int sgpu_last_solve_stats(sgpu_handle* h, int* cg_iterations, int* mg_vcycles, int* coarse_sweeps,
+                          double* rel_residual) {
+    SGPU_NEED_HANDLE(h);
+    return guarded([&] {
+        sgpu::Solver& s = *h->s;
+        if (s.cg_stats_pending && s.cgs) {
+            sgpu::CgScalars sc{};
+            SGPU_CUDA(cudaMemcpyAsync(&sc, s.cgs, sizeof sc, cudaMemcpyDeviceToHost, s.st));
+            s.sync();
+            s.last_cg_iterations = sc.k;
+            s.last_rel = sc.rel;
+            s.cg_stats_pending = false;
+        }
+        s.finish_stats();
+        if (cg_iterations) *cg_iterations = s.last_cg_iterations;
+        if (mg_vcycles) *mg_vcycles = s.last_vcycles;
+        if (coarse_sweeps) *coarse_sweeps = s.last_coarse_sweeps;
+        if (rel_residual) *rel_residual = s.last_rel;
+    });
+}
+
+int sgpu_ordered_sum(const double* values, int nr, int nc, double* out) {
+    if (!values || !out || nr < 0 || nc < 0) return sgpu::fail(SGPU_E_INVALID, "sgpu_ordered_sum: bad arguments");
+    return guarded([&] {
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+            (void)cudaGetLastError();
+            throw sgpu::Error(SGPU_E_NODEVICE, "GPU error: no CUDA device is visible");
+        }
+        const std::size_t n = static_cast<std::size_t>(nr) * nc;
+        double *d = nullptr, *rows = nullptr, *res = nullptr;
+        unsigned int* counter = nullptr;
+        SGPU_CUDA(cudaMalloc(&d, (n ? n : 1) * sizeof(double)));
+        SGPU_CUDA(cudaMalloc(&rows, (nr ? nr : 1) * sizeof(double)));
+        SGPU_CUDA(cudaMalloc(&res, sizeof(double)));
+        SGPU_CUDA(cudaMalloc(&counter, sizeof(unsigned int)));
+        SGPU_CUDA(cudaMemset(counter, 0, sizeof(unsigned int)));
+        SGPU_CUDA(cudaMemcpy(d, values, n * sizeof(double), cudaMemcpyHostToDevice));
+        sgpu::SumScratch ss;
+        ss.rows = rows;
+        ss.counter = counter;
+        ss.max_rows = nr;
+        ss.max_k = 1;
+        sgpu::launch_ordered_sum(d, 0, nc, nr, nc, 1, res, ss, nullptr, 0);
+        SGPU_CUDA(cudaMemcpy(out, res, sizeof(double), cudaMemcpyDeviceToHost));
+        cudaFree(d);
+        cudaFree(rows);
+        cudaFree(res);
+        cudaFree(counter);
+    });
+}
+
+int sgpu_cnn_load(sgpu_handle* h, const char* path) {
+    SGPU_NEED_HANDLE(h);
+    (void)path;
+    return sgpu::fail(SGPU_E_INVALID, "sgpu_cnn_load: not available in this build");
+}
+
+} // extern "C"

@@ -1,0 +1,177 @@
+"""GPU parity: the B200 solver, called through its C ABI, against the oracle — bit for bit.
+
+Mirrors the reference's GPU tests (simple-hpc tests/hip/test_hip.cpp): a per-phase comparison of
+every State array after every phase on non-trivial fields (3 outer iterations of the 32 x 40
+snapshot case), a fixed-work run, and a determinism check. Unlike the reference GPU backend, the
+residuals are required to be bit-identical too (the reference accepts 1e-12 relative), because the
+device reproduces the CPU's fixed summation order.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import bit_equal, config_text, cuda_available, describe_diff, load_golden, snapshot_config
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
+
+ALL_FIELDS = list(range(28))
+
+
+def case_config(base: str, **ov) -> dict:
+    cfg = snapshot_config(base)
+    cfg.update({k: str(v) for k, v in ov.items()})
+    return cfg
+
+
+def make_pair(sgpu_mod, oracle_mod, cfg: dict, warm_iters: int = 3):
+    """Oracle advanced by warm_iters outer iterations, and a GPU solver holding the same State."""
+    p = sgpu_mod.params_from_config(config_text(cfg))
+    o = oracle_mod.Oracle(p)
+    for _ in range(warm_iters):
+        o.outer_iteration()
+    g = sgpu_mod.Solver(p, o.get(0), o.get(1), o.get(2))
+    for f in ALL_FIELDS:
+        g.upload(f, o.get(f))
+    return p, o, g
+
+
+def assert_same(g, o, fields, phase):
+    for f in fields:
+        a, b = g.download(f), o.get(f)
+        assert bit_equal(a, b), f"after {phase}: field {f}: " + describe_diff(a, b)
+
+
+COMBOS = [
+    ("QUICK", 4, "gs_multicolour", "gs_redblack"),
+    ("UDS", 2, "gs_multicolour", "gs_redblack"),
+    ("QUICK", 4, "gs_multicolour", "mg"),
+    ("UDS", 2, "gs_multicolour", "cg"),
+    ("QUICK", 4, "jacobi", "jacobi"),
+    ("QUICK", 2, "jacobi", "mg"),
+]
+
+
+@pytest.mark.parametrize("scheme,order,ms,ps", COMBOS)
+def test_per_phase_bit_exact(sgpu_mod, oracle_mod, scheme, order, ms, ps):
+    cfg = case_config("converged_32x40", convection_scheme=scheme, diffusion_order=order,
+                      momentum_solver=ms, pressure_solver=ps, error_tolerance=0, maxit=3)
+    p, o, g = make_pair(sgpu_mod, oracle_mod, cfg)
+    cu, cv = sgpu_mod.CU, sgpu_mod.CV
+
+    o.assemble_u(); g.assemble_u()
+    assert_same(g, o, cu, "assemble_u")
+    o.bc_u(); g.bc_u()
+    assert_same(g, o, [0], "bc_u")
+    ro, rg = o.residual_u(), g.residual_u()
+    assert rg == ro, f"residual_u {rg!r} vs {ro!r}"
+    o.sweep_u(p.maxit_inner_u); g.sweep_u(p.maxit_inner_u)
+    assert_same(g, o, [0], "sweep_u")
+
+    o.assemble_v(); g.assemble_v()
+    assert_same(g, o, cv, "assemble_v")
+    o.bc_v(); g.bc_v()
+    assert_same(g, o, [1], "bc_v")
+    ro, rg = o.residual_v(), g.residual_v()
+    assert rg == ro, f"residual_v {rg!r} vs {ro!r}"
+    o.sweep_v(p.maxit_inner_v); g.sweep_v(p.maxit_inner_v)
+    assert_same(g, o, [1], "sweep_v")
+
+    ro, rg = o.assemble_p(), g.assemble_p()
+    assert rg == ro, f"res_p {rg!r} vs {ro!r}"
+    assert_same(g, o, [sgpu_mod.F_AEP, sgpu_mod.F_AWP, sgpu_mod.F_ANP, sgpu_mod.F_ASP,
+                       sgpu_mod.F_APP, sgpu_mod.F_B], "assemble_p")
+    o.solve_p(); g.solve_p()
+    assert_same(g, o, [sgpu_mod.F_PC, sgpu_mod.F_B], "solve_p")
+    if ps == "cg":
+        assert g.last_solve_stats()["cg_iterations"] == o.cg_last_iterations()
+    if ps == "mg":
+        assert g.last_solve_stats()["coarse_sweeps"] == o.mg_last_coarse_sweeps()
+    o.correct(); g.correct()
+    assert_same(g, o, [0, 1, 2], "correct")
+    g.close()
+
+
+@pytest.mark.parametrize("scheme,order,ms,ps", COMBOS)
+def test_outer_iteration_bit_exact(sgpu_mod, oracle_mod, scheme, order, ms, ps):
+    """The fused whole-iteration path gives the oracle's residuals and fields."""
+    cfg = case_config("converged_32x40", convection_scheme=scheme, diffusion_order=order,
+                      momentum_solver=ms, pressure_solver=ps, error_tolerance=0, maxit=3)
+    p, o, g = make_pair(sgpu_mod, oracle_mod, cfg)
+    for it in range(4):
+        ro = o.outer_iteration()
+        rg = g.outer_iteration()
+        assert rg == ro, f"iteration {it}: {rg} vs {ro}"
+    assert_same(g, o, [0, 1, 2, sgpu_mod.F_PC], "4 outer iterations")
+    g.close()
+
+
+def test_fixed_work_200_iterations(sgpu_mod, oracle_mod):
+    """200 outer iterations, 32 x 40, QUICK / 4: fields and residual log identical (test_hip.cpp:166)."""
+    cfg = case_config("converged_32x40", momentum_solver="gs_multicolour",
+                      pressure_solver="gs_redblack", error_tolerance=0, maxit=200)
+    p = sgpu_mod.params_from_config(config_text(cfg))
+    o = oracle_mod.Oracle(p)
+    n, conv, olog = o.run(200)
+    with sgpu_mod.Solver(p) as g:
+        res, glog = g.run(200)
+        assert res.iterations == n == 200 and not res.converged
+        assert bit_equal(glog, olog), describe_diff(glog, olog)
+        assert_same(g, o, [0, 1, 2], "200 iterations")
+
+
+@pytest.mark.parametrize("tag", ["mc_rb_quick4_32x40", "mc_mg_quick4_32x40", "mc_cg_uds2_32x40",
+                                 "jac_jac_quick4_16", "cavity32_re100_mc_mg"])
+def test_reference_golden_runs(sgpu_mod, tag):
+    """Runs of the reference's own sources, reproduced bit for bit on the GPU (stopping iteration too)."""
+    gd = load_golden(f"run_{tag}.npz")
+    p = sgpu_mod.params_from_config(config_text(gd["config"]))
+    with sgpu_mod.Solver(p) as g:
+        res, log = g.run(p.maxit)
+        assert res.iterations == gd["log"].shape[0]
+        assert bool(res.converged) == bool(gd["converged"])
+        assert bit_equal(log, gd["log"]), describe_diff(log, gd["log"])
+        for k, fid in (("u", 0), ("v", 1), ("p", 2)):
+            a = g.download(fid)
+            assert bit_equal(a, gd[k]), f"{k}: " + describe_diff(a, gd[k])
+
+
+def test_deterministic(sgpu_mod):
+    cfg = case_config("short_16", momentum_solver="gs_multicolour", pressure_solver="mg", maxit=50)
+    p = sgpu_mod.params_from_config(config_text(cfg))
+    logs, us = [], []
+    for _ in range(2):
+        with sgpu_mod.Solver(p) as g:
+            _, log = g.run(50)
+            logs.append(log)
+            us.append(g.download(0))
+    assert bit_equal(logs[0], logs[1]) and bit_equal(us[0], us[1])
+
+
+@pytest.mark.parametrize("nx,ny,ps", [(9, 11, "mg"), (13, 17, "gs_redblack"), (24, 40, "mg"),
+                                      (48, 32, "cg"), (1, 6, "gs_redblack"), (6, 1, "mg")])
+def test_odd_and_ragged_grids(sgpu_mod, oracle_mod, nx, ny, ps):
+    cfg = case_config("short_16", N_cells_x=nx, N_cells_y=ny, momentum_solver="gs_multicolour",
+                      pressure_solver=ps, maxit=12, error_tolerance=0)
+    p = sgpu_mod.params_from_config(config_text(cfg))
+    o = oracle_mod.Oracle(p)
+    n, conv, olog = o.run(12)
+    with sgpu_mod.Solver(p) as g:
+        res, glog = g.run(12)
+        assert bit_equal(glog, olog), describe_diff(glog, olog)
+        assert_same(g, o, [0, 1, 2, sgpu_mod.F_PC], f"{nx}x{ny}")
+
+
+def test_gs_lex_rejected_with_message(sgpu_mod):
+    cfg = snapshot_config("short_16")  # gs_lex / gs_lex by default
+    p = sgpu_mod.params_from_config(config_text(cfg))
+    with pytest.raises(sgpu_mod.SgpuError, match="backend = gpu supports"):
+        sgpu_mod.Solver(p)
+
+
+@pytest.mark.parametrize("shape", [(1, 1), (1, 7), (5, 1), (33, 65), (4101, 3), (3, 4101), (300, 257)])
+def test_device_ordered_sum(sgpu_mod, oracle_mod, shape):
+    rng = np.random.default_rng(sum(shape))
+    v = rng.standard_normal(shape) * 10.0 ** rng.integers(-6, 6, shape)
+    assert sgpu_mod.ordered_sum(v) == oracle_mod.ordered_sum(v)

@@ -200,6 +200,18 @@ int sgpu_last_solve_stats(sgpu_handle* h, int* cg_iterations, int* mg_vcycles,
  */
 int sgpu_ordered_sum(const double* values, int nrows_v, int ncols_v, double* out);
 
+/*
+ * Instrumentation. With profiling on, every outer iteration records CUDA events between its phases
+ * on the handle's stream and accumulates the device time per phase (sgpu_phase_seconds, indexed by
+ * SGPU_PH_*), the way the reference's PhaseTimers accumulate wall time (include/simple/timer.hpp).
+ * sgpu_stream returns the handle's cudaStream_t (as void*) so a caller can time on it.
+ * sgpu_launch_count returns the number of kernel launches this library has issued in the process.
+ */
+int sgpu_set_profiling(sgpu_handle* h, int on);
+int sgpu_phase_seconds(sgpu_handle* h, double* out /* SGPU_PH_COUNT */);
+int sgpu_stream(sgpu_handle* h, void** stream);
+long long sgpu_launch_count(void);
+
 /* ---- learned warm start for p' (keys warm_start, cnn_weights) ---- */
 /* Load or replace the network weights of a handle from a file written by sgpu_cnn_save. */
 int sgpu_cnn_load(sgpu_handle* h, const char* path);

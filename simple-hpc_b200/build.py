@@ -37,6 +37,8 @@ SOURCES = {
     "reduce.cu": EXACT,
     "mg.cu": EXACT,
     "cg.cu": EXACT,
+    "fused.cu": EXACT,
+    "mg_fast.cu": EXACT,
 }
 DRIVER = ["driver.cpp"]
 

@@ -27,6 +27,8 @@ struct Error : std::runtime_error {
 
 void set_last_error(const std::string& msg);
 int fail(int code, const std::string& msg); // sets the message, returns code
+// Kernel launches issued by this library (process-wide, for the benchmark's launch count).
+void count_launch();
 
 void params_defaults(sgpu_params_t& p);
 void params_finalize(sgpu_params_t& p);
@@ -41,7 +43,11 @@ void params_from_config(const std::string& text, sgpu_params_t& p);
                                 std::string("GPU error: ") + cudaGetErrorString(e_) +         \
                                     " in " #x);                                               \
     } while (0)
-#define SGPU_LAUNCH() SGPU_CUDA(cudaGetLastError())
+#define SGPU_LAUNCH()                                                                         \
+    do {                                                                                      \
+        ::sgpu::count_launch();                                                               \
+        SGPU_CUDA(cudaGetLastError());                                                        \
+    } while (0)
 #endif
 
 // ---- device layout ----

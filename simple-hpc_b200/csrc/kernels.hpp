@@ -73,6 +73,24 @@ void launch_mg_prolong(const LevelView& C, const LevelView& F, double omega, cud
 void launch_mg_sub_mean(const LevelView& L, double* x, const double* sum, cudaStream_t st);
 // Coarsest-level solve in one CTA (coarse_solve, multigrid.cpp:120-140); *sweeps_out gets the count.
 void launch_mg_coarse(const LevelView& L, double* rowbuf, int* sweeps_out, cudaStream_t st);
+// The whole hierarchy, by value, for the single-CTA tail kernel.
+struct MgLevels {
+    LevelView L[24];
+    int n;
+};
+// Levels [first, n) of one V-cycle in one CTA: down-leg, coarse solve, up-leg (mg_vcycle order).
+void launch_mg_tail(const MgLevels& lv, int first, int pre, int post, double omega, double* rowbuf,
+                    int* sweeps_out, cudaStream_t st);
+
+// ---- streaming multigrid level kernels (mg_fast.cu) ----
+bool mg_fast_supported(int pre, int post);
+// pre red-black sweeps on F (x from F.x, or zero), residual, restriction into C.b (C.x = 0); the
+// smoothed iterate is written to xout (F.x is left unchanged when pre > 0).
+void launch_mg_down(const LevelView& F, const LevelView& C, double* xout, int pre, bool x_zero,
+                    int sms, cudaStream_t st);
+// xout = xin + omega * P C.x, then post red-black sweeps (F's coefficients and b).
+void launch_mg_up(const LevelView& C, const LevelView& F, const double* xin, double* xout,
+                  double omega, int post, int sms, cudaStream_t st);
 
 // ---- conjugate gradient (cg.cu) ----
 struct CgScalars {
@@ -92,6 +110,18 @@ void launch_cg_dq(const DevParams& p, PressurePtr w, CgPtr cg, const CgScalars* 
 void launch_cg_update(const DevParams& p, PressurePtr w, CgPtr cg, const CgScalars* sc,
                       double* cells, std::size_t plane, cudaStream_t st);
 void launch_cg_dir(const DevParams& p, CgPtr cg, const CgScalars* sc, cudaStream_t st);
-void launch_cg_copy_x(const DevParams& p, const double* x, double* cells, cudaStream_t st);
+
+// ---- fused fast path (fused.cu) ----
+int stream_seg_rows(const DevParams& p, int sms);
+// Momentum prep: |R| into cells, AP over the update range, frozen copy xF of x.
+void launch_mom_prep(const DevParams& p, bool v_component, const double* x, const double* oth,
+                     const double* pf, double* xF, double* AP, double* cells, cudaStream_t st);
+// One whole multicolour sweep xin -> xout (every cell of xout written).
+void launch_mom_sweep(const DevParams& p, bool v_component, const double* xin, double* xout,
+                      const double* xF, const double* oth, const double* pf, int seg_rows,
+                      cudaStream_t st);
+void launch_assemble_p_fused(const DevParams& p, const double* APU, const double* APV,
+                             const double* u, const double* v, PressurePtr w, double* cabs,
+                             double* cb, cudaStream_t st);
 
 } // namespace sgpu

@@ -161,7 +161,78 @@ __global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(LevelView L, doubl
     if (threadIdx.x == 0 && sweeps_out) *sweeps_out = sweeps;
 }
 
+// restrict_residual (multigrid.cpp:90-103) inside one CTA.
+__device__ void cta_restrict(const LevelView& F, const LevelView& C) {
+    const int n = C.nx * C.ny, fs = F.stride;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const int I = k / C.ny, J = k % C.ny;
+        const int f = 2 * I * fs + 2 * J, c = I * C.stride + J;
+        C.b[c] = F.r[f] + F.r[f + 1] + F.r[f + fs] + F.r[f + fs + 1];
+        C.x[c] = 0.0;
+    }
+    __syncthreads();
+}
+
+// prolong (multigrid.cpp:106-116) inside one CTA.
+__device__ void cta_prolong(const LevelView& C, const LevelView& F, double omega) {
+    const int n = F.nx * F.ny;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const int i = k / F.ny, j = k % F.ny;
+        F.x[i * F.stride + j] += omega * C.x[(i / 2) * C.stride + j / 2];
+    }
+    __syncthreads();
+}
+
+// Levels [first, nl) of one V-cycle (mg_vcycle, multigrid.cpp:299-323) in one CTA: the small
+// levels are latency-bound, so they run back to back with a block barrier between passes.
+__global__ void __launch_bounds__(kCoarseThreads)
+    k_mg_tail(MgLevels lv, int first, int pre, int post, double omega, double* rowbuf,
+              int* sweeps_out) {
+    const int nl = lv.n;
+    for (int l = first; l + 1 < nl; ++l) {
+        for (int s = 0; s < pre; ++s) {
+            cta_smooth_colour(lv.L[l], 0);
+            cta_smooth_colour(lv.L[l], 1);
+        }
+        cta_residual(lv.L[l]);
+        cta_restrict(lv.L[l], lv.L[l + 1]);
+    }
+    // coarse_solve (multigrid.cpp:120-140)
+    const LevelView& L = lv.L[nl - 1];
+    cta_remove_mean(L, rowbuf, L.b);
+    const double* b = L.b;
+    const double bb = cta_det_sum(L, rowbuf, [b](int q) { return b[q] * b[q]; });
+    int sweeps = 0;
+    if (bb > 0.0) {
+        const double bn = sqrt(bb);
+        const double* r = L.r;
+        while (sweeps < 200) {
+            cta_smooth_colour(L, 0);
+            cta_smooth_colour(L, 1);
+            ++sweeps;
+            cta_residual(L);
+            const double rr = cta_det_sum(L, rowbuf, [r](int q) { return r[q] * r[q]; });
+            if (sqrt(rr) < 1e-10 * bn) break;
+        }
+    }
+    cta_remove_mean(L, rowbuf, L.x);
+    if (threadIdx.x == 0 && sweeps_out) *sweeps_out = sweeps;
+    for (int l = nl - 2; l >= first; --l) {
+        cta_prolong(lv.L[l + 1], lv.L[l], omega);
+        for (int s = 0; s < post; ++s) {
+            cta_smooth_colour(lv.L[l], 0);
+            cta_smooth_colour(lv.L[l], 1);
+        }
+    }
+}
+
 } // namespace
+
+void launch_mg_tail(const MgLevels& lv, int first, int pre, int post, double omega, double* rowbuf,
+                    int* sweeps_out, cudaStream_t st) {
+    k_mg_tail<<<1, kCoarseThreads, 0, st>>>(lv, first, pre, post, omega, rowbuf, sweeps_out);
+    SGPU_LAUNCH();
+}
 
 void launch_mg_build(const LevelView& F, const LevelView& C, cudaStream_t st) {
     k_mg_build<<<grid2(C.nx, C.ny), dim3(BX, BY), 0, st>>>(F, C);

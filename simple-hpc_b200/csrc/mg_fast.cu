@@ -1,0 +1,250 @@
+// mg_fast.cu — the multigrid V-cycle of multigrid.cpp with fused, streaming level kernels (FP64,
+// bit-identical to the reference).
+//
+// Per fine level two passes over memory instead of one per colour:
+//  * k_mg_down: `pre` red-black sweeps (smooth, multigrid.cpp:46-70), the residual (:73-87) and the
+//    2x2 restriction (:90-103) in one streaming pass. A CTA owns a strip of columns plus a halo and
+//    walks it top to bottom; in sweep s the cell (I, J) of colour c = (I + J) & 1 is updated at step
+//    t = I + 4s + 2c, so each cell sees its neighbours in exactly the reference's colour order; the
+//    residual of row I is formed at step I + 4 pre, when its neighbours are final, and pairs of
+//    residual rows are summed 2x2 (lanes exchange the odd column by shuffle) into the coarse
+//    right-hand side. The residual array itself is never stored.
+//  * k_mg_up: prolongation with over-correction (:106-116) applied to each row as it arrives,
+//    followed by `post` red-black sweeps, in the same streaming order.
+// The smoothed iterate goes to a second buffer (CTAs read their neighbours' rows as halo). Levels
+// below a size threshold and the coarsest solve run in one CTA (k_mg_tail in mg.cu).
+#include "kernels.hpp"
+
+namespace sgpu {
+
+namespace {
+
+constexpr int kRing = 32;
+constexpr int kPD = 8; // prefetch distance in rows
+
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Window geometry shared by both kernels. Level indices: interior 0 <= I < nx, 0 <= J < ny; the
+// arrays hold a zero ring at I = -1, nx and J = -1, ny.
+struct Win {
+    int R0, R1;      // owned rows
+    int L0, L1;      // loaded rows [L0, L1)
+    int J0, C0;      // first owned column; first loaded column (even)
+    int W;           // owned columns per CTA
+    bool cut_top, cut_bot, cut_left, cut_right;
+};
+
+template <int NT>
+__device__ __forceinline__ Win make_win(const LevelView& L, int seg_rows, int HC) {
+    Win w;
+    w.W = NT - 2 * HC;
+    w.R0 = blockIdx.y * seg_rows;
+    w.R1 = min(w.R0 + seg_rows, L.nx);
+    w.L0 = max(w.R0 - HC, -1);
+    w.L1 = min(w.R1 + HC, L.nx + 1);
+    w.J0 = blockIdx.x * w.W;
+    w.C0 = w.J0 - HC;
+    w.cut_top = w.L0 > -1;
+    w.cut_bot = w.L1 < L.nx + 1;
+    w.cut_left = w.C0 > -1;
+    w.cut_right = w.C0 + NT < L.ny + 1;
+    return w;
+}
+
+// Is pass k's update (or, with k = 2 * sweeps, the residual) of (I, Jc) computable from the window?
+__device__ __forceinline__ bool in_cone(const Win& w, int I, int Jc, int k, int NT) {
+    return (!w.cut_top || I >= w.L0 + 1 + k) && (!w.cut_bot || I <= w.L1 - 2 - k) &&
+           (!w.cut_left || Jc >= w.C0 + 1 + k) && (!w.cut_right || Jc <= w.C0 + NT - 2 - k);
+}
+
+// Red-black two-statement update of one cell (multigrid.cpp:61-63) on the ring.
+template <int NT>
+__device__ __forceinline__ void rb_update(const LevelView& L, double (*ring)[NT], int I, int Jc,
+                                          int tid) {
+    const int q = I * L.stride + Jc;
+    double* row = ring[I & (kRing - 1)];
+    const double ap = L.AP[q];
+    double x = L.b[q] / ap;
+    x += (L.AE[q] * row[tid + 1] + L.AW[q] * row[tid - 1] + L.AS[q] * ring[(I + 1) & (kRing - 1)][tid] +
+          L.AN[q] * ring[(I - 1) & (kRing - 1)][tid]) /
+         ap;
+    row[tid] = x;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT, 2)
+    k_mg_down(LevelView L, LevelView C, double* __restrict__ xout, int pre, int x_zero, int seg_rows,
+              int HC) {
+    extern __shared__ double smem[];
+    double(*ring)[NT] = reinterpret_cast<double(*)[NT]>(smem);
+    const Win w = make_win<NT>(L, seg_rows, HC);
+    const int tid = threadIdx.x;
+    const int Jc = w.C0 + tid;
+    const bool cload = Jc >= -1 && Jc <= L.ny;
+    const bool cint = Jc >= 0 && Jc < L.ny;
+    const bool cown = cint && Jc >= w.J0 && Jc < w.J0 + w.W;
+    const int s = L.stride;
+
+    int next = w.L0;
+    auto issue = [&]() {
+        if (next < w.L1 && cload) {
+            double* dst = &ring[next & (kRing - 1)][tid];
+            if (x_zero) *dst = 0.0;
+            else cp_async8(dst, L.x + next * s + Jc);
+        }
+        cp_async_commit();
+        ++next;
+    };
+    for (int k = 0; k < kPD + 2; ++k) issue(); // rows L0 .. L0 + 1 + kPD
+
+    const int res_lag = 4 * pre;
+    const int t_last = w.R1 - 1 + res_lag;
+    double r_prev = 0.0;
+    for (int t = w.L0; t <= t_last; ++t) {
+        cp_async_wait<kPD>(); // rows <= t + 1 have landed
+        __syncthreads();
+        issue();
+        const int cpar = (t + Jc + 4) & 1;
+        for (int sw = 0; sw < pre; ++sw) {
+            const int I = t - 2 * cpar - 4 * sw;
+            if (cint && I >= 0 && I < L.nx && in_cone(w, I, Jc, 2 * sw + cpar, NT))
+                rb_update<NT>(L, ring, I, Jc, tid);
+        }
+        // Residual of row Ir = t - 4 pre: its neighbours had their last update at step <= t - 1.
+        const int Ir = t - res_lag;
+        double r = 0.0;
+        if (cint && Ir >= 0 && Ir < L.nx && in_cone(w, Ir, Jc, 2 * pre, NT)) {
+            const int q = Ir * s + Jc;
+            const double* row = ring[Ir & (kRing - 1)];
+            r = L.b[q] - (L.AP[q] * row[tid] -
+                          (L.AE[q] * row[tid + 1] + L.AW[q] * row[tid - 1] +
+                           L.AS[q] * ring[(Ir + 1) & (kRing - 1)][tid] +
+                           L.AN[q] * ring[(Ir - 1) & (kRing - 1)][tid]));
+        }
+        // Restriction of the row pair (Ir - 1, Ir): C.b = r[f] + r[f+1] + r[f+fs] + r[f+fs+1].
+        if ((Ir & 1) && Ir >= 1) { // uniform over the CTA
+            const double rp_odd = __shfl_down_sync(0xffffffffu, r_prev, 1);
+            const double r_odd = __shfl_down_sync(0xffffffffu, r, 1);
+            const int R = Ir >> 1;
+            if (cown && !(Jc & 1) && Ir - 1 >= w.R0 && Ir < w.R1 && R < C.nx) {
+                const int cq = R * C.stride + (Jc >> 1);
+                C.b[cq] = r_prev + rp_odd + r + r_odd;
+                C.x[cq] = 0.0;
+            }
+        }
+        r_prev = r;
+        // The smoothed iterate: row t - 4 pre + 1 had its last update at step t - 1.
+        if (pre > 0) {
+            const int rw = t - res_lag + 1;
+            if (cown && rw >= w.R0 && rw < w.R1) xout[rw * s + Jc] = ring[rw & (kRing - 1)][tid];
+        }
+    }
+    cp_async_wait<0>();
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT, 2)
+    k_mg_up(LevelView C, LevelView L, const double* __restrict__ xin, double* __restrict__ xout,
+            double omega, int post, int seg_rows, int HC) {
+    extern __shared__ double smem[];
+    double(*ring)[NT] = reinterpret_cast<double(*)[NT]>(smem);
+    const Win w = make_win<NT>(L, seg_rows, HC);
+    const int tid = threadIdx.x;
+    const int Jc = w.C0 + tid;
+    const bool cload = Jc >= -1 && Jc <= L.ny;
+    const bool cint = Jc >= 0 && Jc < L.ny;
+    const bool cown = cint && Jc >= w.J0 && Jc < w.J0 + w.W;
+    const int s = L.stride;
+
+    int next = w.L0;
+    auto issue = [&]() {
+        if (next < w.L1 && cload) cp_async8(&ring[next & (kRing - 1)][tid], xin + next * s + Jc);
+        cp_async_commit();
+        ++next;
+    };
+    for (int k = 0; k < kPD + 3; ++k) issue(); // rows L0 .. L0 + 2 + kPD
+
+    const int lag = 4 * post;
+    const int t_last = w.R1 - 1 + lag - 1 + 1;
+    for (int t = w.L0 - 2; t <= t_last; ++t) {
+        if (t >= w.L0) cp_async_wait<kPD>(); // rows <= t + 2 have landed
+        else cp_async_wait<kPD + 1>();
+        __syncthreads();
+        if (t >= w.L0) issue();
+        // Prolongation of row t + 2 (read first at step t + 1): x += omega * coarse x.
+        const int Ip = t + 2;
+        if (cint && Ip >= 0 && Ip < L.nx && Ip < w.L1) {
+            double* cell = &ring[Ip & (kRing - 1)][tid];
+            *cell += omega * C.x[(Ip >> 1) * C.stride + (Jc >> 1)];
+        }
+        const int cpar = (t + Jc + 4) & 1;
+        for (int sw = 0; sw < post; ++sw) {
+            const int I = t - 2 * cpar - 4 * sw;
+            if (cint && I >= 0 && I < L.nx && in_cone(w, I, Jc, 2 * sw + cpar, NT))
+                rb_update<NT>(L, ring, I, Jc, tid);
+        }
+        const int rw = t - lag + 1;
+        if (cown && rw >= w.R0 && rw < w.R1) xout[rw * s + Jc] = ring[rw & (kRing - 1)][tid];
+    }
+    cp_async_wait<0>();
+}
+
+constexpr int kNT = 256;
+
+int seg_for(const LevelView& L, int HC, int sms) {
+    const int W = kNT - 2 * HC;
+    const int strips = (L.ny + W - 1) / W;
+    const int want = (2 * sms + strips - 1) / strips;
+    int seg = (L.nx + want - 1) / want;
+    seg = (seg + 1) & ~1; // even: restriction pairs stay inside one CTA
+    const int min_seg = 2 * HC + 8;
+    if (seg < min_seg) seg = min_seg;
+    return seg;
+}
+
+template <class K> void allow_smem(K kernel, bool& done) {
+    if (!done) {
+        SGPU_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kRing * kNT * static_cast<int>(sizeof(double))));
+        done = true;
+    }
+}
+
+} // namespace
+
+bool mg_fast_supported(int pre, int post) { return pre >= 0 && pre <= 4 && post >= 0 && post <= 4; }
+
+void launch_mg_down(const LevelView& F, const LevelView& C, double* xout, int pre, bool x_zero,
+                    int sms, cudaStream_t st) {
+    const int HC = 2 * pre + 2;
+    const int seg = seg_for(F, HC, sms);
+    const int W = kNT - 2 * HC;
+    const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
+    static bool attr = false;
+    allow_smem(k_mg_down<kNT>, attr);
+    k_mg_down<kNT><<<grid, kNT, kRing * kNT * sizeof(double), st>>>(F, C, xout, pre, x_zero ? 1 : 0,
+                                                                   seg, HC);
+    SGPU_LAUNCH();
+}
+
+void launch_mg_up(const LevelView& C, const LevelView& F, const double* xin, double* xout,
+                  double omega, int post, int sms, cudaStream_t st) {
+    const int HC = 2 * post + 2;
+    const int seg = seg_for(F, HC, sms);
+    const int W = kNT - 2 * HC;
+    const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
+    static bool attr = false;
+    allow_smem(k_mg_up<kNT>, attr);
+    k_mg_up<kNT><<<grid, kNT, kRing * kNT * sizeof(double), st>>>(C, F, xin, xout, omega, post, seg,
+                                                                 HC);
+    SGPU_LAUNCH();
+}
+
+} // namespace sgpu

@@ -11,6 +11,7 @@
 //    residuals instead of a device synchronisation per phase.
 #include "kernels.hpp"
 
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -23,7 +24,10 @@ namespace sgpu {
 
 namespace {
 thread_local std::string g_last_error;
+std::atomic<long long> g_launches{0};
 }
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 int fail(int code, const std::string& msg) {
@@ -80,6 +84,18 @@ struct Solver {
     std::vector<LevelView> lv;
     double* mg_r0 = nullptr;
     double* coarse_rowbuf = nullptr;
+    bool mg_fast = false;            // streaming level kernels (mg_fast.cu) + single-CTA tail
+    int mg_tail = 0;                 // first level handled by the tail kernel
+    std::vector<double*> mg_x2;      // second iterate buffer per streamed level (interior (0,0))
+    MgLevels mgl{};
+    void mg_vcycle_fast(bool x_is_zero);
+
+    // fused fast path (multicolour momentum): frozen velocity copy and the sweep ping-pong buffer
+    bool fast = false;
+    double* xF = nullptr;
+    double* tmp = nullptr;
+    int sms = 148;
+    int seg_rows = 64;
 
     int ncol = 5;
     int last_cg_iterations = 0, last_vcycles = 0, last_coarse_sweeps = 0;
@@ -159,18 +175,100 @@ struct Solver {
     void mg_vcycle();
     void remove_mean0(double* f);
 
-    void outer_iteration_enqueue(double* res3) {
-        assemble_u();
-        bc_u();
-        residual_u(res3 + 0);
-        sweep_u(prm.maxit_inner_u);
-        assemble_v();
-        bc_v();
-        residual_v(res3 + 1);
-        sweep_v(prm.maxit_inner_v);
-        assemble_p(res3 + 2);
+    // One momentum phase on the fused path: bc, residual + AP + frozen copy, n streaming sweeps.
+    void fast_momentum(bool vcomp, double* res) {
+        double* x = vcomp ? v : u;
+        const double* oth = vcomp ? u : v;
+        double* AP = vcomp ? cv.a[8] : cu.a[8];
+        // Phase attribution: the prep pass is the assembly, the ordered sum the residual.
+        mark(vcomp ? SGPU_PH_BC_V : SGPU_PH_BC_U);
+        if (vcomp) launch_bc_v(dp, v, st);
+        else launch_bc_u(dp, u, st);
+        mark(vcomp ? SGPU_PH_ASSEMBLE_V : SGPU_PH_ASSEMBLE_U);
+        launch_mom_prep(dp, vcomp, x, oth, pf, xF, AP, cells, st);
+        mark(vcomp ? SGPU_PH_RESIDUAL_V : SGPU_PH_RESIDUAL_U);
+        if (vcomp) launch_ordered_sum(cells, 0, prm.NY, prm.NX - 1, prm.NY, 1, res, ss, nullptr, st);
+        else launch_ordered_sum(cells, 0, prm.NY - 1, prm.NX, prm.NY - 1, 1, res, ss, nullptr, st);
+        mark(vcomp ? SGPU_PH_SWEEP_V : SGPU_PH_SWEEP_U);
+        const int n = vcomp ? prm.maxit_inner_v : prm.maxit_inner_u;
+        double* in = x;
+        double* out = tmp;
+        for (int k = 0; k < n; ++k) {
+            launch_mom_sweep(dp, vcomp, in, out, xF, oth, pf, seg_rows, st);
+            std::swap(in, out);
+        }
+        if (in != x) launch_copy(in, x, g.elems(), st);
+    }
+
+    void fast_iteration_enqueue(double* res3) {
+        fast_momentum(false, res3 + 0);
+        fast_momentum(true, res3 + 1);
+        mark(SGPU_PH_ASSEMBLE_P);
+        launch_assemble_p_fused(dp, cu.a[8], cv.a[8], u, v, w, cells, nullptr, st);
+        launch_ordered_sum(cells, 0, prm.NY, prm.NX, prm.NY, 1, res3 + 2, ss, nullptr, st);
+        mark(SGPU_PH_SOLVE_P);
         solve_p();
+        mark(SGPU_PH_CORRECT);
         correct();
+        mark(SGPU_PH_COUNT);
+    }
+
+    // ---- per-phase device timing (CUDA events on the solver's stream) ----
+    bool profiling = false;
+    cudaEvent_t ev[SGPU_PH_COUNT + 1] = {};
+    bool ev_used[SGPU_PH_COUNT + 1] = {};
+    int ev_order[SGPU_PH_COUNT + 2] = {};
+    int ev_n = 0;
+    double phase_acc[SGPU_PH_COUNT] = {};
+    // Record the start of phase ph (SGPU_PH_COUNT marks the end of the iteration).
+    void mark(int ph) {
+        if (!profiling) return;
+        if (!ev[ph]) SGPU_CUDA(cudaEventCreate(&ev[ph]));
+        SGPU_CUDA(cudaEventRecord(ev[ph], st));
+        ev_order[ev_n++] = ph;
+    }
+    // After the stream is synchronised: add each phase's time to phase_acc (and to out if given).
+    void collect_phases(double* out) {
+        if (!profiling) return;
+        for (int k = 0; k + 1 < ev_n; ++k) {
+            float ms = 0.0f;
+            SGPU_CUDA(cudaEventElapsedTime(&ms, ev[ev_order[k]], ev[ev_order[k + 1]]));
+            phase_acc[ev_order[k]] += ms * 1e-3;
+            if (out) out[ev_order[k]] += ms * 1e-3;
+        }
+        ev_n = 0;
+    }
+
+    void iteration_enqueue(double* res3) {
+        ev_n = 0;
+        if (fast) fast_iteration_enqueue(res3);
+        else outer_iteration_enqueue(res3);
+    }
+
+    void outer_iteration_enqueue(double* res3) {
+        mark(SGPU_PH_ASSEMBLE_U);
+        assemble_u();
+        mark(SGPU_PH_BC_U);
+        bc_u();
+        mark(SGPU_PH_RESIDUAL_U);
+        residual_u(res3 + 0);
+        mark(SGPU_PH_SWEEP_U);
+        sweep_u(prm.maxit_inner_u);
+        mark(SGPU_PH_ASSEMBLE_V);
+        assemble_v();
+        mark(SGPU_PH_BC_V);
+        bc_v();
+        mark(SGPU_PH_RESIDUAL_V);
+        residual_v(res3 + 1);
+        mark(SGPU_PH_SWEEP_V);
+        sweep_v(prm.maxit_inner_v);
+        mark(SGPU_PH_ASSEMBLE_P);
+        assemble_p(res3 + 2);
+        mark(SGPU_PH_SOLVE_P);
+        solve_p();
+        mark(SGPU_PH_CORRECT);
+        correct();
+        mark(SGPU_PH_COUNT);
     }
     void sync() { SGPU_CUDA(cudaStreamSynchronize(st)); }
     double fetch(const double* dev) {
@@ -244,6 +342,15 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
     w.pc = field();
     if (p.momentum_solver == SGPU_MOM_JACOBI || p.pressure_solver == SGPU_P_JACOBI)
         scratch = field();
+    fast = p.momentum_solver == SGPU_MOM_GS_MULTICOLOUR;
+    if (fast) {
+        xF = field();
+        tmp = field();
+        int dev = 0;
+        SGPU_CUDA(cudaGetDevice(&dev));
+        SGPU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        seg_rows = stream_seg_rows(dp, sms);
+    }
     plane = static_cast<std::size_t>(p.NX) * p.NY;
     const int kplanes = p.pressure_solver == SGPU_P_CG ? 4 : 2;
     cells = dalloc<double>(plane * kplanes);
@@ -310,6 +417,23 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
             }
         }
         coarse_rowbuf = dalloc<double>(static_cast<std::size_t>(maxnx) + 1);
+        // Streaming V-cycle: levels above kTailCells cells get a second iterate buffer; the rest
+        // run in the single-CTA tail kernel.
+        constexpr int kTailCells = 1024;
+        mg_fast = mg_fast_supported(p.mg_pre, p.mg_post) && p.mg_pre >= 1 && nl <= 24;
+        mg_tail = 0;
+        while (mg_tail < nl - 1 && lv[mg_tail].nx * lv[mg_tail].ny > kTailCells) ++mg_tail;
+        mg_x2.assign(nl, nullptr);
+        for (int l = 0; mg_fast && l < mg_tail; ++l) {
+            if (l == 0) {
+                mg_x2[0] = field() + (lv[0].x - w.pc);
+            } else {
+                const std::size_t n = static_cast<std::size_t>(lv[l].nx + 2) * lv[l].stride;
+                mg_x2[l] = dalloc<double>(n) + (lv[l].stride + 1);
+            }
+        }
+        mgl.n = nl;
+        for (int l = 0; l < nl && l < 24; ++l) mgl.L[l] = lv[l];
     }
 
     if (hu) upload(u, hu);
@@ -448,9 +572,24 @@ void Solver::solve_mg() {
     for (std::size_t l = 1; l < lv.size(); ++l) launch_mg_build(lv[l - 1], lv[l], st);
     SGPU_CUDA(cudaMemsetAsync(w.pc, 0, g.bytes(), st));
     remove_mean0(w.b);
-    for (int c = 0; c < prm.mg_cycles; ++c) mg_vcycle();
+    for (int c = 0; c < prm.mg_cycles; ++c) {
+        if (mg_fast) mg_vcycle_fast(c == 0);
+        else mg_vcycle();
+    }
     remove_mean0(w.pc);
     last_vcycles = prm.mg_cycles;
+}
+
+// mg_vcycle with the streaming level kernels: levels [0, mg_tail) go down and up in one pass
+// each, the rest (and the coarse solve) in the single-CTA tail kernel.
+void Solver::mg_vcycle_fast(bool x_is_zero) {
+    const int nl = static_cast<int>(lv.size());
+    for (int l = 0; l < mg_tail; ++l)
+        launch_mg_down(lv[l], lv[l + 1], mg_x2[l], prm.mg_pre, x_is_zero || l > 0, sms, st);
+    launch_mg_tail(mgl, mg_tail, prm.mg_pre, prm.mg_post, prm.mg_omega, coarse_rowbuf, stats, st);
+    for (int l = mg_tail - 1; l >= 0; --l)
+        launch_mg_up(lv[l + 1], lv[l], mg_x2[l], lv[l].x, prm.mg_omega, prm.mg_post, sms, st);
+    (void)nl;
 }
 
 void Solver::solve_p() {
@@ -575,13 +714,16 @@ int sgpu_correct(sgpu_handle* h) {
 
 int sgpu_outer_iteration(sgpu_handle* h, double res[3], double* phase_seconds) {
     SGPU_NEED_HANDLE(h);
-    (void)phase_seconds;
     return guarded([&] {
         sgpu::Solver& s = *h->s;
-        s.outer_iteration_enqueue(s.res_dev);
+        const bool was = s.profiling;
+        if (phase_seconds) s.profiling = true;
+        s.iteration_enqueue(s.res_dev);
         SGPU_CUDA(cudaMemcpyAsync(s.host_res, s.res_dev, 3 * sizeof(double), cudaMemcpyDeviceToHost,
                                   s.st));
         s.sync();
+        s.collect_phases(phase_seconds);
+        s.profiling = was;
         if (res) {
             res[0] = s.host_res[0];
             res[1] = s.host_res[1];
@@ -598,10 +740,11 @@ int sgpu_run(sgpu_handle* h, int maxit, double* log, int print_every, sgpu_resul
         const auto t0 = std::chrono::steady_clock::now();
         double mu = 0.0, mv = 0.0, mp = 0.0;
         for (int iter = 1; iter <= maxit; ++iter) {
-            s.outer_iteration_enqueue(s.res_dev);
+            s.iteration_enqueue(s.res_dev);
             SGPU_CUDA(cudaMemcpyAsync(s.host_res, s.res_dev, 3 * sizeof(double),
                                       cudaMemcpyDeviceToHost, s.st));
             s.sync();
+            s.collect_phases(out.phase_seconds);
             const double ru = s.host_res[0], rv = s.host_res[1], rp = s.host_res[2];
             if (log) {
                 log[4 * (iter - 1) + 0] = iter;
@@ -736,6 +879,28 @@ int sgpu_ordered_sum(const double* values, int nr, int nc, double* out) {
         cudaFree(counter);
     });
 }
+
+int sgpu_set_profiling(sgpu_handle* h, int on) {
+    SGPU_NEED_HANDLE(h);
+    h->s->profiling = on != 0;
+    return SGPU_OK;
+}
+
+int sgpu_phase_seconds(sgpu_handle* h, double* out) {
+    SGPU_NEED_HANDLE(h);
+    if (!out) return sgpu::fail(SGPU_E_INVALID, "sgpu_phase_seconds: null output");
+    for (int k = 0; k < SGPU_PH_COUNT; ++k) out[k] = h->s->phase_acc[k];
+    return SGPU_OK;
+}
+
+int sgpu_stream(sgpu_handle* h, void** stream) {
+    SGPU_NEED_HANDLE(h);
+    if (!stream) return sgpu::fail(SGPU_E_INVALID, "sgpu_stream: null output");
+    *stream = static_cast<void*>(h->s->st);
+    return SGPU_OK;
+}
+
+long long sgpu_launch_count(void) { return sgpu::g_launches.load(); }
 
 int sgpu_cnn_load(sgpu_handle* h, const char* path) {
     SGPU_NEED_HANDLE(h);

@@ -109,6 +109,8 @@ def lib() -> C.CDLL:
             "sgpu_mg_levels": (I, [I, I, C.POINTER(I), C.POINTER(I)]),
             "sgpu_last_solve_stats": (I, [H, C.POINTER(I), C.POINTER(I), C.POINTER(I), D]),
             "sgpu_ordered_sum": (I, [D, I, I, D]),
+            "sgpu_set_profiling": (I, [H, I]), "sgpu_phase_seconds": (I, [H, D]),
+            "sgpu_stream": (I, [H, C.POINTER(C.c_void_p)]), "sgpu_launch_count": (C.c_longlong, []),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -149,6 +151,10 @@ def mg_levels(nx: int, ny: int) -> list[tuple[int, int]]:
     dims = (C.c_int * 128)()
     _check(lib().sgpu_mg_levels(nx, ny, C.byref(n), dims))
     return [(dims[2 * k], dims[2 * k + 1]) for k in range(n.value)]
+
+
+def launch_count() -> int:
+    return int(lib().sgpu_launch_count())
 
 
 def ordered_sum(values: np.ndarray) -> float:
@@ -245,6 +251,19 @@ class Solver:
         n = C.c_size_t()
         _check(lib().sgpu_memory_bytes(self._h, C.byref(n)))
         return n.value
+
+    def set_profiling(self, on: bool) -> None:
+        _check(lib().sgpu_set_profiling(self._h, 1 if on else 0))
+
+    def phase_seconds(self) -> dict:
+        out = np.zeros(12)
+        _check(lib().sgpu_phase_seconds(self._h, _dptr(out)))
+        return dict(zip(PHASES, out.tolist()))
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(lib().sgpu_stream(self._h, C.byref(s)))
+        return s.value or 0
 
     def last_solve_stats(self) -> dict:
         a, b, c, r = C.c_int(), C.c_int(), C.c_int(), C.c_double()

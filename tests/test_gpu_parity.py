@@ -163,6 +163,22 @@ def test_odd_and_ragged_grids(sgpu_mod, oracle_mod, nx, ny, ps):
         assert_same(g, o, [0, 1, 2, sgpu_mod.F_PC], f"{nx}x{ny}")
 
 
+@pytest.mark.parametrize("nx,ny,scheme,order", [(200, 520, "QUICK", 4), (130, 600, "UDS", 2),
+                                                (520, 96, "QUICK", 2)])
+def test_strip_and_segment_cuts(sgpu_mod, oracle_mod, nx, ny, scheme, order):
+    """Grids wide and tall enough that the streaming kernels split both rows and columns."""
+    cfg = case_config("short_16", N_cells_x=nx, N_cells_y=ny, Re=1000, convection_scheme=scheme,
+                      diffusion_order=order, momentum_solver="gs_multicolour", pressure_solver="mg",
+                      maxit=3, error_tolerance=0)
+    p = sgpu_mod.params_from_config(config_text(cfg))
+    o = oracle_mod.Oracle(p)
+    n, conv, olog = o.run(3)
+    with sgpu_mod.Solver(p) as g:
+        res, glog = g.run(3)
+        assert bit_equal(glog, olog), describe_diff(glog, olog)
+        assert_same(g, o, [0, 1, 2, sgpu_mod.F_PC, sgpu_mod.F_B, sgpu_mod.F_APP], f"{nx}x{ny}")
+
+
 def test_gs_lex_rejected_with_message(sgpu_mod):
     cfg = snapshot_config("short_16")  # gs_lex / gs_lex by default
     p = sgpu_mod.params_from_config(config_text(cfg))

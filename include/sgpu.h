@@ -200,6 +200,7 @@ int sgpu_last_solve_stats(sgpu_handle* h, int* cg_iterations, int* mg_vcycles,
  */
 int sgpu_ordered_sum(const double* values, int nrows_v, int ncols_v, double* out);
 
+
 /*
  * Instrumentation. With profiling on, every outer iteration records CUDA events between its phases
  * on the handle's stream and accumulates the device time per phase (sgpu_phase_seconds, indexed by
@@ -211,6 +212,16 @@ int sgpu_set_profiling(sgpu_handle* h, int on);
 int sgpu_phase_seconds(sgpu_handle* h, double* out /* SGPU_PH_COUNT */);
 int sgpu_stream(sgpu_handle* h, void** stream);
 long long sgpu_launch_count(void);
+
+/*
+ * Write the reference's output files into p->output_dir from host arrays: u.csv, v.csv, p.csv,
+ * ux_centre.csv, uy_centre.csv (when write_fields), alog.csv, timing.csv, run_info.json, in the
+ * reference's formats (write_outputs, src/io.cpp:43-151; cell_centre, :22-31). log holds
+ * 4 doubles per iteration as sgpu_run writes it. Runs on the host only.
+ */
+int sgpu_write_outputs(const sgpu_params_t* p, const double* u, const double* v, const double* pf,
+                       const double* log, int iterations, const sgpu_result_t* result,
+                       const char* cfg_path, const char* git_hash, const char* compiler);
 
 /* ---- learned warm start for p' (keys warm_start, cnn_weights) ---- */
 /* Load or replace the network weights of a handle from a file written by sgpu_cnn_save. */

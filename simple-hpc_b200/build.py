@@ -39,6 +39,7 @@ SOURCES = {
     "cg.cu": EXACT,
     "fused.cu": EXACT,
     "mg_fast.cu": EXACT,
+    "io.cpp": EXACT,
 }
 DRIVER = ["driver.cpp"]
 
@@ -48,6 +49,15 @@ def nvcc() -> str:
         if cand and Path(cand).exists():
             return cand
     raise RuntimeError("nvcc not found")
+
+
+def git_hash() -> str:
+    try:
+        r = subprocess.run(["git", "-C", str(HERE), "rev-parse", "--short", "HEAD"],
+                           capture_output=True, text=True, timeout=10)
+        return r.stdout.strip() or "unknown"
+    except (OSError, subprocess.SubprocessError):
+        return "unknown"
 
 
 def _compile(src: Path, flags: list[str], verbose: bool) -> Path:
@@ -83,7 +93,8 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     drv = [CSRC / d for d in DRIVER if (CSRC / d).exists()]
     if drv:
-        dobjs = [_compile(d, EXACT, verbose) for d in drv]
+        dflags = EXACT + [f'-DSIMPLE_GIT_HASH="{git_hash()}"', '-DSIMPLE_COMPILER="nvcc 12.9 (sm_100a)"']
+        dobjs = [_compile(d, dflags, verbose) for d in drv]
         if not EXE.exists() or EXE.stat().st_mtime < max(o.stat().st_mtime for o in dobjs + [LIB]):
             cmd = [nvcc(), *ARCH, *map(str, dobjs), "-o", str(EXE), f"-L{HERE}", "-lsgpu",
                    "-Xlinker", "-rpath,$ORIGIN"]

@@ -1,0 +1,130 @@
+// driver.cpp — `simple <config>`: the reference's command-line entry point for backend = gpu.
+//
+// Same behaviour as simple-hpc's main (src/main.cpp:18-89) on its GPU branch: parse the config
+// (same keys and errors), print the parameters (print_params, src/params.cpp:182-214), print the
+// device, run the outer loop with the reference's stopping rule and its "iter k ..." lines, write
+// the reference's output files, print "converged|not converged after N iterations in T s", and on
+// any error print "error (rank 0): <message>" to stderr and exit 1. The solver is reached only
+// through the C ABI (include/sgpu.h).
+#include "../../include/sgpu.h"
+
+#include <cuda_runtime.h>
+
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#ifndef SIMPLE_GIT_HASH
+#define SIMPLE_GIT_HASH "unknown"
+#endif
+#ifndef SIMPLE_COMPILER
+#define SIMPLE_COMPILER "nvcc"
+#endif
+
+namespace {
+
+void check(int rc) {
+    if (rc != SGPU_OK) throw std::runtime_error(sgpu_last_error());
+}
+
+const char* conv_name(int c) { return c == SGPU_UDS ? "UDS" : "QUICK"; }
+const char* backend_name(int b) {
+    return b == SGPU_BACKEND_SERIAL ? "serial" : b == SGPU_BACKEND_OPENMP ? "openmp" : "gpu";
+}
+const char* mom_name(int m) {
+    return m == SGPU_MOM_GS_LEX ? "gs_lex" : m == SGPU_MOM_JACOBI ? "jacobi" : "gs_multicolour";
+}
+const char* p_name(int s) {
+    return s == SGPU_P_GS_LEX        ? "gs_lex"
+           : s == SGPU_P_JACOBI      ? "jacobi"
+           : s == SGPU_P_GS_REDBLACK ? "gs_redblack"
+           : s == SGPU_P_CG          ? "cg"
+                                     : "mg";
+}
+
+// print_params (src/params.cpp:182-214): same lines, same stream precision.
+void print_params(std::ostream& os, const sgpu_params_t& p) {
+    os << std::setprecision(10);
+    os << "NX = " << p.NX << "\nNY = " << p.NY << "\nH = " << p.H << "\n"
+       << "nrows = " << p.nrows << "\nncols = " << p.ncols << "\n"
+       << "dx = " << p.dx << "\ndy = " << p.dy << "\nRe = " << p.Re << "\nnu = " << p.nu << "\n"
+       << "maxit = " << p.maxit << "\nmaxit_inner_u = " << p.maxit_inner_u
+       << "\nmaxit_inner_v = " << p.maxit_inner_v << "\nmaxit_inner_p = " << p.maxit_inner_p
+       << "\nerror_tolerance = " << p.error_tolerance
+       << "\nrelaxation_factor_u = " << p.relaxation_factor_u
+       << "\nrelaxation_factor_v = " << p.relaxation_factor_v
+       << "\nrelaxation_factor_p = " << p.relaxation_factor_p
+       << "\nconvection_scheme = " << conv_name(p.convection_scheme)
+       << "\ndiffusion_order = " << p.diffusion_order
+       << "\nHybrid_switch = " << (p.hybrid_switch ? "True" : "False")
+       << "\nbackend = " << backend_name(p.backend) << "\nmomentum_solver = " << mom_name(p.momentum_solver)
+       << "\npressure_solver = " << p_name(p.pressure_solver) << "\nresidual_normalisation = "
+       << (p.residual_normalisation == SGPU_NORM_ABSOLUTE ? "absolute" : "running_max")
+       << "\noutput_dir = " << p.output_dir << "\npressure_tolerance = " << p.pressure_tolerance
+       << "\npressure_maxit = " << p.pressure_maxit << "\nmg_cycles = " << p.mg_cycles
+       << "\nmg_pre = " << p.mg_pre << "\nmg_post = " << p.mg_post << "\nmg_omega = " << p.mg_omega
+       << "\nhalo_overlap = " << (p.halo_overlap ? "True" : "False")
+       << "\nwrite_fields = " << (p.write_fields ? "True" : "False") << "\n";
+}
+
+struct Handle {
+    sgpu_handle* h = nullptr;
+    ~Handle() {
+        if (h) sgpu_destroy(h);
+    }
+};
+
+} // namespace
+
+extern "C" int sgpu_write_outputs(const sgpu_params_t* p, const double* u, const double* v,
+                                  const double* pf, const double* log, int iterations,
+                                  const sgpu_result_t* result, const char* cfg_path,
+                                  const char* git_hash, const char* compiler);
+
+int main(int argc, char** argv) {
+    if (argc != 2) {
+        std::cerr << "usage: simple <config>\n";
+        return 1;
+    }
+    try {
+        std::ifstream f(argv[1]);
+        if (!f) throw std::runtime_error(std::string("cannot open config file: ") + argv[1]);
+        std::stringstream ss;
+        ss << f.rdbuf();
+        sgpu_params_t p;
+        check(sgpu_params_from_config(ss.str().c_str(), &p));
+        print_params(std::cout, p);
+        if (p.backend != SGPU_BACKEND_GPU)
+            throw std::runtime_error(std::string("backend = ") + backend_name(p.backend) +
+                                     " is the reference's CPU path; this build provides backend = gpu");
+        cudaDeviceProp prop{};
+        if (cudaGetDeviceProperties(&prop, 0) != cudaSuccess)
+            throw std::runtime_error("GPU error: no CUDA device is visible");
+        std::printf("gpu: %s (sm_%d%d)\n", prop.name, prop.major, prop.minor);
+        std::fflush(stdout);
+
+        Handle h;
+        check(sgpu_create(&p, nullptr, nullptr, nullptr, &h.h));
+        check(sgpu_set_profiling(h.h, 1));
+        std::vector<double> log(4 * static_cast<std::size_t>(p.maxit > 0 ? p.maxit : 1));
+        sgpu_result_t r{};
+        check(sgpu_run(h.h, p.maxit, log.data(), 100, &r));
+        const std::size_t n = static_cast<std::size_t>(p.nrows) * p.ncols;
+        std::vector<double> u(n), v(n), pf(n);
+        check(sgpu_download(h.h, SGPU_F_U, u.data()));
+        check(sgpu_download(h.h, SGPU_F_V, v.data()));
+        check(sgpu_download(h.h, SGPU_F_P, pf.data()));
+        check(sgpu_write_outputs(&p, u.data(), v.data(), pf.data(), log.data(), r.iterations, &r,
+                                 argv[1], SIMPLE_GIT_HASH, SIMPLE_COMPILER));
+        std::cout << (r.converged ? "converged" : "not converged") << " after " << r.iterations
+                  << " iterations in " << r.seconds << " s\n";
+    } catch (const std::exception& e) {
+        std::cerr << "error (rank 0): " << e.what() << "\n";
+        return 1;
+    }
+    return 0;
+}

@@ -10,13 +10,14 @@
 //    owns a strip of columns plus a halo and walks it top to bottom; cell (r, j) of colour c is
 //    updated at step t = r + 2c. Every stencil neighbour of a cell is updated at least two steps
 //    before it (if its colour comes first) or two steps after it (if later), so the update order
-//    of each cell relative to its neighbours is exactly the reference's colour order and one
-//    barrier per step suffices. Rows stream through a shared-memory ring filled by cp.async; halo
-//    cells are updated redundantly and only the owned block is written, to a second buffer.
+//    of each cell relative to its neighbours is exactly the reference's colour order. Rows stream
+//    through a shared-memory ring filled by cp.async; halo cells are updated redundantly and only
+//    the owned block is written, to a second buffer.
 // Pressure assembly (assemble_p, pressure.cpp:14-54) is one kernel with the wall zeros folded in.
 #include "kernels.hpp"
 #include "stencil.cuh"
 
+#include <algorithm>
 #include <climits>
 
 namespace sgpu {
@@ -72,8 +73,8 @@ __global__ void k_mom_prep(DevParams p, const double* __restrict__ x, const doub
     AP[q] = c.AP;
 }
 
-constexpr int kRing = 32; // rows held in the shared-memory ring (power of two)
-constexpr int kPrefetch = 8;
+constexpr int kRing = 32;    // rows held in the shared-memory ring (power of two)
+constexpr int kPrefetch = 8; // rows the cp.async ring runs ahead of the rows being read
 
 __device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -84,19 +85,91 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// The 9 global inputs of one cell's coefficient recomputation and pressure term, read through
+// per-thread column pointers (xF, oth, pf already offset by the thread's column) at row offset o.
+//   u cell: uF(r, j-1), uF(r, j), uF(r, j+1), v(r, j), v(r, j+1), v(r+1, j), v(r+1, j+1),
+//           p(r, j), p(r, j+1)
+//   v cell: u(r-1, j), u(r, j), u(r, j-1), u(r-1, j-1), vF(r, j), vF(r-1, j), vF(r+1, j),
+//           p(r, j), p(r-1, j)
+template <bool V>
+__device__ __forceinline__ void load_inputs(const double* __restrict__ xF,
+                                            const double* __restrict__ oth,
+                                            const double* __restrict__ pf, int o, int ld,
+                                            double a[9]) {
+    if (!V) {
+        const double* f = xF + o;
+        const double* g = oth + o;
+        const double* h = pf + o;
+        a[0] = __ldg(f - 1); a[1] = __ldg(f); a[2] = __ldg(f + 1);
+        a[3] = __ldg(g); a[4] = __ldg(g + 1); a[5] = __ldg(g + ld); a[6] = __ldg(g + ld + 1);
+        a[7] = __ldg(h); a[8] = __ldg(h + 1);
+    } else {
+        const double* f = xF + o;
+        const double* g = oth + o;
+        const double* h = pf + o;
+        a[0] = __ldg(g - ld); a[1] = __ldg(g); a[2] = __ldg(g - 1); a[3] = __ldg(g - ld - 1);
+        a[4] = __ldg(f); a[5] = __ldg(f - ld); a[6] = __ldg(f + ld);
+        a[7] = __ldg(h); a[8] = __ldg(h - ld);
+    }
+}
+
+// The 9 coefficients of a momentum cell from its face velocities: convective_coefficients
+// (coefficients.cpp:15-39) plus the precomputed diffusive ones (:41-63), specialised on the scheme
+// and the diffusion order; band cells take the UDS / 2nd-order branch like the reference.
+template <bool QUICK, int ORDER>
+__device__ __forceinline__ Coef9 coef_spec(const DevParams& p, double ue, double uw, double vn,
+                                           double vs, bool band) {
+    const double dx = p.dx, dy = p.dy;
+    double AE, AW, AN, AS, AEE, AWW, ANN, ASS;
+    if (!QUICK || band) {
+        AE = dy * mx0(-ue);
+        AW = dy * mx0(uw);
+        AN = dx * mx0(-vn);
+        AS = dx * mx0(vs);
+        AEE = AWW = ANN = ASS = 0.0;
+    } else {
+        AE = -dy * (-0.75 * mx0(-ue) + 0.375 * mx0(ue) - 0.125 * mx0(-uw));
+        AW = -dy * (-0.125 * mx0(ue) + 0.375 * mx0(-uw) - 0.75 * mx0(uw));
+        AN = -dx * (-0.75 * mx0(-vn) + 0.375 * mx0(vn) - 0.125 * mx0(-vs));
+        AS = -dx * (-0.125 * mx0(vn) + 0.375 * mx0(-vn) - 0.75 * mx0(vs));
+        AEE = -0.125 * dy * mx0(-ue);
+        AWW = -0.125 * dy * mx0(uw);
+        ANN = -0.125 * dx * mx0(-vn);
+        ASS = -0.125 * dx * mx0(vs);
+    }
+    const double APc = AS + AW + AN + AE + ASS + AWW + ANN + AEE;
+    const bool d2 = ORDER == 2 || band;
+    Coef9 c;
+    c.AE = AE + (d2 ? p.dband[0] : p.dint[0]);
+    c.AW = AW + (d2 ? p.dband[1] : p.dint[1]);
+    c.AN = AN + (d2 ? p.dband[2] : p.dint[2]);
+    c.AS = AS + (d2 ? p.dband[3] : p.dint[3]);
+    c.AEE = AEE + (d2 ? p.dband[4] : p.dint[4]);
+    c.AWW = AWW + (d2 ? p.dband[5] : p.dint[5]);
+    c.ANN = ANN + (d2 ? p.dband[6] : p.dint[6]);
+    c.ASS = ASS + (d2 ? p.dband[7] : p.dint[7]);
+    c.AP = APc + (d2 ? p.dband[8] : p.dint[8]);
+    return c;
+}
+
 // One multicolour sweep of u (V = false) or v (V = true) from xin to xout. NT threads per CTA, one
 // column each; the CTA owns W = NT - 4 * NCOL columns starting at blockIdx.x * W and rows
-// [blockIdx.y * seg_rows, + seg_rows).
-template <int NCOL, bool V, int NT>
+// [blockIdx.y * seg_rows, + seg_rows). For five colours every dependency between two updates is at
+// least two steps apart, so two steps run between barriers (SPB = 2). Each super-step prefetches
+// the next one's coefficient inputs into registers (two register sets, alternating), so their
+// latency overlaps the current updates.
+template <int NCOL, bool V, int NT, bool QUICK, int ORDER>
 __global__ void __launch_bounds__(NT, 2)
     k_mom_stream(DevParams p, const double* __restrict__ xin, double* __restrict__ xout,
                  const double* __restrict__ xF, const double* __restrict__ oth,
                  const double* __restrict__ pf, int seg_rows) {
-    static_assert(kPrefetch <= kRing - 2 * NCOL - 4, "ring too small for the prefetch distance");
-    extern __shared__ double ring_mem[];
-    double(*ring)[NT] = reinterpret_cast<double(*)[NT]>(ring_mem); // kRing rows of NT columns
-    constexpr int HC = 2 * NCOL; // halo: a sweep's dependency reach (2 cells per colour)
+    constexpr int SPB = NCOL == 5 ? 2 : 1;       // steps per barrier
+    constexpr int HC = 2 * NCOL;                 // halo: a sweep's dependency reach
     constexpr int W = NT - 2 * HC;
+    constexpr int A = kPrefetch + SPB + 2;       // rows issued ahead of the first super-step
+    static_assert(kPrefetch + 2 * SPB + 1 < kRing - 2 * NCOL, "ring too small for the prefetch");
+    extern __shared__ double ring_mem[];
+    __shared__ int s_rmin[NCOL], s_rmax[NCOL];
     const int tid = threadIdx.x;
     const int j0 = blockIdx.x * W;
     const int C0 = j0 - HC, C1 = j0 + W + HC; // loaded columns [C0, C1)
@@ -104,56 +177,135 @@ __global__ void __launch_bounds__(NT, 2)
     const int R0 = blockIdx.y * seg_rows;
     const int R1 = min(R0 + seg_rows, p.nrows);
     const int L0 = max(R0 - HC, 0), L1 = min(R1 + HC, p.nrows); // loaded rows [L0, L1)
+    const int ld = p.pitch;
     const bool col_in = col >= 0 && col < p.ncols;
     const bool col_out = col_in && col >= j0 && col < j0 + W;
     const int H = p.H;
-    const int iu0 = V ? H + 1 : H, iu1 = p.NX + H - 1;
-    const int ju0 = H + 1, ju1 = V ? p.NY + H : p.NY + H - 1;
-    const bool cut_top = L0 > 0, cut_bot = L1 < p.nrows, cut_left = C0 > 0, cut_right = C1 < p.ncols;
-    const std::size_t ld = p.pitch;
+    // Per colour: the rows a cell of that colour may be updated at (the update range clipped to
+    // the window's dependency cone; only cut sides constrain).
+    if (tid < NCOL) {
+        const int c = tid;
+        int lo = V ? H + 1 : H, hi = p.NX + H - 1;
+        if (L0 > 0) lo = max(lo, L0 + 2 + 2 * c);
+        if (L1 < p.nrows) hi = min(hi, L1 - 3 - 2 * c);
+        s_rmin[c] = lo;
+        s_rmax[c] = hi;
+    }
+    // Colours for which this column is updatable (update range and cut columns).
+    unsigned colmask = 0;
+    {
+        const int ju0 = H + 1, ju1 = V ? p.NY + H : p.NY + H - 1;
+#pragma unroll
+        for (int c = 0; c < NCOL; ++c) {
+            bool ok = col >= ju0 && col <= ju1;
+            if (C0 > 0) ok = ok && col >= C0 + 2 + 2 * c;
+            if (C1 < p.ncols) ok = ok && col <= C1 - 3 - 2 * c;
+            colmask |= (ok ? 1u : 0u) << c;
+        }
+    }
+    // Band tests need global indices: in_boundary_band (coefficients.cpp:10-13).
+    const bool col_band = col == p.Hy + 1 || col == p.NY + p.Hy;
     const double relax = V ? p.av : p.au;
+    const double omr = 1 - relax;
+    const double* xFc = xF + col;
+    const double* othc = oth + col;
+    const double* pfc = pf + col;
+    double* ringc = ring_mem + tid; // column tid of ring row k at ringc[k * NT]
+    const double* xinc = xin + col;
 
     int next = L0;
     auto issue = [&]() {
-        if (next < L1 && col_in) cp_async8(&ring[next & (kRing - 1)][tid], xin + ix(p, next, col));
+        if (next < L1 && col_in) cp_async8(ringc + (next & (kRing - 1)) * NT, xinc + next * ld);
         cp_async_commit();
         ++next;
     };
-    for (int k = 0; k < kPrefetch + 3; ++k) issue(); // rows L0 .. L0 + 2 + kPrefetch
-
-    const int t_last = R1 + 2 * NCOL - 2; // the step that writes back row R1 - 1
-    for (int t = L0; t <= t_last; ++t) {
-        cp_async_wait<kPrefetch>(); // row t + 2 has landed (this thread's copies)
-        __syncthreads();            // ... everyone's, and step t - 1's updates are visible
-        issue();                    // row t + 3 + kPrefetch into the slot of a row no longer read
-
-        // The one cell of this column updated at step t: colour c at row t - 2c.
-        const int c = NCOL == 5 ? (2 * t + col + 1000) % 5 : (t + col + 1000) & 1;
-        const int r = t - 2 * c;
-        bool ok = r >= iu0 && r <= iu1 && col >= ju0 && col <= ju1;
-        ok = ok && (!cut_top || r >= L0 + 2 + 2 * c) && (!cut_bot || r <= L1 - 3 - 2 * c);
-        ok = ok && (!cut_left || col >= C0 + 2 + 2 * c) && (!cut_right || col <= C1 - 3 - 2 * c);
-        if (ok) {
-            const Coef9 k = V ? coef_v(p, oth, xF, r, col) : coef_u(p, xF, oth, r, col);
-            const double* rc = ring[r & (kRing - 1)];
-            const double xe = rc[tid + 1], xw = rc[tid - 1];
-            const double xn = ring[(r - 1) & (kRing - 1)][tid], xs = ring[(r + 1) & (kRing - 1)][tid];
-            // near_sum for two colours (momentum_u.cpp:84-87), nb_sum for five (:36-41).
-            double nb = k.AE * xe + k.AW * xw + k.AN * xn + k.AS * xs;
-            if (NCOL == 5) {
-                const double xee = rc[tid + 2], xww = rc[tid - 2];
-                const double xnn = ring[(r - 2) & (kRing - 1)][tid];
-                const double xss = ring[(r + 2) & (kRing - 1)][tid];
-                nb = nb + (k.AEE * xee + k.AWW * xww + k.ANN * xnn + k.ASS * xss);
-            }
-            const std::size_t q = ix(p, r, col);
-            const double pt = V ? (pf[q] - pf[q - ld]) * p.dx : (pf[q] - pf[q + 1]) * p.dy;
-            const double xo = rc[tid];
-            ring[r & (kRing - 1)][tid] = relax * (nb + pt) / k.AP + (1 - relax) * xo;
+    // Colour of the cell this column updates at step t: (2t + col) mod 5, or (t + col) mod 2.
+    auto colour_at = [&](int t) {
+        return NCOL == 5 ? (2 * t + col + 1000) % 5 : (t + col + 1000) & 1;
+    };
+    auto step_cell = [&](int c, int t, int& r) -> bool {
+        r = t - 2 * c;
+        return ((colmask >> c) & 1u) && r >= s_rmin[c] && r <= s_rmax[c];
+    };
+    auto update = [&](int r, const double a[9]) {
+        double ue, uw, vn, vs, pt;
+        if (!V) {
+            ue = (a[1] + a[2]) / 2;
+            uw = (a[1] + a[0]) / 2;
+            vn = (a[3] + a[4]) / 2;
+            vs = (a[5] + a[6]) / 2;
+            pt = (a[7] - a[8]) * p.dy;
+        } else {
+            ue = (a[0] + a[1]) / 2;
+            uw = (a[2] + a[3]) / 2;
+            vn = (a[4] + a[5]) / 2;
+            vs = (a[4] + a[6]) / 2;
+            pt = (a[7] - a[8]) * p.dx;
         }
-        // Row t - (2 NCOL - 1) had its last update at step t - 1: write the owned part back.
-        const int rw = t - (2 * NCOL - 1);
-        if (rw >= R0 && rw < R1 && col_out) xout[ix(p, rw, col)] = ring[rw & (kRing - 1)][tid];
+        const bool band = col_band || r == p.NX + p.Hx - 1 || r == p.Hx;
+        const Coef9 k = coef_spec<QUICK, ORDER>(p, ue, uw, vn, vs, band);
+        double* rc = ringc + (r & (kRing - 1)) * NT;
+        const double xe = rc[1], xw = rc[-1];
+        const double xn = ringc[((r - 1) & (kRing - 1)) * NT];
+        const double xs = ringc[((r + 1) & (kRing - 1)) * NT];
+        // near_sum for two colours (momentum_u.cpp:84-87), nb_sum for five (:36-41).
+        double nb = k.AE * xe + k.AW * xw + k.AN * xn + k.AS * xs;
+        if (NCOL == 5) {
+            const double xee = rc[2], xww = rc[-2];
+            const double xnn = ringc[((r - 2) & (kRing - 1)) * NT];
+            const double xss = ringc[((r + 2) & (kRing - 1)) * NT];
+            nb = nb + (k.AEE * xee + k.AWW * xww + k.ANN * xnn + k.ASS * xss);
+        }
+        const double xo = rc[0];
+        rc[0] = relax * (nb + pt) / k.AP + omr * xo;
+    };
+
+    for (int k = 0; k < A; ++k) issue(); // rows L0 .. L0 + A - 1
+    __syncthreads();                     // s_rmin / s_rmax
+
+    // One super-step starting at step t: cells with inputs `cur`; prefetch step t + SPB's into nxt.
+    int cA = colour_at(L0);
+    double bufA[SPB][9], bufB[SPB][9];
+    int rA[SPB], rB[SPB];
+    bool okA[SPB], okB[SPB];
+#pragma unroll
+    for (int s = 0; s < SPB; ++s) {
+        const int c = NCOL == 5 ? (cA + 2 * s) % 5 : (cA + s) & 1;
+        okA[s] = step_cell(c, L0 + s, rA[s]);
+        if (okA[s]) load_inputs<V>(xFc, othc, pfc, rA[s] * ld, ld, bufA[s]);
+    }
+    auto super_step = [&](int t, int c0, double (&cur)[SPB][9], const int (&rcur)[SPB],
+                          const bool (&okcur)[SPB], double (&nxt)[SPB][9], int (&rnxt)[SPB],
+                          bool (&oknxt)[SPB]) {
+        cp_async_wait<kPrefetch>(); // rows <= t + SPB + 1 have landed (this thread's copies)
+        __syncthreads();            // ... everyone's, and the previous super-step's updates
+#pragma unroll
+        for (int s = 0; s < SPB; ++s) issue();
+        const int cn = NCOL == 5 ? (c0 + 2 * SPB) % 5 : (c0 + SPB) & 1; // colour at t + SPB
+#pragma unroll
+        for (int s = 0; s < SPB; ++s) {
+            const int c = NCOL == 5 ? (cn + 2 * s) % 5 : (cn + s) & 1;
+            oknxt[s] = step_cell(c, t + SPB + s, rnxt[s]);
+            if (oknxt[s]) load_inputs<V>(xFc, othc, pfc, rnxt[s] * ld, ld, nxt[s]);
+        }
+#pragma unroll
+        for (int s = 0; s < SPB; ++s)
+            if (okcur[s]) update(rcur[s], cur[s]);
+        // Rows whose last update was in an earlier super-step: write the owned part back.
+#pragma unroll
+        for (int s = 0; s < SPB; ++s) {
+            const int rw = t - 2 * NCOL + 1 - (SPB - 1) + s;
+            if (rw >= R0 && rw < R1 && col_out) xout[col + rw * ld] = ringc[(rw & (kRing - 1)) * NT];
+        }
+        return cn;
+    };
+
+    // Row R1 - 1 is written back by the super-step starting at R1 + 2 NCOL - 2 or one later.
+    const int t_last = R1 + 2 * NCOL - 2 + (SPB - 1);
+    int c0 = cA;
+    for (int t = L0; t <= t_last; t += 2 * SPB) {
+        c0 = super_step(t, c0, bufA, rA, okA, bufB, rB, okB);
+        if (t + SPB <= t_last) c0 = super_step(t + SPB, c0, bufB, rB, okB, bufA, rA, okA);
     }
     cp_async_wait<0>();
 }
@@ -197,7 +349,7 @@ void prep_ranges(const DevParams& p, Range& ur, Range& cr) {
     }
 }
 
-template <int NCOL, bool V, int NT>
+template <int NCOL, bool V, int NT, bool QUICK, int ORDER>
 void launch_stream(const DevParams& p, const double* xin, double* xout, const double* xF,
                    const double* oth, const double* pf, int seg_rows, cudaStream_t st) {
     constexpr int W = NT - 4 * NCOL;
@@ -205,22 +357,31 @@ void launch_stream(const DevParams& p, const double* xin, double* xout, const do
     constexpr int smem = kRing * NT * static_cast<int>(sizeof(double));
     static bool attr_set = false; // per process; the attribute applies to every device
     if (!attr_set) {
-        SGPU_CUDA(cudaFuncSetAttribute(k_mom_stream<NCOL, V, NT>,
+        SGPU_CUDA(cudaFuncSetAttribute(k_mom_stream<NCOL, V, NT, QUICK, ORDER>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         attr_set = true;
     }
-    k_mom_stream<NCOL, V, NT><<<grid, NT, smem, st>>>(p, xin, xout, xF, oth, pf, seg_rows);
+    k_mom_stream<NCOL, V, NT, QUICK, ORDER><<<grid, NT, smem, st>>>(p, xin, xout, xF, oth, pf, seg_rows);
     SGPU_LAUNCH();
+}
+
+template <bool V>
+void launch_stream_v(const DevParams& p, const double* xin, double* xout, const double* xF,
+                     const double* oth, const double* pf, int seg_rows, cudaStream_t st) {
+    if (p.uds && p.order == 2) launch_stream<2, V, 256, false, 2>(p, xin, xout, xF, oth, pf, seg_rows, st);
+    else if (p.uds) launch_stream<5, V, 256, false, 4>(p, xin, xout, xF, oth, pf, seg_rows, st);
+    else if (p.order == 2) launch_stream<5, V, 256, true, 2>(p, xin, xout, xF, oth, pf, seg_rows, st);
+    else launch_stream<5, V, 256, true, 4>(p, xin, xout, xF, oth, pf, seg_rows, st);
 }
 
 } // namespace
 
-// Rows per CTA segment of the streaming sweep: enough segments to fill the GPU (2 CTAs per SM),
-// but never so short that the 2 * NCOL-row halo dominates.
+// Rows per CTA segment of the streaming sweep: enough segments to fill the GPU with one wave of
+// 2 CTAs per SM, but never so short that the 2 * NCOL-row halo dominates.
 int stream_seg_rows(const DevParams& p, int sms) {
     const int W = 256 - 4 * p.ncol;
     const int strips = (p.ncols + W - 1) / W;
-    const int want = (2 * sms + strips - 1) / strips;
+    const int want = std::max(1, (2 * sms) / strips);
     int seg = (p.nrows + want - 1) / want;
     const int min_seg = 8 * p.ncol;
     if (seg < min_seg) seg = min_seg;
@@ -242,13 +403,8 @@ void launch_mom_prep(const DevParams& p, bool v_component, const double* x, cons
 void launch_mom_sweep(const DevParams& p, bool v_component, const double* xin, double* xout,
                       const double* xF, const double* oth, const double* pf, int seg_rows,
                       cudaStream_t st) {
-    if (p.ncol == 5) {
-        if (v_component) launch_stream<5, true, 256>(p, xin, xout, xF, oth, pf, seg_rows, st);
-        else launch_stream<5, false, 256>(p, xin, xout, xF, oth, pf, seg_rows, st);
-    } else {
-        if (v_component) launch_stream<2, true, 256>(p, xin, xout, xF, oth, pf, seg_rows, st);
-        else launch_stream<2, false, 256>(p, xin, xout, xF, oth, pf, seg_rows, st);
-    }
+    if (v_component) launch_stream_v<true>(p, xin, xout, xF, oth, pf, seg_rows, st);
+    else launch_stream_v<false>(p, xin, xout, xF, oth, pf, seg_rows, st);
 }
 
 void launch_assemble_p_fused(const DevParams& p, const double* APU, const double* APV,

@@ -64,23 +64,32 @@ __device__ __forceinline__ bool in_cone(const Win& w, int I, int Jc, int k, int 
            (!w.cut_left || Jc >= w.C0 + 1 + k) && (!w.cut_right || Jc <= w.C0 + NT - 2 - k);
 }
 
+// The 6 per-cell inputs of a red-black update or a residual: AE, AW, AN, AS, AP, b.
+__device__ __forceinline__ void load6(const LevelView& L, int q, double a[6]) {
+    a[0] = __ldg(L.AE + q);
+    a[1] = __ldg(L.AW + q);
+    a[2] = __ldg(L.AN + q);
+    a[3] = __ldg(L.AS + q);
+    a[4] = __ldg(L.AP + q);
+    a[5] = __ldg(L.b + q);
+}
+
 // Red-black two-statement update of one cell (multigrid.cpp:61-63) on the ring.
 template <int NT>
-__device__ __forceinline__ void rb_update(const LevelView& L, double (*ring)[NT], int I, int Jc,
-                                          int tid) {
-    const int q = I * L.stride + Jc;
+__device__ __forceinline__ void rb_update(double (*ring)[NT], int I, int tid, const double a[6]) {
     double* row = ring[I & (kRing - 1)];
-    const double ap = L.AP[q];
-    double x = L.b[q] / ap;
-    x += (L.AE[q] * row[tid + 1] + L.AW[q] * row[tid - 1] + L.AS[q] * ring[(I + 1) & (kRing - 1)][tid] +
-          L.AN[q] * ring[(I - 1) & (kRing - 1)][tid]) /
-         ap;
+    double x = a[5] / a[4];
+    x += (a[0] * row[tid + 1] + a[1] * row[tid - 1] + a[3] * ring[(I + 1) & (kRing - 1)][tid] +
+          a[2] * ring[(I - 1) & (kRing - 1)][tid]) /
+         a[4];
     row[tid] = x;
 }
 
-template <int NT>
+// PRE red-black sweeps, residual and restriction in one streaming pass (see the file comment).
+// Each step prefetches the next step's coefficients into registers.
+template <int NT, int PRE>
 __global__ void __launch_bounds__(NT, 2)
-    k_mg_down(LevelView L, LevelView C, double* __restrict__ xout, int pre, int x_zero, int seg_rows,
+    k_mg_down(LevelView L, LevelView C, double* __restrict__ xout, int x_zero, int seg_rows,
               int HC) {
     extern __shared__ double smem[];
     double(*ring)[NT] = reinterpret_cast<double(*)[NT]>(smem);
@@ -102,31 +111,62 @@ __global__ void __launch_bounds__(NT, 2)
         cp_async_commit();
         ++next;
     };
+    // Cells of step t: PRE updates (rows t - 2c - 4 sw) and the residual (row t - 4 PRE).
+    constexpr int NC = PRE + 1;
+    auto cells = [&](int t, int* I, bool* ok) {
+        const int cpar = (t + Jc + 4) & 1;
+#pragma unroll
+        for (int sw = 0; sw < PRE; ++sw) {
+            I[sw] = t - 2 * cpar - 4 * sw;
+            ok[sw] = cint && I[sw] >= 0 && I[sw] < L.nx && in_cone(w, I[sw], Jc, 2 * sw + cpar, NT);
+        }
+        I[PRE] = t - 4 * PRE;
+        ok[PRE] = cint && I[PRE] >= 0 && I[PRE] < L.nx && in_cone(w, I[PRE], Jc, 2 * PRE, NT);
+    };
     for (int k = 0; k < kPD + 2; ++k) issue(); // rows L0 .. L0 + 1 + kPD
 
-    const int res_lag = 4 * pre;
-    const int t_last = w.R1 - 1 + res_lag;
+    int In[NC];
+    bool okn[NC];
+    double an[NC][6];
+    cells(w.L0, In, okn);
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+        if (okn[c]) load6(L, In[c] * s + Jc, an[c]);
+
+    const int t_last = w.R1 - 1 + 4 * PRE;
     double r_prev = 0.0;
     for (int t = w.L0; t <= t_last; ++t) {
         cp_async_wait<kPD>(); // rows <= t + 1 have landed
         __syncthreads();
         issue();
-        const int cpar = (t + Jc + 4) & 1;
-        for (int sw = 0; sw < pre; ++sw) {
-            const int I = t - 2 * cpar - 4 * sw;
-            if (cint && I >= 0 && I < L.nx && in_cone(w, I, Jc, 2 * sw + cpar, NT))
-                rb_update<NT>(L, ring, I, Jc, tid);
+        int I[NC];
+        bool ok[NC];
+        double a[NC][6];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            I[c] = In[c];
+            ok[c] = okn[c];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) a[c][m] = an[c][m];
         }
-        // Residual of row Ir = t - 4 pre: its neighbours had their last update at step <= t - 1.
-        const int Ir = t - res_lag;
+        cells(t + 1, In, okn);
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+            if (okn[c]) load6(L, In[c] * s + Jc, an[c]);
+
+#pragma unroll
+        for (int sw = 0; sw < PRE; ++sw)
+            if (ok[sw]) rb_update<NT>(ring, I[sw], tid, a[sw]);
+        // Residual of row Ir = t - 4 PRE (multigrid.cpp:84-85): its neighbours are final.
+        const int Ir = I[PRE];
         double r = 0.0;
-        if (cint && Ir >= 0 && Ir < L.nx && in_cone(w, Ir, Jc, 2 * pre, NT)) {
-            const int q = Ir * s + Jc;
+        if (ok[PRE]) {
             const double* row = ring[Ir & (kRing - 1)];
-            r = L.b[q] - (L.AP[q] * row[tid] -
-                          (L.AE[q] * row[tid + 1] + L.AW[q] * row[tid - 1] +
-                           L.AS[q] * ring[(Ir + 1) & (kRing - 1)][tid] +
-                           L.AN[q] * ring[(Ir - 1) & (kRing - 1)][tid]));
+            const double* aa = a[PRE];
+            r = aa[5] - (aa[4] * row[tid] -
+                         (aa[0] * row[tid + 1] + aa[1] * row[tid - 1] +
+                          aa[3] * ring[(Ir + 1) & (kRing - 1)][tid] +
+                          aa[2] * ring[(Ir - 1) & (kRing - 1)][tid]));
         }
         // Restriction of the row pair (Ir - 1, Ir): C.b = r[f] + r[f+1] + r[f+fs] + r[f+fs+1].
         if ((Ir & 1) && Ir >= 1) { // uniform over the CTA
@@ -140,19 +180,18 @@ __global__ void __launch_bounds__(NT, 2)
             }
         }
         r_prev = r;
-        // The smoothed iterate: row t - 4 pre + 1 had its last update at step t - 1.
-        if (pre > 0) {
-            const int rw = t - res_lag + 1;
-            if (cown && rw >= w.R0 && rw < w.R1) xout[rw * s + Jc] = ring[rw & (kRing - 1)][tid];
-        }
+        // The smoothed iterate: row t - 4 PRE + 1 had its last update at step t - 1.
+        const int rw = t - 4 * PRE + 1;
+        if (cown && rw >= w.R0 && rw < w.R1) xout[rw * s + Jc] = ring[rw & (kRing - 1)][tid];
     }
     cp_async_wait<0>();
 }
 
-template <int NT>
+// Prolongation and POST red-black sweeps in one streaming pass (see the file comment).
+template <int NT, int POST>
 __global__ void __launch_bounds__(NT, 2)
     k_mg_up(LevelView C, LevelView L, const double* __restrict__ xin, double* __restrict__ xout,
-            double omega, int post, int seg_rows, int HC) {
+            double omega, int seg_rows, int HC) {
     extern __shared__ double smem[];
     double(*ring)[NT] = reinterpret_cast<double(*)[NT]>(smem);
     const Win w = make_win<NT>(L, seg_rows, HC);
@@ -169,28 +208,69 @@ __global__ void __launch_bounds__(NT, 2)
         cp_async_commit();
         ++next;
     };
+    auto cells = [&](int t, int* I, bool* ok) {
+        const int cpar = (t + Jc + 4) & 1;
+#pragma unroll
+        for (int sw = 0; sw < POST; ++sw) {
+            I[sw] = t - 2 * cpar - 4 * sw;
+            ok[sw] = cint && I[sw] >= 0 && I[sw] < L.nx && in_cone(w, I[sw], Jc, 2 * sw + cpar, NT);
+        }
+    };
     for (int k = 0; k < kPD + 3; ++k) issue(); // rows L0 .. L0 + 2 + kPD
 
-    const int lag = 4 * post;
-    const int t_last = w.R1 - 1 + lag - 1 + 1;
-    for (int t = w.L0 - 2; t <= t_last; ++t) {
+    constexpr int NC = POST > 0 ? POST : 1;
+    int In[NC];
+    bool okn[NC];
+    double an[NC][6];
+    double cxn = 0.0; // coarse correction of the next row to prolong
+    const int t0 = w.L0 - 2;
+    if (POST > 0) {
+        cells(t0, In, okn);
+#pragma unroll
+        for (int c = 0; c < POST; ++c)
+            if (okn[c]) load6(L, In[c] * s + Jc, an[c]);
+    }
+    auto coarse_at = [&](int Ip) {
+        return (cint && Ip >= 0 && Ip < L.nx && Ip < w.L1)
+                   ? __ldg(C.x + (Ip >> 1) * C.stride + (Jc >> 1))
+                   : 0.0;
+    };
+    cxn = coarse_at(t0 + 2);
+
+    const int t_last = w.R1 - 1 + 4 * POST;
+    for (int t = t0; t <= t_last; ++t) {
         if (t >= w.L0) cp_async_wait<kPD>(); // rows <= t + 2 have landed
         else cp_async_wait<kPD + 1>();
         __syncthreads();
         if (t >= w.L0) issue();
+        int I[NC];
+        bool ok[NC];
+        double a[NC][6];
+        if (POST > 0) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                I[c] = In[c];
+                ok[c] = okn[c];
+#pragma unroll
+                for (int m = 0; m < 6; ++m) a[c][m] = an[c][m];
+            }
+            cells(t + 1, In, okn);
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+                if (okn[c]) load6(L, In[c] * s + Jc, an[c]);
+        }
+        const double cx = cxn;
+        cxn = coarse_at(t + 3);
         // Prolongation of row t + 2 (read first at step t + 1): x += omega * coarse x.
         const int Ip = t + 2;
         if (cint && Ip >= 0 && Ip < L.nx && Ip < w.L1) {
             double* cell = &ring[Ip & (kRing - 1)][tid];
-            *cell += omega * C.x[(Ip >> 1) * C.stride + (Jc >> 1)];
+            *cell += omega * cx;
         }
-        const int cpar = (t + Jc + 4) & 1;
-        for (int sw = 0; sw < post; ++sw) {
-            const int I = t - 2 * cpar - 4 * sw;
-            if (cint && I >= 0 && I < L.nx && in_cone(w, I, Jc, 2 * sw + cpar, NT))
-                rb_update<NT>(L, ring, I, Jc, tid);
-        }
-        const int rw = t - lag + 1;
+#pragma unroll
+        for (int sw = 0; sw < POST; ++sw)
+            if (ok[sw]) rb_update<NT>(ring, I[sw], tid, a[sw]);
+        const int rw = t - 4 * POST + 1;
         if (cown && rw >= w.R0 && rw < w.R1) xout[rw * s + Jc] = ring[rw & (kRing - 1)][tid];
     }
     cp_async_wait<0>();
@@ -201,7 +281,7 @@ constexpr int kNT = 256;
 int seg_for(const LevelView& L, int HC, int sms) {
     const int W = kNT - 2 * HC;
     const int strips = (L.ny + W - 1) / W;
-    const int want = (2 * sms + strips - 1) / strips;
+    const int want = (2 * sms) / strips > 0 ? (2 * sms) / strips : 1; // one wave, 2 CTAs per SM
     int seg = (L.nx + want - 1) / want;
     seg = (seg + 1) & ~1; // even: restriction pairs stay inside one CTA
     const int min_seg = 2 * HC + 8;
@@ -219,32 +299,58 @@ template <class K> void allow_smem(K kernel, bool& done) {
 
 } // namespace
 
-bool mg_fast_supported(int pre, int post) { return pre >= 0 && pre <= 4 && post >= 0 && post <= 4; }
+bool mg_fast_supported(int pre, int post) { return pre >= 1 && pre <= 4 && post >= 0 && post <= 4; }
 
-void launch_mg_down(const LevelView& F, const LevelView& C, double* xout, int pre, bool x_zero,
-                    int sms, cudaStream_t st) {
-    const int HC = 2 * pre + 2;
+namespace {
+template <int PRE>
+void down_t(const LevelView& F, const LevelView& C, double* xout, bool x_zero, int sms,
+            cudaStream_t st) {
+    const int HC = 2 * PRE + 2;
     const int seg = seg_for(F, HC, sms);
     const int W = kNT - 2 * HC;
     const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
     static bool attr = false;
-    allow_smem(k_mg_down<kNT>, attr);
-    k_mg_down<kNT><<<grid, kNT, kRing * kNT * sizeof(double), st>>>(F, C, xout, pre, x_zero ? 1 : 0,
-                                                                   seg, HC);
+    allow_smem(k_mg_down<kNT, PRE>, attr);
+    k_mg_down<kNT, PRE><<<grid, kNT, kRing * kNT * sizeof(double), st>>>(F, C, xout, x_zero ? 1 : 0,
+                                                                        seg, HC);
     SGPU_LAUNCH();
+}
+template <int POST>
+void up_t(const LevelView& C, const LevelView& F, const double* xin, double* xout, double omega,
+          int sms, cudaStream_t st) {
+    const int HC = 2 * POST + 2;
+    const int seg = seg_for(F, HC, sms);
+    const int W = kNT - 2 * HC;
+    const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
+    static bool attr = false;
+    allow_smem(k_mg_up<kNT, POST>, attr);
+    k_mg_up<kNT, POST><<<grid, kNT, kRing * kNT * sizeof(double), st>>>(C, F, xin, xout, omega, seg,
+                                                                       HC);
+    SGPU_LAUNCH();
+}
+} // namespace
+
+void launch_mg_down(const LevelView& F, const LevelView& C, double* xout, int pre, bool x_zero,
+                    int sms, cudaStream_t st) {
+    switch (pre) {
+    case 1: down_t<1>(F, C, xout, x_zero, sms, st); break;
+    case 2: down_t<2>(F, C, xout, x_zero, sms, st); break;
+    case 3: down_t<3>(F, C, xout, x_zero, sms, st); break;
+    case 4: down_t<4>(F, C, xout, x_zero, sms, st); break;
+    default: throw Error(SGPU_E_INVALID, "streaming multigrid supports mg_pre 1..4");
+    }
 }
 
 void launch_mg_up(const LevelView& C, const LevelView& F, const double* xin, double* xout,
                   double omega, int post, int sms, cudaStream_t st) {
-    const int HC = 2 * post + 2;
-    const int seg = seg_for(F, HC, sms);
-    const int W = kNT - 2 * HC;
-    const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
-    static bool attr = false;
-    allow_smem(k_mg_up<kNT>, attr);
-    k_mg_up<kNT><<<grid, kNT, kRing * kNT * sizeof(double), st>>>(C, F, xin, xout, omega, post, seg,
-                                                                 HC);
-    SGPU_LAUNCH();
+    switch (post) {
+    case 0: up_t<0>(C, F, xin, xout, omega, sms, st); break;
+    case 1: up_t<1>(C, F, xin, xout, omega, sms, st); break;
+    case 2: up_t<2>(C, F, xin, xout, omega, sms, st); break;
+    case 3: up_t<3>(C, F, xin, xout, omega, sms, st); break;
+    case 4: up_t<4>(C, F, xin, xout, omega, sms, st); break;
+    default: throw Error(SGPU_E_INVALID, "streaming multigrid supports mg_post 0..4");
+    }
 }
 
 } // namespace sgpu

@@ -3,71 +3,95 @@
 // The reference sums a per-cell quantity by adding each row left to right from 0.0 and then the
 // row sums top to bottom from 0.0 (CellSums::sum and add_rows, src/decomp.cpp:176-205; det_sum,
 // src/multigrid.cpp:18-34). Floating-point addition is not associative, so the same bits need the
-// same chain: one dependent chain per row, then one chain over the rows. This file runs the row
-// chains in parallel (one thread per row) over tiles staged through shared memory, so the global
-// reads stay coalesced, and the last CTA to finish adds the row sums in order.
+// same chain: one dependent chain per row, then one chain over the rows.
+//
+// One lane per row: a warp owns 32 rows and streams them through a ring of 32 x 32 tiles in shared
+// memory, filled by cp.async many tiles ahead; each lane then adds its row's 32 values of a tile in
+// column order. A tile costs a lane 32 shared loads and 32 adds for 32 rows' worth of data, so the
+// kernel is bound by the memory stream and the add latency, not by instruction issue. The last CTA
+// to finish adds the row sums in row order.
 #include "kernels.hpp"
 
 namespace sgpu {
 
 namespace {
 
-constexpr int kTileRows = 32; // rows per CTA (one summing lane each)
-constexpr int kTileCols = 32; // columns per staged chunk
-constexpr int kLoadWarps = 8;
+constexpr int kTile = 32;   // columns per tile (and rows per warp)
+constexpr int kStages = 12; // tiles in flight per warp
+constexpr int kPitch = kTile + 1; // padded tile row: lanes reading one column hit distinct banks
 
-__global__ void __launch_bounds__(32 * kLoadWarps)
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// One warp per CTA (32 rows); the grid covers ceil(nr / 32) x K planes.
+__global__ void __launch_bounds__(32)
     k_ordered_sum(const double* __restrict__ vals, std::size_t plane_stride, int ld, int nr, int nc,
                   double* __restrict__ rows, unsigned int* counter, double* __restrict__ out,
                   const int* skip) {
     if (skip && *skip) return;
-    __shared__ double tile[2][kTileRows][kTileCols + 1];
+    extern __shared__ double tile_mem[];
+    double(*tile)[kTile][kPitch] = reinterpret_cast<double(*)[kTile][kPitch]>(tile_mem);
     __shared__ bool last_block;
     const int m = blockIdx.y;
-    const double* src = vals + m * plane_stride;
-    const int r0 = blockIdx.x * kTileRows;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int nchunks = (nc + kTileCols - 1) / kTileCols;
+    const int lane = threadIdx.x;
+    const int r0 = blockIdx.x * kTile;
+    const int nrow = min(kTile, nr - r0);
+    const double* src = vals + m * plane_stride + static_cast<std::size_t>(r0) * ld;
+    const int ntiles = (nc + kTile - 1) / kTile;
 
-    auto load = [&](int chunk, int buf) {
-        const int c = chunk * kTileCols + tx;
-        for (int rr = ty; rr < kTileRows; rr += kLoadWarps) {
-            const int r = r0 + rr;
-            tile[buf][rr][tx] = (r < nr && c < nc) ? src[static_cast<std::size_t>(r) * ld + c] : 0.0;
+    // Tile k: rows r0 .. r0 + 31, columns 32k .. 32k + 31; lane = column while loading.
+    auto issue = [&](int k) {
+        if (k < ntiles) {
+            const int c = k * kTile + lane;
+            if (c < nc)
+                for (int rr = 0; rr < nrow; ++rr)
+                    cp_async8(&tile[k % kStages][rr][lane], src + static_cast<std::size_t>(rr) * ld + c);
         }
+        cp_async_commit();
     };
+    for (int k = 0; k < kStages - 1; ++k) issue(k);
 
-    double acc = 0.0;
-    if (nchunks > 0) load(0, 0);
-    __syncthreads();
-    for (int k = 0; k < nchunks; ++k) {
-        const int buf = k & 1;
-        if (k + 1 < nchunks) load(k + 1, buf ^ 1);
-        if (ty == 0) {
-            const int cmax = min(kTileCols, nc - k * kTileCols);
-            for (int c = 0; c < cmax; ++c) acc += tile[buf][tx][c];
+    double s = 0.0; // this lane's row: r0 + lane
+    for (int k = 0; k < ntiles; ++k) {
+        issue(k + kStages - 1);
+        cp_async_wait<kStages - 1>(); // tile k has landed (this lane's copies)
+        __syncwarp();                 // ... and everyone's
+        const int cnt = min(kTile, nc - k * kTile);
+        const double* t = tile[k % kStages][lane];
+        if (cnt == kTile) {
+#pragma unroll
+            for (int c = 0; c < kTile; ++c) s += t[c];
+        } else {
+            for (int c = 0; c < cnt; ++c) s += t[c];
         }
-        __syncthreads();
+        __syncwarp(); // the slot is refilled by the next issue
     }
-    if (ty == 0 && r0 + tx < nr) rows[static_cast<std::size_t>(m) * nr + r0 + tx] = acc;
+    cp_async_wait<0>();
+    if (lane < nrow) rows[static_cast<std::size_t>(m) * nr + r0 + lane] = s;
 
     // The last CTA to finish adds every plane's row sums in row order.
     __threadfence();
-    __syncthreads();
-    if (tx == 0 && ty == 0) {
+    __syncwarp();
+    if (lane == 0) {
         const unsigned int total = gridDim.x * gridDim.y;
         last_block = (atomicAdd(counter, 1u) == total - 1);
     }
-    __syncthreads();
+    __syncwarp();
     if (!last_block) return;
     __threadfence();
-    if (ty == 0 && tx < static_cast<int>(gridDim.y)) {
-        const double* rs = rows + static_cast<std::size_t>(tx) * nr;
-        double s = 0.0;
-        for (int r = 0; r < nr; ++r) s += __ldcg(rs + r); // L2: written by other CTAs
-        out[tx] = s;
+    if (lane < static_cast<int>(gridDim.y)) {
+        const double* rs = rows + static_cast<std::size_t>(lane) * nr;
+        double acc = 0.0;
+        for (int k = 0; k < nr; ++k) acc += __ldcg(rs + k); // L2: written by other CTAs
+        out[lane] = acc;
     }
-    if (tx == 0 && ty == 0) *counter = 0u; // ready for the next launch on this stream
+    if (lane == 0) *counter = 0u; // ready for the next launch on this stream
 }
 
 } // namespace
@@ -80,9 +104,14 @@ void launch_ordered_sum(const double* vals, std::size_t plane_stride, int ld, in
         SGPU_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * K, st));
         return;
     }
-    const dim3 grid((nr + kTileRows - 1) / kTileRows, K);
-    k_ordered_sum<<<grid, dim3(32, kLoadWarps), 0, st>>>(vals, plane_stride, ld, nr, nc, s.rows,
-                                                         s.counter, out, skip);
+    const dim3 grid((nr + kTile - 1) / kTile, K);
+    constexpr int smem = kStages * kTile * kPitch * static_cast<int>(sizeof(double));
+    static bool attr = false; // per process
+    if (!attr) {
+        SGPU_CUDA(cudaFuncSetAttribute(k_ordered_sum, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        attr = true;
+    }
+    k_ordered_sum<<<grid, 32, smem, st>>>(vals, plane_stride, ld, nr, nc, s.rows, s.counter, out, skip);
     SGPU_LAUNCH();
 }
 

@@ -743,8 +743,19 @@ int sgpu_run(sgpu_handle* h, int maxit, double* log, int print_every, sgpu_resul
             s.iteration_enqueue(s.res_dev);
             SGPU_CUDA(cudaMemcpyAsync(s.host_res, s.res_dev, 3 * sizeof(double),
                                       cudaMemcpyDeviceToHost, s.st));
+            if (s.cgs)  // CG iterations of this outer iteration (CGWork::last_iterations)
+                SGPU_CUDA(cudaMemcpyAsync(s.host_res + 4, &s.cgs->k, sizeof(int),
+                                          cudaMemcpyDeviceToHost, s.st));
             s.sync();
             s.collect_phases(out.phase_seconds);
+            if (s.cgs) {
+                int k = 0;
+                std::memcpy(&k, s.host_res + 4, sizeof k);
+                out.cg_iterations += k;
+                s.cg_stats_pending = false;
+                s.last_cg_iterations = k;
+            }
+            if (s.prm.pressure_solver == SGPU_P_MG) out.mg_vcycles += s.prm.mg_cycles;
             const double ru = s.host_res[0], rv = s.host_res[1], rp = s.host_res[2];
             if (log) {
                 log[4 * (iter - 1) + 0] = iter;

@@ -111,6 +111,8 @@ def lib() -> C.CDLL:
             "sgpu_ordered_sum": (I, [D, I, I, D]),
             "sgpu_set_profiling": (I, [H, I]), "sgpu_phase_seconds": (I, [H, D]),
             "sgpu_stream": (I, [H, C.POINTER(C.c_void_p)]), "sgpu_launch_count": (C.c_longlong, []),
+            "sgpu_write_outputs": (I, [P, D, D, D, D, I, C.POINTER(Result), C.c_char_p, C.c_char_p,
+                                       C.c_char_p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -151,6 +153,20 @@ def mg_levels(nx: int, ny: int) -> list[tuple[int, int]]:
     dims = (C.c_int * 128)()
     _check(lib().sgpu_mg_levels(nx, ny, C.byref(n), dims))
     return [(dims[2 * k], dims[2 * k + 1]) for k in range(n.value)]
+
+
+def write_outputs(p: Params, u: np.ndarray, v: np.ndarray, pf: np.ndarray, log: np.ndarray,
+                  result: Result | None = None, cfg_path: str = "", git_hash: str = "unknown",
+                  compiler: str = "unknown") -> None:
+    """The reference's output files from host arrays (write_outputs, src/io.cpp:43-151)."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, pf)]
+    lg = np.ascontiguousarray(log, dtype=np.float64).reshape(-1, 4)
+    if result is None:
+        result = Result()
+        result.iterations = lg.shape[0]
+    _check(lib().sgpu_write_outputs(C.byref(p), *(_dptr(a) for a in arrs), _dptr(lg), lg.shape[0],
+                                    C.byref(result), cfg_path.encode(), git_hash.encode(),
+                                    compiler.encode()))
 
 
 def launch_count() -> int:

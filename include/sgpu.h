@@ -200,6 +200,18 @@ int sgpu_last_solve_stats(sgpu_handle* h, int* cg_iterations, int* mg_vcycles,
  */
 int sgpu_ordered_sum(const double* values, int nrows_v, int ncols_v, double* out);
 
+/*
+ * The same ordered sum for callers that cannot allocate device memory (no counterpart in the
+ * reference). values and out are DEVICE pointers: nrows_v rows of ncols_v doubles, row k starting
+ * at values + k * ld; *out receives the sum. stream is a cudaStream_t (NULL = legacy default). The
+ * call allocates nothing: its scratch is a fixed array inside the library (16384 rows at most;
+ * larger blocks are refused with SGPU_E_INVALID), fetched per device by the first call made on that
+ * device, which should come before any stream capture. The call is asynchronous on stream; calls
+ * that overlap on the GPU (other streams, other host threads) share that scratch and race, so
+ * serialise them.
+ */
+int sgpu_ordered_sum_noalloc(const double* values, int nrows_v, int ncols_v, int ld, double* out,
+                             void* stream);
 
 /*
  * Instrumentation. With profiling on, every outer iteration records CUDA events between its phases

@@ -40,6 +40,7 @@ SOURCES = {
     "fused.cu": EXACT,
     "mg_fast.cu": EXACT,
     "io.cpp": EXACT,
+    "noalloc.cu": EXACT,
 }
 DRIVER = ["driver.cpp"]
 

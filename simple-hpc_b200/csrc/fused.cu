@@ -75,6 +75,10 @@ __global__ void k_mom_prep(DevParams p, const double* __restrict__ x, const doub
 
 constexpr int kRing = 32;    // rows held in the shared-memory ring (power of two)
 constexpr int kPrefetch = 8; // rows the cp.async ring runs ahead of the rows being read
+#ifndef SGPU_STREAM_PF
+#define SGPU_STREAM_PF 0
+#endif
+constexpr int kStreamPF = SGPU_STREAM_PF; // input staging of k_mom_stream (see the kernel)
 
 __device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -113,53 +117,88 @@ __device__ __forceinline__ void load_inputs(const double* __restrict__ xF,
     }
 }
 
+// max(0, a) for the coefficient recomputation. The reference's std::max(0.0, a) returns +0.0 for
+// a = -0.0, where fmax may return either zero; the sign of that zero never reaches a coefficient,
+// because every coefficient adds its diffusive part, which is non-zero or +0.0, to the convective
+// part last (coefficients.cpp:5-8), and x + d == x' + d for the two zeros x, x'. NaN gives 0.0 in
+// both forms.
+__device__ __forceinline__ double mxf(double a) { return fmax(a, 0.0); }
+
 // The 9 coefficients of a momentum cell from its face velocities: convective_coefficients
 // (coefficients.cpp:15-39) plus the precomputed diffusive ones (:41-63), specialised on the scheme
-// and the diffusion order; band cells take the UDS / 2nd-order branch like the reference.
+// and the diffusion order. Band cells (rare: two rows and two columns) take the UDS / 2nd-order
+// branch like the reference; warp_has_band (the same for the whole warp) keeps every other warp
+// off that path.
 template <bool QUICK, int ORDER>
 __device__ __forceinline__ Coef9 coef_spec(const DevParams& p, double ue, double uw, double vn,
-                                           double vs, bool band) {
+                                           double vs, bool band, bool warp_has_band) {
     const double dx = p.dx, dy = p.dy;
-    double AE, AW, AN, AS, AEE, AWW, ANN, ASS;
-    if (!QUICK || band) {
-        AE = dy * mx0(-ue);
-        AW = dy * mx0(uw);
-        AN = dx * mx0(-vn);
-        AS = dx * mx0(vs);
-        AEE = AWW = ANN = ASS = 0.0;
-    } else {
-        AE = -dy * (-0.75 * mx0(-ue) + 0.375 * mx0(ue) - 0.125 * mx0(-uw));
-        AW = -dy * (-0.125 * mx0(ue) + 0.375 * mx0(-uw) - 0.75 * mx0(uw));
-        AN = -dx * (-0.75 * mx0(-vn) + 0.375 * mx0(vn) - 0.125 * mx0(-vs));
-        AS = -dx * (-0.125 * mx0(vn) + 0.375 * mx0(-vn) - 0.75 * mx0(vs));
-        AEE = -0.125 * dy * mx0(-ue);
-        AWW = -0.125 * dy * mx0(uw);
-        ANN = -0.125 * dx * mx0(-vn);
-        ASS = -0.125 * dx * mx0(vs);
-    }
-    const double APc = AS + AW + AN + AE + ASS + AWW + ANN + AEE;
-    const bool d2 = ORDER == 2 || band;
     Coef9 c;
-    c.AE = AE + (d2 ? p.dband[0] : p.dint[0]);
-    c.AW = AW + (d2 ? p.dband[1] : p.dint[1]);
-    c.AN = AN + (d2 ? p.dband[2] : p.dint[2]);
-    c.AS = AS + (d2 ? p.dband[3] : p.dint[3]);
-    c.AEE = AEE + (d2 ? p.dband[4] : p.dint[4]);
-    c.AWW = AWW + (d2 ? p.dband[5] : p.dint[5]);
-    c.ANN = ANN + (d2 ? p.dband[6] : p.dint[6]);
-    c.ASS = ASS + (d2 ? p.dband[7] : p.dint[7]);
-    c.AP = APc + (d2 ? p.dband[8] : p.dint[8]);
+    if (QUICK) {
+        c.AE = -dy * (-0.75 * mxf(-ue) + 0.375 * mxf(ue) - 0.125 * mxf(-uw));
+        c.AW = -dy * (-0.125 * mxf(ue) + 0.375 * mxf(-uw) - 0.75 * mxf(uw));
+        c.AN = -dx * (-0.75 * mxf(-vn) + 0.375 * mxf(vn) - 0.125 * mxf(-vs));
+        c.AS = -dx * (-0.125 * mxf(vn) + 0.375 * mxf(-vn) - 0.75 * mxf(vs));
+        c.AEE = -0.125 * dy * mxf(-ue);
+        c.AWW = -0.125 * dy * mxf(uw);
+        c.ANN = -0.125 * dx * mxf(-vn);
+        c.ASS = -0.125 * dx * mxf(vs);
+    } else {
+        c.AE = dy * mxf(-ue);
+        c.AW = dy * mxf(uw);
+        c.AN = dx * mxf(-vn);
+        c.AS = dx * mxf(vs);
+        c.AEE = c.AWW = c.ANN = c.ASS = 0.0;
+    }
+    // Diffusive part: the 2nd-order (band) values for ORDER 2, else the 4th-order ones. Indexed
+    // directly so the parameter arrays stay in constant space.
+#define SGPU_D(k) (ORDER == 2 ? p.dband[k] : p.dint[k])
+    c.AP = c.AS + c.AW + c.AN + c.AE + c.ASS + c.AWW + c.ANN + c.AEE;
+    c.AE += SGPU_D(0);
+    c.AW += SGPU_D(1);
+    c.AN += SGPU_D(2);
+    c.AS += SGPU_D(3);
+    c.AEE += SGPU_D(4);
+    c.AWW += SGPU_D(5);
+    c.ANN += SGPU_D(6);
+    c.ASS += SGPU_D(7);
+    c.AP += SGPU_D(8);
+#undef SGPU_D
+    if (QUICK || ORDER == 4) {
+        if (warp_has_band && band) {
+            // in_boundary_band: UDS convection and 2nd-order diffusion (coefficients.cpp:20-27, 45-51).
+            c.AE = dy * mxf(-ue);
+            c.AW = dy * mxf(uw);
+            c.AN = dx * mxf(-vn);
+            c.AS = dx * mxf(vs);
+            c.AP = c.AS + c.AW + c.AN + c.AE + 0.0 + 0.0 + 0.0 + 0.0;
+            c.AE += p.dband[0];
+            c.AW += p.dband[1];
+            c.AN += p.dband[2];
+            c.AS += p.dband[3];
+            c.AEE = 0.0 + p.dband[4];
+            c.AWW = 0.0 + p.dband[5];
+            c.ANN = 0.0 + p.dband[6];
+            c.ASS = 0.0 + p.dband[7];
+            c.AP += p.dband[8];
+        }
+    }
     return c;
+}
+
+__device__ __forceinline__ void prefetch_l1(const double* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
 // One multicolour sweep of u (V = false) or v (V = true) from xin to xout. NT threads per CTA, one
 // column each; the CTA owns W = NT - 4 * NCOL columns starting at blockIdx.x * W and rows
 // [blockIdx.y * seg_rows, + seg_rows). For five colours every dependency between two updates is at
-// least two steps apart, so two steps run between barriers (SPB = 2). Each super-step prefetches
-// the next one's coefficient inputs into registers (two register sets, alternating), so their
-// latency overlaps the current updates.
-template <int NCOL, bool V, int NT, bool QUICK, int ORDER>
-__global__ void __launch_bounds__(NT, 2)
+// least two steps apart, so two steps run between barriers (SPB = 2). PF selects how the cells'
+// global inputs are brought in: 0 = loaded into registers one super-step ahead, 1 = loaded when
+// used (more CTAs per SM hide the latency), 2 = their cache lines prefetched into L1 one
+// super-step ahead and loaded when used.
+template <int NCOL, bool V, int NT, bool QUICK, int ORDER, int PF>
+__global__ void __launch_bounds__(NT, PF == 0 ? 2 : 3)
     k_mom_stream(DevParams p, const double* __restrict__ xin, double* __restrict__ xout,
                  const double* __restrict__ xF, const double* __restrict__ oth,
                  const double* __restrict__ pf, int seg_rows) {
@@ -205,6 +244,7 @@ __global__ void __launch_bounds__(NT, 2)
     }
     // Band tests need global indices: in_boundary_band (coefficients.cpp:10-13).
     const bool col_band = col == p.Hy + 1 || col == p.NY + p.Hy;
+    const int band_r0 = p.Hx, band_r1 = p.NX + p.Hx - 1;
     const double relax = V ? p.av : p.au;
     const double omr = 1 - relax;
     const double* xFc = xF + col;
@@ -219,15 +259,29 @@ __global__ void __launch_bounds__(NT, 2)
         cp_async_commit();
         ++next;
     };
-    // Colour of the cell this column updates at step t: (2t + col) mod 5, or (t + col) mod 2.
-    auto colour_at = [&](int t) {
-        return NCOL == 5 ? (2 * t + col + 1000) % 5 : (t + col + 1000) & 1;
-    };
     auto step_cell = [&](int c, int t, int& r) -> bool {
         r = t - 2 * c;
         return ((colmask >> c) & 1u) && r >= s_rmin[c] && r <= s_rmax[c];
     };
-    auto update = [&](int r, const double a[9]) {
+    auto prefetch_cell = [&](int r) {
+        const int o = r * ld;
+        if (!V) {
+            prefetch_l1(xFc + o);
+            prefetch_l1(othc + o);
+            prefetch_l1(othc + o + ld);
+            prefetch_l1(pfc + o);
+        } else {
+            prefetch_l1(othc + o - ld);
+            prefetch_l1(othc + o);
+            prefetch_l1(xFc + o - ld);
+            prefetch_l1(xFc + o);
+            prefetch_l1(xFc + o + ld);
+            prefetch_l1(pfc + o - ld);
+            prefetch_l1(pfc + o);
+        }
+    };
+    auto is_band = [&](bool ok, int r) { return ok && (col_band || r == band_r1 || r == band_r0); };
+    auto update = [&](int r, const double a[9], bool warp_has_band) {
         double ue, uw, vn, vs, pt;
         if (!V) {
             ue = (a[1] + a[2]) / 2;
@@ -242,8 +296,8 @@ __global__ void __launch_bounds__(NT, 2)
             vs = (a[4] + a[6]) / 2;
             pt = (a[7] - a[8]) * p.dx;
         }
-        const bool band = col_band || r == p.NX + p.Hx - 1 || r == p.Hx;
-        const Coef9 k = coef_spec<QUICK, ORDER>(p, ue, uw, vn, vs, band);
+        const bool band = col_band || r == band_r1 || r == band_r0;
+        const Coef9 k = coef_spec<QUICK, ORDER>(p, ue, uw, vn, vs, band, warp_has_band);
         double* rc = ringc + (r & (kRing - 1)) * NT;
         const double xe = rc[1], xw = rc[-1];
         const double xn = ringc[((r - 1) & (kRing - 1)) * NT];
@@ -263,49 +317,95 @@ __global__ void __launch_bounds__(NT, 2)
     for (int k = 0; k < A; ++k) issue(); // rows L0 .. L0 + A - 1
     __syncthreads();                     // s_rmin / s_rmax
 
-    // One super-step starting at step t: cells with inputs `cur`; prefetch step t + SPB's into nxt.
-    int cA = colour_at(L0);
-    double bufA[SPB][9], bufB[SPB][9];
-    int rA[SPB], rB[SPB];
-    bool okA[SPB], okB[SPB];
-#pragma unroll
-    for (int s = 0; s < SPB; ++s) {
-        const int c = NCOL == 5 ? (cA + 2 * s) % 5 : (cA + s) & 1;
-        okA[s] = step_cell(c, L0 + s, rA[s]);
-        if (okA[s]) load_inputs<V>(xFc, othc, pfc, rA[s] * ld, ld, bufA[s]);
-    }
-    auto super_step = [&](int t, int c0, double (&cur)[SPB][9], const int (&rcur)[SPB],
-                          const bool (&okcur)[SPB], double (&nxt)[SPB][9], int (&rnxt)[SPB],
-                          bool (&oknxt)[SPB]) {
-        cp_async_wait<kPrefetch>(); // rows <= t + SPB + 1 have landed (this thread's copies)
-        __syncthreads();            // ... everyone's, and the previous super-step's updates
-#pragma unroll
-        for (int s = 0; s < SPB; ++s) issue();
-        const int cn = NCOL == 5 ? (c0 + 2 * SPB) % 5 : (c0 + SPB) & 1; // colour at t + SPB
-#pragma unroll
-        for (int s = 0; s < SPB; ++s) {
-            const int c = NCOL == 5 ? (cn + 2 * s) % 5 : (cn + s) & 1;
-            oknxt[s] = step_cell(c, t + SPB + s, rnxt[s]);
-            if (oknxt[s]) load_inputs<V>(xFc, othc, pfc, rnxt[s] * ld, ld, nxt[s]);
-        }
-#pragma unroll
-        for (int s = 0; s < SPB; ++s)
-            if (okcur[s]) update(rcur[s], cur[s]);
-        // Rows whose last update was in an earlier super-step: write the owned part back.
+    const int c_start = NCOL == 5 ? (2 * L0 + col + 1000) % 5 : (L0 + col + 1000) & 1;
+    auto next_colour = [&](int c, int steps) {
+        return NCOL == 5 ? (c + 2 * steps) % 5 : (c + steps) & 1;
+    };
+    // Row R1 - 1 is written back by the super-step starting at R1 + 2 NCOL - 2 or one later.
+    const int t_last = R1 + 2 * NCOL - 2 + (SPB - 1);
+
+    auto write_back = [&](int t) {
 #pragma unroll
         for (int s = 0; s < SPB; ++s) {
             const int rw = t - 2 * NCOL + 1 - (SPB - 1) + s;
             if (rw >= R0 && rw < R1 && col_out) xout[col + rw * ld] = ringc[(rw & (kRing - 1)) * NT];
         }
-        return cn;
     };
 
-    // Row R1 - 1 is written back by the super-step starting at R1 + 2 NCOL - 2 or one later.
-    const int t_last = R1 + 2 * NCOL - 2 + (SPB - 1);
-    int c0 = cA;
-    for (int t = L0; t <= t_last; t += 2 * SPB) {
-        c0 = super_step(t, c0, bufA, rA, okA, bufB, rB, okB);
-        if (t + SPB <= t_last) c0 = super_step(t + SPB, c0, bufB, rB, okB, bufA, rA, okA);
+    if (PF == 0) {
+        // Register prefetch: two register sets, alternating between consecutive super-steps.
+        double bufA[SPB][9], bufB[SPB][9];
+        int rA[SPB], rB[SPB];
+        bool okA[SPB], okB[SPB];
+#pragma unroll
+        for (int s = 0; s < SPB; ++s) {
+            okA[s] = step_cell(next_colour(c_start, s), L0 + s, rA[s]);
+            if (okA[s]) load_inputs<V>(xFc, othc, pfc, rA[s] * ld, ld, bufA[s]);
+        }
+        auto super_step = [&](int t, int c0, double (&cur)[SPB][9], const int (&rcur)[SPB],
+                              const bool (&okcur)[SPB], double (&nxt)[SPB][9], int (&rnxt)[SPB],
+                              bool (&oknxt)[SPB]) {
+            cp_async_wait<kPrefetch>(); // rows <= t + SPB + 1 have landed (this thread's copies)
+            __syncthreads();            // ... everyone's, and the previous super-step's updates
+#pragma unroll
+            for (int s = 0; s < SPB; ++s) issue();
+            const int cn = next_colour(c0, SPB);
+#pragma unroll
+            for (int s = 0; s < SPB; ++s) {
+                oknxt[s] = step_cell(next_colour(cn, s), t + SPB + s, rnxt[s]);
+                if (oknxt[s]) load_inputs<V>(xFc, othc, pfc, rnxt[s] * ld, ld, nxt[s]);
+            }
+#pragma unroll
+            for (int s = 0; s < SPB; ++s) {
+                const bool wb = __any_sync(0xffffffffu, is_band(okcur[s], rcur[s]));
+                if (okcur[s]) update(rcur[s], cur[s], wb);
+            }
+            write_back(t);
+            return cn;
+        };
+        int c0 = c_start;
+        for (int t = L0; t <= t_last; t += 2 * SPB) {
+            c0 = super_step(t, c0, bufA, rA, okA, bufB, rB, okB);
+            if (t + SPB <= t_last) c0 = super_step(t + SPB, c0, bufB, rB, okB, bufA, rA, okA);
+        }
+    } else {
+        int c0 = c_start;
+        if (PF == 2) {
+#pragma unroll
+            for (int s = 0; s < SPB; ++s) {
+                int r;
+                if (step_cell(next_colour(c0, s), L0 + s, r)) prefetch_cell(r);
+            }
+        }
+        for (int t = L0; t <= t_last; t += SPB) {
+            cp_async_wait<kPrefetch>();
+            __syncthreads();
+#pragma unroll
+            for (int s = 0; s < SPB; ++s) issue();
+            const int cn = next_colour(c0, SPB);
+            if (PF == 2) {
+#pragma unroll
+                for (int s = 0; s < SPB; ++s) {
+                    int r;
+                    if (step_cell(next_colour(cn, s), t + SPB + s, r)) prefetch_cell(r);
+                }
+            }
+            int r[SPB];
+            bool ok[SPB];
+            double a[SPB][9];
+#pragma unroll
+            for (int s = 0; s < SPB; ++s) {
+                ok[s] = step_cell(next_colour(c0, s), t + s, r[s]);
+                if (ok[s]) load_inputs<V>(xFc, othc, pfc, r[s] * ld, ld, a[s]);
+            }
+#pragma unroll
+            for (int s = 0; s < SPB; ++s) {
+                const bool wb = __any_sync(0xffffffffu, is_band(ok[s], r[s]));
+                if (ok[s]) update(r[s], a[s], wb);
+            }
+            write_back(t);
+            c0 = cn;
+        }
     }
     cp_async_wait<0>();
 }
@@ -349,7 +449,7 @@ void prep_ranges(const DevParams& p, Range& ur, Range& cr) {
     }
 }
 
-template <int NCOL, bool V, int NT, bool QUICK, int ORDER>
+template <int NCOL, bool V, int NT, bool QUICK, int ORDER, int PF>
 void launch_stream(const DevParams& p, const double* xin, double* xout, const double* xF,
                    const double* oth, const double* pf, int seg_rows, cudaStream_t st) {
     constexpr int W = NT - 4 * NCOL;
@@ -357,21 +457,21 @@ void launch_stream(const DevParams& p, const double* xin, double* xout, const do
     constexpr int smem = kRing * NT * static_cast<int>(sizeof(double));
     static bool attr_set = false; // per process; the attribute applies to every device
     if (!attr_set) {
-        SGPU_CUDA(cudaFuncSetAttribute(k_mom_stream<NCOL, V, NT, QUICK, ORDER>,
+        SGPU_CUDA(cudaFuncSetAttribute(k_mom_stream<NCOL, V, NT, QUICK, ORDER, PF>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         attr_set = true;
     }
-    k_mom_stream<NCOL, V, NT, QUICK, ORDER><<<grid, NT, smem, st>>>(p, xin, xout, xF, oth, pf, seg_rows);
+    k_mom_stream<NCOL, V, NT, QUICK, ORDER, PF><<<grid, NT, smem, st>>>(p, xin, xout, xF, oth, pf, seg_rows);
     SGPU_LAUNCH();
 }
 
-template <bool V>
+template <bool V, int PF>
 void launch_stream_v(const DevParams& p, const double* xin, double* xout, const double* xF,
                      const double* oth, const double* pf, int seg_rows, cudaStream_t st) {
-    if (p.uds && p.order == 2) launch_stream<2, V, 256, false, 2>(p, xin, xout, xF, oth, pf, seg_rows, st);
-    else if (p.uds) launch_stream<5, V, 256, false, 4>(p, xin, xout, xF, oth, pf, seg_rows, st);
-    else if (p.order == 2) launch_stream<5, V, 256, true, 2>(p, xin, xout, xF, oth, pf, seg_rows, st);
-    else launch_stream<5, V, 256, true, 4>(p, xin, xout, xF, oth, pf, seg_rows, st);
+    if (p.uds && p.order == 2) launch_stream<2, V, 256, false, 2, PF>(p, xin, xout, xF, oth, pf, seg_rows, st);
+    else if (p.uds) launch_stream<5, V, 256, false, 4, PF>(p, xin, xout, xF, oth, pf, seg_rows, st);
+    else if (p.order == 2) launch_stream<5, V, 256, true, 2, PF>(p, xin, xout, xF, oth, pf, seg_rows, st);
+    else launch_stream<5, V, 256, true, 4, PF>(p, xin, xout, xF, oth, pf, seg_rows, st);
 }
 
 } // namespace
@@ -403,8 +503,8 @@ void launch_mom_prep(const DevParams& p, bool v_component, const double* x, cons
 void launch_mom_sweep(const DevParams& p, bool v_component, const double* xin, double* xout,
                       const double* xF, const double* oth, const double* pf, int seg_rows,
                       cudaStream_t st) {
-    if (v_component) launch_stream_v<true>(p, xin, xout, xF, oth, pf, seg_rows, st);
-    else launch_stream_v<false>(p, xin, xout, xF, oth, pf, seg_rows, st);
+    if (v_component) launch_stream_v<true, kStreamPF>(p, xin, xout, xF, oth, pf, seg_rows, st);
+    else launch_stream_v<false, kStreamPF>(p, xin, xout, xF, oth, pf, seg_rows, st);
 }
 
 void launch_assemble_p_fused(const DevParams& p, const double* APU, const double* APV,

@@ -39,6 +39,7 @@ SOURCES = {
     "cg.cu": EXACT,
     "fused.cu": EXACT,
     "mg_fast.cu": EXACT,
+    "mixed.cu": EXACT,
     "io.cpp": EXACT,
     "noalloc.cu": EXACT,
 }

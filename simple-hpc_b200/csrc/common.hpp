@@ -87,9 +87,11 @@ struct DevParams {
 // Multigrid level view (the reference's MGView, include/simple/multigrid.hpp:59-66): element
 // (I, J), 0 <= I < nx, 0 <= J < ny, of each array is ptr[I * stride + J]; the pointers address
 // interior cell (0, 0) and every neighbour of an interior cell lies inside the allocation.
-struct LevelView {
+template <class T> struct LevelViewT {
     int nx, ny, stride;
-    double *AE, *AW, *AN, *AS, *AP, *b, *x, *r;
+    T *AE, *AW, *AN, *AS, *AP, *b, *x, *r;
 };
+using LevelView = LevelViewT<double>;
+using LevelView32 = LevelViewT<float>;
 
 } // namespace sgpu

@@ -21,6 +21,9 @@ struct SumScratch {
 };
 void launch_ordered_sum(const double* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
                         double* out, const SumScratch& s, const int* skip, cudaStream_t st);
+// The same order over FP32 values, each widened to double before it is added.
+void launch_ordered_sum(const float* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
+                        double* out, const SumScratch& s, const int* skip, cudaStream_t st);
 
 // ---- momentum and pressure phases, reference-shaped (phases.cu) ----
 struct Coef9Ptr {
@@ -64,32 +67,42 @@ void launch_correct(const DevParams& p, PressurePtr w, const double* APU, const 
 void launch_copy(const double* src, double* dst, std::size_t n, cudaStream_t st);
 
 // ---- multigrid (mg.cu) ----
-void launch_mg_build(const LevelView& F, const LevelView& C, cudaStream_t st);
-void launch_mg_smooth_colour(const LevelView& L, int colour, cudaStream_t st);
-void launch_mg_residual(const LevelView& L, cudaStream_t st);
-void launch_mg_restrict(const LevelView& F, const LevelView& C, cudaStream_t st);
-void launch_mg_prolong(const LevelView& C, const LevelView& F, double omega, cudaStream_t st);
+// Every multigrid launcher is instantiated for double (the reference's bits) and float (the
+// mixed-precision V-cycle).
+template <class T> void launch_mg_build(const LevelViewT<T>& F, const LevelViewT<T>& C, cudaStream_t st);
+template <class T> void launch_mg_smooth_colour(const LevelViewT<T>& L, int colour, cudaStream_t st);
+template <class T> void launch_mg_residual(const LevelViewT<T>& L, cudaStream_t st);
+template <class T> void launch_mg_restrict(const LevelViewT<T>& F, const LevelViewT<T>& C, cudaStream_t st);
+template <class T>
+void launch_mg_prolong(const LevelViewT<T>& C, const LevelViewT<T>& F, double omega, cudaStream_t st);
 // x[I, J] -= *sum / (nx * ny) over the level interior (the mean removal after an ordered sum).
 void launch_mg_sub_mean(const LevelView& L, double* x, const double* sum, cudaStream_t st);
-// Coarsest-level solve in one CTA (coarse_solve, multigrid.cpp:120-140); *sweeps_out gets the count.
-void launch_mg_coarse(const LevelView& L, double* rowbuf, int* sweeps_out, cudaStream_t st);
+// Coarsest-level solve in one CTA (coarse_solve, multigrid.cpp:120-140) with relative tolerance
+// tol (the reference's 1e-10 in FP64); *sweeps_out gets the sweep count.
+template <class T>
+void launch_mg_coarse(const LevelViewT<T>& L, double* rowbuf, double tol, int* sweeps_out,
+                      cudaStream_t st);
 // The whole hierarchy, by value, for the single-CTA tail kernel.
-struct MgLevels {
-    LevelView L[24];
+template <class T> struct MgLevelsT {
+    LevelViewT<T> L[24];
     int n;
 };
+using MgLevels = MgLevelsT<double>;
 // Levels [first, n) of one V-cycle in one CTA: down-leg, coarse solve, up-leg (mg_vcycle order).
-void launch_mg_tail(const MgLevels& lv, int first, int pre, int post, double omega, double* rowbuf,
-                    int* sweeps_out, cudaStream_t st);
+template <class T>
+void launch_mg_tail(const MgLevelsT<T>& lv, int first, int pre, int post, double omega, double tol,
+                    double* rowbuf, int* sweeps_out, cudaStream_t st);
 
-// ---- streaming multigrid level kernels (mg_fast.cu) ----
+// ---- streaming multigrid level kernels (mg_fast.cu), double and float ----
 bool mg_fast_supported(int pre, int post);
 // pre red-black sweeps on F (x from F.x, or zero), residual, restriction into C.b (C.x = 0); the
 // smoothed iterate is written to xout (F.x is left unchanged when pre > 0).
-void launch_mg_down(const LevelView& F, const LevelView& C, double* xout, int pre, bool x_zero,
+template <class T>
+void launch_mg_down(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, int pre, bool x_zero,
                     int sms, cudaStream_t st);
 // xout = xin + omega * P C.x, then post red-black sweeps (F's coefficients and b).
-void launch_mg_up(const LevelView& C, const LevelView& F, const double* xin, double* xout,
+template <class T>
+void launch_mg_up(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, T* xout,
                   double omega, int post, int sms, cudaStream_t st);
 
 // ---- conjugate gradient (cg.cu) ----
@@ -110,6 +123,31 @@ void launch_cg_dq(const DevParams& p, PressurePtr w, CgPtr cg, const CgScalars* 
 void launch_cg_update(const DevParams& p, PressurePtr w, CgPtr cg, const CgScalars* sc,
                       double* cells, std::size_t plane, cudaStream_t st);
 void launch_cg_dir(const DevParams& p, CgPtr cg, const CgScalars* sc, cudaStream_t st);
+
+// ---- mixed precision (mixed.cu) ----
+struct Coef9Ptr32 {
+    float* a[9]; // AE AW AN AS AEE AWW ANN ASS AP
+};
+void init_mixed_kernels();
+// FP64 prep: |R| into cells, AP (FP64), R and the 9 coefficients in FP32, over the update range.
+void launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x, const double* oth,
+                           const double* pf, double* AP, double* cells, float* r32,
+                           const Coef9Ptr32& c32, cudaStream_t st);
+// One FP32 multicolour correction sweep e_in -> e_out (e_zero: e_in is zero and not read).
+void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, float* eout,
+                       const float* r32, const Coef9Ptr32& c32, bool e_zero, int seg_rows,
+                       cudaStream_t st);
+// x += e over the component's update range.
+void launch_add_correction(const DevParams& p, bool v_component, double* x, const float* e,
+                           cudaStream_t st);
+void launch_assemble_p_mixed(const DevParams& p, const double* APU, const double* APV,
+                             const double* u, const double* v, double* bfield,
+                             const LevelView32& L0, double* cabs, double* cb, cudaStream_t st);
+void launch_b_to_f32(const DevParams& p, const double* bfield, const double* sum_b,
+                     const LevelView32& L0, cudaStream_t st);
+void launch_correct_mixed(const DevParams& p, const LevelView32& L0, const double* sum_pc,
+                          const double* APU, const double* APV, double* u, double* v, double* pf,
+                          double* pc64, cudaStream_t st);
 
 // ---- fused fast path (fused.cu) ----
 int stream_seg_rows(const DevParams& p, int sms);

@@ -1,11 +1,12 @@
-// mg.cu — geometric multigrid for p' on the device, FP64, bit-identical to the reference.
+// mg.cu — geometric multigrid for p' on the device, bit-identical to the reference in FP64.
 //
 // The reference runs multigrid on the CPU only (src/multigrid.cpp). These kernels restate each of
 // its loops with the same per-cell expression order: the Galerkin 2x2 build (mg_build, :232-261),
 // the red-black two-statement smoother (smooth, :46-70), residual (:73-87), restriction (:90-103),
 // prolongation with over-correction (:106-116), and the coarsest-level solve with its fixed-order
 // norms (coarse_solve, :120-140), which runs inside one CTA so its data-dependent sweep count
-// needs no host round trip.
+// needs no host round trip. Every kernel is a template on the element type: double gives the
+// reference's bits; float is the mixed-precision mode's V-cycle (sums and norms still in double).
 #include "kernels.hpp"
 
 namespace sgpu {
@@ -17,15 +18,15 @@ constexpr int BX = 32, BY = 8;
 dim3 grid2(int nx, int ny) { return dim3((ny + BX - 1) / BX, (nx + BY - 1) / BY); }
 
 // mg_build: coarse links are the sums of the two fine links crossing each coarse face.
-__global__ void k_mg_build(LevelView F, LevelView C) {
+template <class T> __global__ void k_mg_build(LevelViewT<T> F, LevelViewT<T> C) {
     const int J = blockIdx.x * BX + threadIdx.x, I = blockIdx.y * BY + threadIdx.y;
     if (I >= C.nx || J >= C.ny) return;
     const int fs = F.stride;
     const int f = 2 * I * fs + 2 * J, c = I * C.stride + J;
-    const double ae = F.AE[f + 1] + F.AE[f + fs + 1];
-    const double aw = F.AW[f] + F.AW[f + fs];
-    const double an = F.AN[f] + F.AN[f + 1];
-    const double as = F.AS[f + fs] + F.AS[f + fs + 1];
+    const T ae = F.AE[f + 1] + F.AE[f + fs + 1];
+    const T aw = F.AW[f] + F.AW[f + fs];
+    const T an = F.AN[f] + F.AN[f + 1];
+    const T as = F.AS[f + fs] + F.AS[f + fs + 1];
     C.AE[c] = ae;
     C.AW[c] = aw;
     C.AN[c] = an;
@@ -34,38 +35,38 @@ __global__ void k_mg_build(LevelView F, LevelView C) {
 }
 
 // One colour of smooth: colour (I + J) & 1, update x = b/AP; x += (E W S N)/AP.
-__global__ void k_mg_smooth(LevelView L, int colour) {
+template <class T> __global__ void k_mg_smooth(LevelViewT<T> L, int colour) {
     const int J = blockIdx.x * BX + threadIdx.x, I = blockIdx.y * BY + threadIdx.y;
     if (I >= L.nx || J >= L.ny || ((I + J) & 1) != colour) return;
     const int s = L.stride, q = I * s + J;
-    double* x = L.x;
-    double t = L.b[q] / L.AP[q];
+    T* x = L.x;
+    T t = L.b[q] / L.AP[q];
     t += (L.AE[q] * x[q + 1] + L.AW[q] * x[q - 1] + L.AS[q] * x[q + s] + L.AN[q] * x[q - s]) / L.AP[q];
     x[q] = t;
 }
 
-__global__ void k_mg_residual(LevelView L) {
+template <class T> __global__ void k_mg_residual(LevelViewT<T> L) {
     const int J = blockIdx.x * BX + threadIdx.x, I = blockIdx.y * BY + threadIdx.y;
     if (I >= L.nx || J >= L.ny) return;
     const int s = L.stride, q = I * s + J;
-    const double* x = L.x;
+    const T* x = L.x;
     L.r[q] = L.b[q] - (L.AP[q] * x[q] -
                        (L.AE[q] * x[q + 1] + L.AW[q] * x[q - 1] + L.AS[q] * x[q + s] +
                         L.AN[q] * x[q - s]));
 }
 
-__global__ void k_mg_restrict(LevelView F, LevelView C) {
+template <class T> __global__ void k_mg_restrict(LevelViewT<T> F, LevelViewT<T> C) {
     const int J = blockIdx.x * BX + threadIdx.x, I = blockIdx.y * BY + threadIdx.y;
     if (I >= F.nx / 2 || J >= F.ny / 2) return;
     const int fs = F.stride, f = 2 * I * fs + 2 * J, c = I * C.stride + J;
     C.b[c] = F.r[f] + F.r[f + 1] + F.r[f + fs] + F.r[f + fs + 1];
-    C.x[c] = 0.0;
+    C.x[c] = T(0);
 }
 
-__global__ void k_mg_prolong(LevelView C, LevelView F, double omega) {
+template <class T> __global__ void k_mg_prolong(LevelViewT<T> C, LevelViewT<T> F, double omega) {
     const int j = blockIdx.x * BX + threadIdx.x, i = blockIdx.y * BY + threadIdx.y;
     if (i >= F.nx || j >= F.ny) return;
-    F.x[i * F.stride + j] += omega * C.x[(i / 2) * C.stride + j / 2];
+    F.x[i * F.stride + j] += static_cast<T>(omega) * C.x[(i / 2) * C.stride + j / 2];
 }
 
 __global__ void k_mg_sub_mean(LevelView L, double* x, const double* sum) {
@@ -75,13 +76,14 @@ __global__ void k_mg_sub_mean(LevelView L, double* x, const double* sum) {
     x[I * L.stride + J] -= m;
 }
 
-// ---- coarsest level in one CTA ----
+// ---- levels inside one CTA ----
 
 constexpr int kCoarseThreads = 512;
 
 // det_sum (multigrid.cpp:18-34) of f(q) in one CTA: one thread per row chain, then row order.
-template <class F>
-__device__ double cta_det_sum(const LevelView& L, double* rowbuf, F f) {
+// Accumulates in double for both element types.
+template <class T, class F>
+__device__ double cta_det_sum(const LevelViewT<T>& L, double* rowbuf, F f) {
     for (int I = threadIdx.x; I < L.nx; I += blockDim.x) {
         double s = 0.0;
         for (int J = 0; J < L.ny; ++J) s += f(I * L.stride + J);
@@ -100,25 +102,25 @@ __device__ double cta_det_sum(const LevelView& L, double* rowbuf, F f) {
     return t;
 }
 
-__device__ void cta_remove_mean(const LevelView& L, double* rowbuf, double* x) {
-    const double m =
-        cta_det_sum(L, rowbuf, [x](int q) { return x[q]; }) / (static_cast<double>(L.nx) * L.ny);
+template <class T> __device__ void cta_remove_mean(const LevelViewT<T>& L, double* rowbuf, T* x) {
+    const double m = cta_det_sum(L, rowbuf, [x](int q) { return static_cast<double>(x[q]); }) /
+                     (static_cast<double>(L.nx) * L.ny);
     const int n = L.nx * L.ny;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const int I = k / L.ny, J = k % L.ny;
-        x[I * L.stride + J] -= m;
+        x[I * L.stride + J] = static_cast<T>(x[I * L.stride + J] - m);
     }
     __syncthreads();
 }
 
-__device__ void cta_smooth_colour(const LevelView& L, int colour) {
+template <class T> __device__ void cta_smooth_colour(const LevelViewT<T>& L, int colour) {
     const int n = L.nx * L.ny, s = L.stride;
-    double* x = L.x;
+    T* x = L.x;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const int I = k / L.ny, J = k % L.ny;
         if (((I + J) & 1) != colour) continue;
         const int q = I * s + J;
-        double t = L.b[q] / L.AP[q];
+        T t = L.b[q] / L.AP[q];
         t += (L.AE[q] * x[q + 1] + L.AW[q] * x[q - 1] + L.AS[q] * x[q + s] + L.AN[q] * x[q - s]) /
              L.AP[q];
         x[q] = t;
@@ -126,9 +128,9 @@ __device__ void cta_smooth_colour(const LevelView& L, int colour) {
     __syncthreads();
 }
 
-__device__ void cta_residual(const LevelView& L) {
+template <class T> __device__ void cta_residual(const LevelViewT<T>& L) {
     const int n = L.nx * L.ny, s = L.stride;
-    const double* x = L.x;
+    const T* x = L.x;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const int I = k / L.ny, J = k % L.ny, q = I * s + J;
         L.r[q] = L.b[q] - (L.AP[q] * x[q] - (L.AE[q] * x[q + 1] + L.AW[q] * x[q - 1] +
@@ -137,57 +139,72 @@ __device__ void cta_residual(const LevelView& L) {
     __syncthreads();
 }
 
+// restrict_residual (multigrid.cpp:90-103) inside one CTA.
+template <class T> __device__ void cta_restrict(const LevelViewT<T>& F, const LevelViewT<T>& C) {
+    const int n = C.nx * C.ny, fs = F.stride;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const int I = k / C.ny, J = k % C.ny;
+        const int f = 2 * I * fs + 2 * J, c = I * C.stride + J;
+        C.b[c] = F.r[f] + F.r[f + 1] + F.r[f + fs] + F.r[f + fs + 1];
+        C.x[c] = T(0);
+    }
+    __syncthreads();
+}
+
+// prolong (multigrid.cpp:106-116) inside one CTA.
+template <class T>
+__device__ void cta_prolong(const LevelViewT<T>& C, const LevelViewT<T>& F, double omega) {
+    const int n = F.nx * F.ny;
+    const T om = static_cast<T>(omega);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const int i = k / F.ny, j = k % F.ny;
+        F.x[i * F.stride + j] += om * C.x[(i / 2) * C.stride + j / 2];
+    }
+    __syncthreads();
+}
+
 // coarse_solve (multigrid.cpp:120-140): remove the mean of b; red-black sweeps until
-// ||b - A x|| < 1e-10 ||b|| or 200 sweeps; remove the mean of x.
-__global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(LevelView L, double* rowbuf,
-                                                              int* sweeps_out) {
+// ||b - A x|| < tol ||b|| (tol = 1e-10 in the reference) or 200 sweeps; remove the mean of x.
+template <class T>
+__device__ void cta_coarse_solve(const LevelViewT<T>& L, double* rowbuf, double tol, int* sweeps_out) {
     cta_remove_mean(L, rowbuf, L.b);
-    const double* b = L.b;
-    const double bb = cta_det_sum(L, rowbuf, [b](int q) { return b[q] * b[q]; });
+    const T* b = L.b;
+    const double bb = cta_det_sum(L, rowbuf, [b](int q) {
+        const double v = b[q];
+        return v * v;
+    });
     int sweeps = 0;
     if (bb > 0.0) {
         const double bn = sqrt(bb);
-        const double* r = L.r;
+        const T* r = L.r;
         while (sweeps < 200) {
             cta_smooth_colour(L, 0);
             cta_smooth_colour(L, 1);
             ++sweeps;
             cta_residual(L);
-            const double rr = cta_det_sum(L, rowbuf, [r](int q) { return r[q] * r[q]; });
-            if (sqrt(rr) < 1e-10 * bn) break;
+            const double rr = cta_det_sum(L, rowbuf, [r](int q) {
+                const double v = r[q];
+                return v * v;
+            });
+            if (sqrt(rr) < tol * bn) break;
         }
     }
     cta_remove_mean(L, rowbuf, L.x);
     if (threadIdx.x == 0 && sweeps_out) *sweeps_out = sweeps;
 }
 
-// restrict_residual (multigrid.cpp:90-103) inside one CTA.
-__device__ void cta_restrict(const LevelView& F, const LevelView& C) {
-    const int n = C.nx * C.ny, fs = F.stride;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        const int I = k / C.ny, J = k % C.ny;
-        const int f = 2 * I * fs + 2 * J, c = I * C.stride + J;
-        C.b[c] = F.r[f] + F.r[f + 1] + F.r[f + fs] + F.r[f + fs + 1];
-        C.x[c] = 0.0;
-    }
-    __syncthreads();
-}
-
-// prolong (multigrid.cpp:106-116) inside one CTA.
-__device__ void cta_prolong(const LevelView& C, const LevelView& F, double omega) {
-    const int n = F.nx * F.ny;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        const int i = k / F.ny, j = k % F.ny;
-        F.x[i * F.stride + j] += omega * C.x[(i / 2) * C.stride + j / 2];
-    }
-    __syncthreads();
+template <class T>
+__global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(LevelViewT<T> L, double* rowbuf,
+                                                              double tol, int* sweeps_out) {
+    cta_coarse_solve(L, rowbuf, tol, sweeps_out);
 }
 
 // Levels [first, nl) of one V-cycle (mg_vcycle, multigrid.cpp:299-323) in one CTA: the small
 // levels are latency-bound, so they run back to back with a block barrier between passes.
+template <class T>
 __global__ void __launch_bounds__(kCoarseThreads)
-    k_mg_tail(MgLevels lv, int first, int pre, int post, double omega, double* rowbuf,
-              int* sweeps_out) {
+    k_mg_tail(MgLevelsT<T> lv, int first, int pre, int post, double omega, double tol,
+              double* rowbuf, int* sweeps_out) {
     const int nl = lv.n;
     for (int l = first; l + 1 < nl; ++l) {
         for (int s = 0; s < pre; ++s) {
@@ -197,26 +214,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
         cta_residual(lv.L[l]);
         cta_restrict(lv.L[l], lv.L[l + 1]);
     }
-    // coarse_solve (multigrid.cpp:120-140)
-    const LevelView& L = lv.L[nl - 1];
-    cta_remove_mean(L, rowbuf, L.b);
-    const double* b = L.b;
-    const double bb = cta_det_sum(L, rowbuf, [b](int q) { return b[q] * b[q]; });
-    int sweeps = 0;
-    if (bb > 0.0) {
-        const double bn = sqrt(bb);
-        const double* r = L.r;
-        while (sweeps < 200) {
-            cta_smooth_colour(L, 0);
-            cta_smooth_colour(L, 1);
-            ++sweeps;
-            cta_residual(L);
-            const double rr = cta_det_sum(L, rowbuf, [r](int q) { return r[q] * r[q]; });
-            if (sqrt(rr) < 1e-10 * bn) break;
-        }
-    }
-    cta_remove_mean(L, rowbuf, L.x);
-    if (threadIdx.x == 0 && sweeps_out) *sweeps_out = sweeps;
+    cta_coarse_solve(lv.L[nl - 1], rowbuf, tol, sweeps_out);
     for (int l = nl - 2; l >= first; --l) {
         cta_prolong(lv.L[l + 1], lv.L[l], omega);
         for (int s = 0; s < post; ++s) {
@@ -228,39 +226,55 @@ __global__ void __launch_bounds__(kCoarseThreads)
 
 } // namespace
 
-void launch_mg_tail(const MgLevels& lv, int first, int pre, int post, double omega, double* rowbuf,
-                    int* sweeps_out, cudaStream_t st) {
-    k_mg_tail<<<1, kCoarseThreads, 0, st>>>(lv, first, pre, post, omega, rowbuf, sweeps_out);
+template <class T>
+void launch_mg_tail(const MgLevelsT<T>& lv, int first, int pre, int post, double omega, double tol,
+                    double* rowbuf, int* sweeps_out, cudaStream_t st) {
+    k_mg_tail<T><<<1, kCoarseThreads, 0, st>>>(lv, first, pre, post, omega, tol, rowbuf, sweeps_out);
     SGPU_LAUNCH();
 }
-
-void launch_mg_build(const LevelView& F, const LevelView& C, cudaStream_t st) {
-    k_mg_build<<<grid2(C.nx, C.ny), dim3(BX, BY), 0, st>>>(F, C);
+template <class T> void launch_mg_build(const LevelViewT<T>& F, const LevelViewT<T>& C, cudaStream_t st) {
+    k_mg_build<T><<<grid2(C.nx, C.ny), dim3(BX, BY), 0, st>>>(F, C);
     SGPU_LAUNCH();
 }
-void launch_mg_smooth_colour(const LevelView& L, int colour, cudaStream_t st) {
-    k_mg_smooth<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, st>>>(L, colour);
+template <class T> void launch_mg_smooth_colour(const LevelViewT<T>& L, int colour, cudaStream_t st) {
+    k_mg_smooth<T><<<grid2(L.nx, L.ny), dim3(BX, BY), 0, st>>>(L, colour);
     SGPU_LAUNCH();
 }
-void launch_mg_residual(const LevelView& L, cudaStream_t st) {
-    k_mg_residual<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, st>>>(L);
+template <class T> void launch_mg_residual(const LevelViewT<T>& L, cudaStream_t st) {
+    k_mg_residual<T><<<grid2(L.nx, L.ny), dim3(BX, BY), 0, st>>>(L);
     SGPU_LAUNCH();
 }
-void launch_mg_restrict(const LevelView& F, const LevelView& C, cudaStream_t st) {
-    k_mg_restrict<<<grid2(F.nx / 2, F.ny / 2), dim3(BX, BY), 0, st>>>(F, C);
+template <class T> void launch_mg_restrict(const LevelViewT<T>& F, const LevelViewT<T>& C, cudaStream_t st) {
+    k_mg_restrict<T><<<grid2(F.nx / 2, F.ny / 2), dim3(BX, BY), 0, st>>>(F, C);
     SGPU_LAUNCH();
 }
-void launch_mg_prolong(const LevelView& C, const LevelView& F, double omega, cudaStream_t st) {
-    k_mg_prolong<<<grid2(F.nx, F.ny), dim3(BX, BY), 0, st>>>(C, F, omega);
+template <class T>
+void launch_mg_prolong(const LevelViewT<T>& C, const LevelViewT<T>& F, double omega, cudaStream_t st) {
+    k_mg_prolong<T><<<grid2(F.nx, F.ny), dim3(BX, BY), 0, st>>>(C, F, omega);
+    SGPU_LAUNCH();
+}
+template <class T>
+void launch_mg_coarse(const LevelViewT<T>& L, double* rowbuf, double tol, int* sweeps_out, cudaStream_t st) {
+    k_mg_coarse<T><<<1, kCoarseThreads, 0, st>>>(L, rowbuf, tol, sweeps_out);
     SGPU_LAUNCH();
 }
 void launch_mg_sub_mean(const LevelView& L, double* x, const double* sum, cudaStream_t st) {
     k_mg_sub_mean<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, st>>>(L, x, sum);
     SGPU_LAUNCH();
 }
-void launch_mg_coarse(const LevelView& L, double* rowbuf, int* sweeps_out, cudaStream_t st) {
-    k_mg_coarse<<<1, kCoarseThreads, 0, st>>>(L, rowbuf, sweeps_out);
-    SGPU_LAUNCH();
-}
+
+#define SGPU_MG_INST(T)                                                                            \
+    template void launch_mg_tail<T>(const MgLevelsT<T>&, int, int, int, double, double, double*,   \
+                                    int*, cudaStream_t);                                           \
+    template void launch_mg_build<T>(const LevelViewT<T>&, const LevelViewT<T>&, cudaStream_t);    \
+    template void launch_mg_smooth_colour<T>(const LevelViewT<T>&, int, cudaStream_t);             \
+    template void launch_mg_residual<T>(const LevelViewT<T>&, cudaStream_t);                       \
+    template void launch_mg_restrict<T>(const LevelViewT<T>&, const LevelViewT<T>&, cudaStream_t); \
+    template void launch_mg_prolong<T>(const LevelViewT<T>&, const LevelViewT<T>&, double,         \
+                                       cudaStream_t);                                              \
+    template void launch_mg_coarse<T>(const LevelViewT<T>&, double*, double, int*, cudaStream_t);
+SGPU_MG_INST(double)
+SGPU_MG_INST(float)
+#undef SGPU_MG_INST
 
 } // namespace sgpu

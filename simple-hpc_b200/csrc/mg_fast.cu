@@ -1,5 +1,5 @@
-// mg_fast.cu — the multigrid V-cycle of multigrid.cpp with fused, streaming level kernels (FP64,
-// bit-identical to the reference).
+// mg_fast.cu — the multigrid V-cycle of multigrid.cpp with fused, streaming level kernels
+// (bit-identical to the reference in FP64; the float instantiation is the mixed-precision mode's).
 //
 // Per fine level two passes over memory instead of one per colour:
 //  * k_mg_down: `pre` red-black sweeps (smooth, multigrid.cpp:46-70), the residual (:73-87) and the
@@ -22,9 +22,12 @@ namespace {
 constexpr int kRing = 32;
 constexpr int kPD = 8; // prefetch distance in rows
 
-__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+template <class T> __device__ __forceinline__ void cp_async(T* smem, const T* gmem) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+    if (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_async_wait() {
@@ -42,19 +45,19 @@ struct Win {
 };
 
 template <int NT>
-__device__ __forceinline__ Win make_win(const LevelView& L, int seg_rows, int HC) {
+__device__ __forceinline__ Win make_win(int nx, int ny, int seg_rows, int HC) {
     Win w;
     w.W = NT - 2 * HC;
     w.R0 = blockIdx.y * seg_rows;
-    w.R1 = min(w.R0 + seg_rows, L.nx);
+    w.R1 = min(w.R0 + seg_rows, nx);
     w.L0 = max(w.R0 - HC, -1);
-    w.L1 = min(w.R1 + HC, L.nx + 1);
+    w.L1 = min(w.R1 + HC, nx + 1);
     w.J0 = blockIdx.x * w.W;
     w.C0 = w.J0 - HC;
     w.cut_top = w.L0 > -1;
-    w.cut_bot = w.L1 < L.nx + 1;
+    w.cut_bot = w.L1 < nx + 1;
     w.cut_left = w.C0 > -1;
-    w.cut_right = w.C0 + NT < L.ny + 1;
+    w.cut_right = w.C0 + NT < ny + 1;
     return w;
 }
 
@@ -65,7 +68,7 @@ __device__ __forceinline__ bool in_cone(const Win& w, int I, int Jc, int k, int 
 }
 
 // The 6 per-cell inputs of a red-black update or a residual: AE, AW, AN, AS, AP, b.
-__device__ __forceinline__ void load6(const LevelView& L, int q, double a[6]) {
+template <class T> __device__ __forceinline__ void load6(const LevelViewT<T>& L, int q, T a[6]) {
     a[0] = __ldg(L.AE + q);
     a[1] = __ldg(L.AW + q);
     a[2] = __ldg(L.AN + q);
@@ -75,10 +78,10 @@ __device__ __forceinline__ void load6(const LevelView& L, int q, double a[6]) {
 }
 
 // Red-black two-statement update of one cell (multigrid.cpp:61-63) on the ring.
-template <int NT>
-__device__ __forceinline__ void rb_update(double (*ring)[NT], int I, int tid, const double a[6]) {
-    double* row = ring[I & (kRing - 1)];
-    double x = a[5] / a[4];
+template <int NT, class T>
+__device__ __forceinline__ void rb_update(T (*ring)[NT], int I, int tid, const T a[6]) {
+    T* row = ring[I & (kRing - 1)];
+    T x = a[5] / a[4];
     x += (a[0] * row[tid + 1] + a[1] * row[tid - 1] + a[3] * ring[(I + 1) & (kRing - 1)][tid] +
           a[2] * ring[(I - 1) & (kRing - 1)][tid]) /
          a[4];
@@ -87,13 +90,13 @@ __device__ __forceinline__ void rb_update(double (*ring)[NT], int I, int tid, co
 
 // PRE red-black sweeps, residual and restriction in one streaming pass (see the file comment).
 // Each step prefetches the next step's coefficients into registers.
-template <int NT, int PRE>
+template <int NT, int PRE, class T>
 __global__ void __launch_bounds__(NT, 2)
-    k_mg_down(LevelView L, LevelView C, double* __restrict__ xout, int x_zero, int seg_rows,
+    k_mg_down(LevelViewT<T> L, LevelViewT<T> C, T* __restrict__ xout, int x_zero, int seg_rows,
               int HC) {
-    extern __shared__ double smem[];
-    double(*ring)[NT] = reinterpret_cast<double(*)[NT]>(smem);
-    const Win w = make_win<NT>(L, seg_rows, HC);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T(*ring)[NT] = reinterpret_cast<T(*)[NT]>(smem_raw);
+    const Win w = make_win<NT>(L.nx, L.ny, seg_rows, HC);
     const int tid = threadIdx.x;
     const int Jc = w.C0 + tid;
     const bool cload = Jc >= -1 && Jc <= L.ny;
@@ -104,9 +107,9 @@ __global__ void __launch_bounds__(NT, 2)
     int next = w.L0;
     auto issue = [&]() {
         if (next < w.L1 && cload) {
-            double* dst = &ring[next & (kRing - 1)][tid];
-            if (x_zero) *dst = 0.0;
-            else cp_async8(dst, L.x + next * s + Jc);
+            T* dst = &ring[next & (kRing - 1)][tid];
+            if (x_zero) *dst = T(0);
+            else cp_async(dst, L.x + next * s + Jc);
         }
         cp_async_commit();
         ++next;
@@ -127,21 +130,21 @@ __global__ void __launch_bounds__(NT, 2)
 
     int In[NC];
     bool okn[NC];
-    double an[NC][6];
+    T an[NC][6];
     cells(w.L0, In, okn);
 #pragma unroll
     for (int c = 0; c < NC; ++c)
         if (okn[c]) load6(L, In[c] * s + Jc, an[c]);
 
     const int t_last = w.R1 - 1 + 4 * PRE;
-    double r_prev = 0.0;
+    T r_prev = T(0);
     for (int t = w.L0; t <= t_last; ++t) {
         cp_async_wait<kPD>(); // rows <= t + 1 have landed
         __syncthreads();
         issue();
         int I[NC];
         bool ok[NC];
-        double a[NC][6];
+        T a[NC][6];
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
             I[c] = In[c];
@@ -159,10 +162,10 @@ __global__ void __launch_bounds__(NT, 2)
             if (ok[sw]) rb_update<NT>(ring, I[sw], tid, a[sw]);
         // Residual of row Ir = t - 4 PRE (multigrid.cpp:84-85): its neighbours are final.
         const int Ir = I[PRE];
-        double r = 0.0;
+        T r = T(0);
         if (ok[PRE]) {
-            const double* row = ring[Ir & (kRing - 1)];
-            const double* aa = a[PRE];
+            const T* row = ring[Ir & (kRing - 1)];
+            const T* aa = a[PRE];
             r = aa[5] - (aa[4] * row[tid] -
                          (aa[0] * row[tid + 1] + aa[1] * row[tid - 1] +
                           aa[3] * ring[(Ir + 1) & (kRing - 1)][tid] +
@@ -170,13 +173,13 @@ __global__ void __launch_bounds__(NT, 2)
         }
         // Restriction of the row pair (Ir - 1, Ir): C.b = r[f] + r[f+1] + r[f+fs] + r[f+fs+1].
         if ((Ir & 1) && Ir >= 1) { // uniform over the CTA
-            const double rp_odd = __shfl_down_sync(0xffffffffu, r_prev, 1);
-            const double r_odd = __shfl_down_sync(0xffffffffu, r, 1);
+            const T rp_odd = __shfl_down_sync(0xffffffffu, r_prev, 1);
+            const T r_odd = __shfl_down_sync(0xffffffffu, r, 1);
             const int R = Ir >> 1;
             if (cown && !(Jc & 1) && Ir - 1 >= w.R0 && Ir < w.R1 && R < C.nx) {
                 const int cq = R * C.stride + (Jc >> 1);
                 C.b[cq] = r_prev + rp_odd + r + r_odd;
-                C.x[cq] = 0.0;
+                C.x[cq] = T(0);
             }
         }
         r_prev = r;
@@ -188,23 +191,24 @@ __global__ void __launch_bounds__(NT, 2)
 }
 
 // Prolongation and POST red-black sweeps in one streaming pass (see the file comment).
-template <int NT, int POST>
+template <int NT, int POST, class T>
 __global__ void __launch_bounds__(NT, 2)
-    k_mg_up(LevelView C, LevelView L, const double* __restrict__ xin, double* __restrict__ xout,
+    k_mg_up(LevelViewT<T> C, LevelViewT<T> L, const T* __restrict__ xin, T* __restrict__ xout,
             double omega, int seg_rows, int HC) {
-    extern __shared__ double smem[];
-    double(*ring)[NT] = reinterpret_cast<double(*)[NT]>(smem);
-    const Win w = make_win<NT>(L, seg_rows, HC);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T(*ring)[NT] = reinterpret_cast<T(*)[NT]>(smem_raw);
+    const Win w = make_win<NT>(L.nx, L.ny, seg_rows, HC);
     const int tid = threadIdx.x;
     const int Jc = w.C0 + tid;
     const bool cload = Jc >= -1 && Jc <= L.ny;
     const bool cint = Jc >= 0 && Jc < L.ny;
     const bool cown = cint && Jc >= w.J0 && Jc < w.J0 + w.W;
     const int s = L.stride;
+    const T om = static_cast<T>(omega);
 
     int next = w.L0;
     auto issue = [&]() {
-        if (next < w.L1 && cload) cp_async8(&ring[next & (kRing - 1)][tid], xin + next * s + Jc);
+        if (next < w.L1 && cload) cp_async(&ring[next & (kRing - 1)][tid], xin + next * s + Jc);
         cp_async_commit();
         ++next;
     };
@@ -221,8 +225,7 @@ __global__ void __launch_bounds__(NT, 2)
     constexpr int NC = POST > 0 ? POST : 1;
     int In[NC];
     bool okn[NC];
-    double an[NC][6];
-    double cxn = 0.0; // coarse correction of the next row to prolong
+    T an[NC][6];
     const int t0 = w.L0 - 2;
     if (POST > 0) {
         cells(t0, In, okn);
@@ -233,9 +236,9 @@ __global__ void __launch_bounds__(NT, 2)
     auto coarse_at = [&](int Ip) {
         return (cint && Ip >= 0 && Ip < L.nx && Ip < w.L1)
                    ? __ldg(C.x + (Ip >> 1) * C.stride + (Jc >> 1))
-                   : 0.0;
+                   : T(0);
     };
-    cxn = coarse_at(t0 + 2);
+    T cxn = coarse_at(t0 + 2); // coarse correction of the next row to prolong
 
     const int t_last = w.R1 - 1 + 4 * POST;
     for (int t = t0; t <= t_last; ++t) {
@@ -245,7 +248,7 @@ __global__ void __launch_bounds__(NT, 2)
         if (t >= w.L0) issue();
         int I[NC];
         bool ok[NC];
-        double a[NC][6];
+        T a[NC][6];
         if (POST > 0) {
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
@@ -259,13 +262,13 @@ __global__ void __launch_bounds__(NT, 2)
             for (int c = 0; c < NC; ++c)
                 if (okn[c]) load6(L, In[c] * s + Jc, an[c]);
         }
-        const double cx = cxn;
+        const T cx = cxn;
         cxn = coarse_at(t + 3);
         // Prolongation of row t + 2 (read first at step t + 1): x += omega * coarse x.
         const int Ip = t + 2;
         if (cint && Ip >= 0 && Ip < L.nx && Ip < w.L1) {
-            double* cell = &ring[Ip & (kRing - 1)][tid];
-            *cell += omega * cx;
+            T* cell = &ring[Ip & (kRing - 1)][tid];
+            *cell += om * cx;
         }
 #pragma unroll
         for (int sw = 0; sw < POST; ++sw)
@@ -278,59 +281,58 @@ __global__ void __launch_bounds__(NT, 2)
 
 constexpr int kNT = 256;
 
-int seg_for(const LevelView& L, int HC, int sms) {
+int seg_for(int nx, int ny, int HC, int sms) {
     const int W = kNT - 2 * HC;
-    const int strips = (L.ny + W - 1) / W;
+    const int strips = (ny + W - 1) / W;
     const int want = (2 * sms) / strips > 0 ? (2 * sms) / strips : 1; // one wave, 2 CTAs per SM
-    int seg = (L.nx + want - 1) / want;
+    int seg = (nx + want - 1) / want;
     seg = (seg + 1) & ~1; // even: restriction pairs stay inside one CTA
     const int min_seg = 2 * HC + 8;
     if (seg < min_seg) seg = min_seg;
     return seg;
 }
 
-template <class K> void allow_smem(K kernel, bool& done) {
+template <class K> void allow_smem(K kernel, int bytes, bool& done) {
     if (!done) {
-        SGPU_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       kRing * kNT * static_cast<int>(sizeof(double))));
+        SGPU_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
         done = true;
     }
+}
+
+template <int PRE, class T>
+void down_t(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, bool x_zero, int sms,
+            cudaStream_t st) {
+    const int HC = 2 * PRE + 2;
+    const int seg = seg_for(F.nx, F.ny, HC, sms);
+    const int W = kNT - 2 * HC;
+    const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
+    constexpr int smem = kRing * kNT * static_cast<int>(sizeof(T));
+    static bool attr = false;
+    allow_smem(k_mg_down<kNT, PRE, T>, smem, attr);
+    k_mg_down<kNT, PRE, T><<<grid, kNT, smem, st>>>(F, C, xout, x_zero ? 1 : 0, seg, HC);
+    SGPU_LAUNCH();
+}
+
+template <int POST, class T>
+void up_t(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, T* xout, double omega,
+          int sms, cudaStream_t st) {
+    const int HC = 2 * POST + 2;
+    const int seg = seg_for(F.nx, F.ny, HC, sms);
+    const int W = kNT - 2 * HC;
+    const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
+    constexpr int smem = kRing * kNT * static_cast<int>(sizeof(T));
+    static bool attr = false;
+    allow_smem(k_mg_up<kNT, POST, T>, smem, attr);
+    k_mg_up<kNT, POST, T><<<grid, kNT, smem, st>>>(C, F, xin, xout, omega, seg, HC);
+    SGPU_LAUNCH();
 }
 
 } // namespace
 
 bool mg_fast_supported(int pre, int post) { return pre >= 1 && pre <= 4 && post >= 0 && post <= 4; }
 
-namespace {
-template <int PRE>
-void down_t(const LevelView& F, const LevelView& C, double* xout, bool x_zero, int sms,
-            cudaStream_t st) {
-    const int HC = 2 * PRE + 2;
-    const int seg = seg_for(F, HC, sms);
-    const int W = kNT - 2 * HC;
-    const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
-    static bool attr = false;
-    allow_smem(k_mg_down<kNT, PRE>, attr);
-    k_mg_down<kNT, PRE><<<grid, kNT, kRing * kNT * sizeof(double), st>>>(F, C, xout, x_zero ? 1 : 0,
-                                                                        seg, HC);
-    SGPU_LAUNCH();
-}
-template <int POST>
-void up_t(const LevelView& C, const LevelView& F, const double* xin, double* xout, double omega,
-          int sms, cudaStream_t st) {
-    const int HC = 2 * POST + 2;
-    const int seg = seg_for(F, HC, sms);
-    const int W = kNT - 2 * HC;
-    const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
-    static bool attr = false;
-    allow_smem(k_mg_up<kNT, POST>, attr);
-    k_mg_up<kNT, POST><<<grid, kNT, kRing * kNT * sizeof(double), st>>>(C, F, xin, xout, omega, seg,
-                                                                       HC);
-    SGPU_LAUNCH();
-}
-} // namespace
-
-void launch_mg_down(const LevelView& F, const LevelView& C, double* xout, int pre, bool x_zero,
+template <class T>
+void launch_mg_down(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, int pre, bool x_zero,
                     int sms, cudaStream_t st) {
     switch (pre) {
     case 1: down_t<1>(F, C, xout, x_zero, sms, st); break;
@@ -341,7 +343,8 @@ void launch_mg_down(const LevelView& F, const LevelView& C, double* xout, int pr
     }
 }
 
-void launch_mg_up(const LevelView& C, const LevelView& F, const double* xin, double* xout,
+template <class T>
+void launch_mg_up(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, T* xout,
                   double omega, int post, int sms, cudaStream_t st) {
     switch (post) {
     case 0: up_t<0>(C, F, xin, xout, omega, sms, st); break;
@@ -352,5 +355,14 @@ void launch_mg_up(const LevelView& C, const LevelView& F, const double* xin, dou
     default: throw Error(SGPU_E_INVALID, "streaming multigrid supports mg_post 0..4");
     }
 }
+
+template void launch_mg_down<double>(const LevelViewT<double>&, const LevelViewT<double>&, double*,
+                                     int, bool, int, cudaStream_t);
+template void launch_mg_down<float>(const LevelViewT<float>&, const LevelViewT<float>&, float*, int,
+                                    bool, int, cudaStream_t);
+template void launch_mg_up<double>(const LevelViewT<double>&, const LevelViewT<double>&,
+                                   const double*, double*, double, int, int, cudaStream_t);
+template void launch_mg_up<float>(const LevelViewT<float>&, const LevelViewT<float>&, const float*,
+                                  float*, double, int, int, cudaStream_t);
 
 } // namespace sgpu

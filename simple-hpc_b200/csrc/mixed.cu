@@ -1,0 +1,378 @@
+// mixed.cu — the mixed-precision outer iteration (config key precision = mixed).
+//
+// Defect correction around FP32 inner solves; everything SIMPLE's stability and stopping test
+// depend on stays FP64:
+//  * Momentum. The FP64 prep pass computes each cell's coefficients and the residual
+//    R = nb(u) + pressure term - AP u exactly as the FP64 path does (momentum_u.cpp:43-59), so
+//    res_u / res_v and their ordered sums are FP64. It also stores R and the 9 coefficients in
+//    FP32. The maxit_inner multicolour sweeps then run on the correction e = u_new - u in FP32:
+//    the reference's update u <- a (nb(u) + pt) / AP + (1 - a) u (momentum_u.cpp:136-137) is, for
+//    u = u0 + e, exactly e <- e + a (R(u0) + nb(e) - AP e) / AP, applied in the same colour order by
+//    the same time-skewed streaming kernel. The field update u += e is FP64.
+//  * Pressure correction. assemble_p (pressure.cpp:14-54) stays FP64 for b, its |b| sum (res_p)
+//    and its mean; the p' system's operator is stored in FP32 and solved by the FP32 V-cycle
+//    (mg_fast.cu / mg.cu, float instantiation). The mean of p' and the velocity / pressure
+//    correction (pressure.cpp:136-157) are FP64.
+// Fixed points are those of the FP64 iteration: when R and the continuity residual vanish, e and
+// p' vanish too, whatever their precision.
+#include "kernels.hpp"
+#include "stencil.cuh"
+
+namespace sgpu {
+
+namespace {
+
+__device__ __forceinline__ std::size_t ix(const DevParams& p, int i, int j) {
+    return static_cast<std::size_t>(i) * p.pitch + j;
+}
+
+template <class T> __device__ __forceinline__ void cp_async(T* smem, const T* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    if (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// FP64 prep over the update range: |R| for the ordered residual sum, AP (FP64, for assemble_p and
+// correct), R and the 9 coefficients in FP32 for the correction sweeps.
+template <bool V>
+__global__ void k_mom_prep_mixed(DevParams p, const double* __restrict__ x,
+                                 const double* __restrict__ oth, const double* __restrict__ pf,
+                                 double* __restrict__ AP, double* __restrict__ cells,
+                                 float* __restrict__ r32, Coef9Ptr32 c32, Range ur) {
+    const int j = ur.j0 + static_cast<int>(blockIdx.x * 32 + threadIdx.x);
+    const int i = ur.i0 + static_cast<int>(blockIdx.y * 8 + threadIdx.y);
+    if (i > ur.i1 || j > ur.j1) return;
+    const std::size_t q = ix(p, i, j), ld = p.pitch;
+    double ue, uw, vn, vs;
+    if (!V) {
+        ue = (x[q] + x[q + 1]) / 2;
+        uw = (x[q] + x[q - 1]) / 2;
+        vn = (oth[q] + oth[q + 1]) / 2;
+        vs = (oth[q + ld] + oth[q + ld + 1]) / 2;
+    } else {
+        ue = (oth[q - ld] + oth[q]) / 2;
+        uw = (oth[q - 1] + oth[q - ld - 1]) / 2;
+        vn = (x[q] + x[q - ld]) / 2;
+        vs = (x[q] + x[q + ld]) / 2;
+    }
+    const Coef9 c = momentum_coef(p, ue, uw, vn, vs, i, j);
+    const double nb = (c.AE * x[q + 1] + c.AW * x[q - 1] + c.AN * x[q - ld] + c.AS * x[q + ld]) +
+                      (c.AEE * x[q + 2] + c.AWW * x[q - 2] + c.ANN * x[q - 2 * ld] +
+                       c.ASS * x[q + 2 * ld]);
+    const double pt = V ? (pf[q] - pf[q - ld]) * p.dx : (pf[q] - pf[q + 1]) * p.dy;
+    const double R = nb + pt - c.AP * x[q];
+    cells[static_cast<std::size_t>(i - ur.i0) * ur.cols() + (j - ur.j0)] = fabs(R);
+    AP[q] = c.AP;
+    r32[q] = static_cast<float>(R);
+    c32.a[0][q] = static_cast<float>(c.AE);
+    c32.a[1][q] = static_cast<float>(c.AW);
+    c32.a[2][q] = static_cast<float>(c.AN);
+    c32.a[3][q] = static_cast<float>(c.AS);
+    c32.a[4][q] = static_cast<float>(c.AEE);
+    c32.a[5][q] = static_cast<float>(c.AWW);
+    c32.a[6][q] = static_cast<float>(c.ANN);
+    c32.a[7][q] = static_cast<float>(c.ASS);
+    c32.a[8][q] = static_cast<float>(c.AP);
+}
+
+constexpr int kRing = 32;
+constexpr int kPrefetch = 8;
+
+// One FP32 multicolour correction sweep e_in -> e_out with stored FP32 coefficients; the same
+// time-skewed streaming as k_mom_stream (fused.cu): cell (r, j) of colour c at step r + 2c, two
+// steps per barrier for five colours, strip halo 2 per colour. e_zero: e_in is all zero (first
+// sweep) and is not read.
+template <int NCOL, bool V, int NT>
+__global__ void __launch_bounds__(NT, 3)
+    k_corr_stream(DevParams p, const float* __restrict__ ein, float* __restrict__ eout,
+                  const float* __restrict__ r32, Coef9Ptr32 c32, int e_zero, int seg_rows) {
+    constexpr int SPB = NCOL == 5 ? 2 : 1;
+    constexpr int HC = 2 * NCOL;
+    constexpr int W = NT - 2 * HC;
+    constexpr int A = kPrefetch + SPB + 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float* ring_mem = reinterpret_cast<float*>(smem_raw);
+    __shared__ int s_rmin[NCOL], s_rmax[NCOL];
+    const int tid = threadIdx.x;
+    const int j0 = blockIdx.x * W;
+    const int C0 = j0 - HC, C1 = j0 + W + HC;
+    const int col = C0 + tid;
+    const int R0 = blockIdx.y * seg_rows;
+    const int R1 = min(R0 + seg_rows, p.nrows);
+    const int L0 = max(R0 - HC, 0), L1 = min(R1 + HC, p.nrows);
+    const int ld = p.pitch;
+    const bool col_in = col >= 0 && col < p.ncols;
+    const bool col_out = col_in && col >= j0 && col < j0 + W;
+    const int H = p.H;
+    if (tid < NCOL) {
+        const int c = tid;
+        int lo = V ? H + 1 : H, hi = p.NX + H - 1;
+        if (L0 > 0) lo = max(lo, L0 + 2 + 2 * c);
+        if (L1 < p.nrows) hi = min(hi, L1 - 3 - 2 * c);
+        s_rmin[c] = lo;
+        s_rmax[c] = hi;
+    }
+    unsigned colmask = 0;
+    {
+        const int ju0 = H + 1, ju1 = V ? p.NY + H : p.NY + H - 1;
+#pragma unroll
+        for (int c = 0; c < NCOL; ++c) {
+            bool ok = col >= ju0 && col <= ju1;
+            if (C0 > 0) ok = ok && col >= C0 + 2 + 2 * c;
+            if (C1 < p.ncols) ok = ok && col <= C1 - 3 - 2 * c;
+            colmask |= (ok ? 1u : 0u) << c;
+        }
+    }
+    const float relax = static_cast<float>(V ? p.av : p.au);
+    float* ringc = ring_mem + tid;
+    int next = L0;
+    auto issue = [&]() {
+        if (next < L1 && col_in) {
+            float* dst = ringc + (next & (kRing - 1)) * NT;
+            if (e_zero) *dst = 0.0f;
+            else cp_async(dst, ein + col + next * ld);
+        }
+        cp_async_commit();
+        ++next;
+    };
+    auto step_cell = [&](int c, int t, int& r) -> bool {
+        r = t - 2 * c;
+        return ((colmask >> c) & 1u) && r >= s_rmin[c] && r <= s_rmax[c];
+    };
+    // Inputs of one cell: AE AW AN AS AEE AWW ANN ASS AP, then R.
+    auto load_in = [&](int r, float a[10]) {
+        const int q = r * ld + col;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) a[k] = __ldg(c32.a[k] + q);
+        a[9] = __ldg(r32 + q);
+    };
+    auto update = [&](int r, const float a[10]) {
+        float* rc = ringc + (r & (kRing - 1)) * NT;
+        const float ee = rc[1], ew = rc[-1];
+        const float en = ringc[((r - 1) & (kRing - 1)) * NT];
+        const float es = ringc[((r + 1) & (kRing - 1)) * NT];
+        float nb = a[0] * ee + a[1] * ew + a[2] * en + a[3] * es;
+        if (NCOL == 5) {
+            const float eee = rc[2], eww = rc[-2];
+            const float enn = ringc[((r - 2) & (kRing - 1)) * NT];
+            const float ess = ringc[((r + 2) & (kRing - 1)) * NT];
+            nb += a[4] * eee + a[5] * eww + a[6] * enn + a[7] * ess;
+        }
+        const float e0 = rc[0];
+        rc[0] = e0 + relax * (a[9] + nb - a[8] * e0) / a[8];
+    };
+    auto next_colour = [&](int c, int steps) {
+        return NCOL == 5 ? (c + 2 * steps) % 5 : (c + steps) & 1;
+    };
+
+    for (int k = 0; k < A; ++k) issue();
+    __syncthreads();
+    const int c_start = NCOL == 5 ? (2 * L0 + col + 1000) % 5 : (L0 + col + 1000) & 1;
+    const int t_last = R1 + 2 * NCOL - 2 + (SPB - 1);
+    float in[SPB][10];
+    int rr[SPB];
+    bool okk[SPB];
+#pragma unroll
+    for (int s = 0; s < SPB; ++s) {
+        okk[s] = step_cell(next_colour(c_start, s), L0 + s, rr[s]);
+        if (okk[s]) load_in(rr[s], in[s]);
+    }
+    int c0 = c_start;
+    for (int t = L0; t <= t_last; t += SPB) {
+        cp_async_wait<kPrefetch>();
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < SPB; ++s) issue();
+        float cur[SPB][10];
+        int rc_[SPB];
+        bool okc[SPB];
+#pragma unroll
+        for (int s = 0; s < SPB; ++s) {
+            okc[s] = okk[s];
+            rc_[s] = rr[s];
+#pragma unroll
+            for (int m = 0; m < 10; ++m) cur[s][m] = in[s][m];
+        }
+        const int cn = next_colour(c0, SPB);
+#pragma unroll
+        for (int s = 0; s < SPB; ++s) {
+            okk[s] = step_cell(next_colour(cn, s), t + SPB + s, rr[s]);
+            if (okk[s]) load_in(rr[s], in[s]);
+        }
+#pragma unroll
+        for (int s = 0; s < SPB; ++s)
+            if (okc[s]) update(rc_[s], cur[s]);
+#pragma unroll
+        for (int s = 0; s < SPB; ++s) {
+            const int rw = t - 2 * NCOL + 1 - (SPB - 1) + s;
+            if (rw >= R0 && rw < R1 && col_out) eout[col + rw * ld] = ringc[(rw & (kRing - 1)) * NT];
+        }
+        c0 = cn;
+    }
+    cp_async_wait<0>();
+}
+
+// x += e over the update range (the FP64 field update).
+__global__ void k_add_correction(DevParams p, double* __restrict__ x, const float* __restrict__ e,
+                                 Range ur) {
+    const int j = ur.j0 + static_cast<int>(blockIdx.x * 32 + threadIdx.x);
+    const int i = ur.i0 + static_cast<int>(blockIdx.y * 8 + threadIdx.y);
+    if (i > ur.i1 || j > ur.j1) return;
+    const std::size_t q = ix(p, i, j);
+    x[q] += static_cast<double>(e[q]);
+}
+
+// assemble_p (pressure.cpp:14-54) in FP64 with the p' operator stored in FP32 (level 0 of the FP32
+// hierarchy) and |b|, b per cell for the ordered sums (res_p and the mean of b).
+__global__ void k_assemble_p_mixed(DevParams p, const double* __restrict__ APU,
+                                   const double* __restrict__ APV, const double* __restrict__ u,
+                                   const double* __restrict__ v, double* __restrict__ bfield,
+                                   LevelView32 L0, double* __restrict__ cabs,
+                                   double* __restrict__ cb) {
+    const int H = p.H;
+    const int J = static_cast<int>(blockIdx.x * 32 + threadIdx.x);
+    const int I = static_cast<int>(blockIdx.y * 8 + threadIdx.y);
+    if (I >= p.NX || J >= p.NY) return;
+    const int i = H + I, j = H + 1 + J;
+    const std::size_t q = ix(p, i, j), ld = p.pitch;
+    const double dx = p.dx, dy = p.dy;
+    const double aep = (j == p.NY + H) ? 0.0 : dy * dy / APU[q];
+    const double awp = (j == H + 1) ? 0.0 : dy * dy / APU[q - 1];
+    const double anp = (i == H) ? 0.0 : dx * dx / APV[q];
+    const double asp = (i == p.NX + H - 1) ? 0.0 : dx * dx / APV[q + ld];
+    const int lq = I * L0.stride + J;
+    L0.AE[lq] = static_cast<float>(aep);
+    L0.AW[lq] = static_cast<float>(awp);
+    L0.AN[lq] = static_cast<float>(anp);
+    L0.AS[lq] = static_cast<float>(asp);
+    L0.AP[lq] = static_cast<float>(aep + awp + anp + asp);
+    const double b = -dx * (-v[q + ld] + v[q]) - dy * (-u[q - 1] + u[q]);
+    bfield[q] = b;
+    const std::size_t c = static_cast<std::size_t>(I) * p.NY + J;
+    cabs[c] = fabs(b);
+    cb[c] = b;
+}
+
+// b32 = b - mean(b), rounded to FP32 (remove_mean0, multigrid.cpp:327-345, in FP64 first).
+__global__ void k_b_to_f32(DevParams p, const double* __restrict__ bfield, const double* __restrict__ sum_b,
+                           LevelView32 L0) {
+    const int J = static_cast<int>(blockIdx.x * 32 + threadIdx.x);
+    const int I = static_cast<int>(blockIdx.y * 8 + threadIdx.y);
+    if (I >= p.NX || J >= p.NY) return;
+    const double m = *sum_b / (static_cast<double>(p.NX) * p.NY);
+    L0.b[I * L0.stride + J] = static_cast<float>(bfield[ix(p, p.H + I, p.H + 1 + J)] - m);
+}
+
+// correct (pressure.cpp:136-157) in FP64 from the FP32 p' minus its FP64 mean; also stores that
+// p' in the FP64 pc field.
+__global__ void k_correct_mixed(DevParams p, const float* __restrict__ pc32, int ld32,
+                                const double* __restrict__ sum_pc, const double* __restrict__ APU,
+                                const double* __restrict__ APV, double* u, double* v, double* pf,
+                                double* pc64) {
+    const int J = static_cast<int>(blockIdx.x * 32 + threadIdx.x);
+    const int I = static_cast<int>(blockIdx.y * 8 + threadIdx.y);
+    if (I >= p.NX || J >= p.NY) return;
+    const int H = p.H, i = H + I, j = H + 1 + J;
+    const std::size_t q = ix(p, i, j);
+    const double m = *sum_pc / (static_cast<double>(p.NX) * p.NY);
+    const float* pcr = pc32 + I * ld32 + J; // level-0 p' at (I, J); neighbours inside its zero ring
+    const double pc = static_cast<double>(pcr[0]) - m;
+    if (j <= p.NY + H - 1) {
+        const double pce = static_cast<double>(pcr[1]) - m;
+        u[q] += p.dy * (pc - pce) / APU[q];
+    }
+    if (i >= H + 1) {
+        const double pcn = static_cast<double>(pcr[-ld32]) - m;
+        v[q] += p.dx * (pc - pcn) / APV[q];
+    }
+    pf[q] += p.ap * pc;
+    pc64[q] = pc;
+}
+
+template <int NCOL, bool V, int NT>
+void launch_corr(const DevParams& p, const float* ein, float* eout, const float* r32,
+                 const Coef9Ptr32& c32, bool e_zero, int seg_rows, cudaStream_t st) {
+    constexpr int W = NT - 4 * NCOL;
+    const dim3 grid((p.ncols + W - 1) / W, (p.nrows + seg_rows - 1) / seg_rows);
+    constexpr int smem = kRing * NT * static_cast<int>(sizeof(float));
+    k_corr_stream<NCOL, V, NT><<<grid, NT, smem, st>>>(p, ein, eout, r32, c32, e_zero ? 1 : 0, seg_rows);
+    SGPU_LAUNCH();
+}
+
+Range update_range(const DevParams& p, bool v) {
+    const int H = p.H;
+    return v ? Range{H + 1, p.NX + H - 1, H + 1, p.NY + H} : Range{H, p.NX + H - 1, H + 1, p.NY + H - 1};
+}
+
+} // namespace
+
+void launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x, const double* oth,
+                           const double* pf, double* AP, double* cells, float* r32,
+                           const Coef9Ptr32& c32, cudaStream_t st) {
+    const Range ur = update_range(p, v_component);
+    if (ur.rows() <= 0 || ur.cols() <= 0) return;
+    const dim3 grid((ur.cols() + 31) / 32, (ur.rows() + 7) / 8);
+    if (v_component) k_mom_prep_mixed<true><<<grid, dim3(32, 8), 0, st>>>(p, x, oth, pf, AP, cells, r32, c32, ur);
+    else k_mom_prep_mixed<false><<<grid, dim3(32, 8), 0, st>>>(p, x, oth, pf, AP, cells, r32, c32, ur);
+    SGPU_LAUNCH();
+}
+
+void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, float* eout,
+                       const float* r32, const Coef9Ptr32& c32, bool e_zero, int seg_rows,
+                       cudaStream_t st) {
+    if (p.ncol == 5) {
+        if (v_component) launch_corr<5, true, 256>(p, ein, eout, r32, c32, e_zero, seg_rows, st);
+        else launch_corr<5, false, 256>(p, ein, eout, r32, c32, e_zero, seg_rows, st);
+    } else {
+        if (v_component) launch_corr<2, true, 256>(p, ein, eout, r32, c32, e_zero, seg_rows, st);
+        else launch_corr<2, false, 256>(p, ein, eout, r32, c32, e_zero, seg_rows, st);
+    }
+}
+
+void launch_add_correction(const DevParams& p, bool v_component, double* x, const float* e,
+                           cudaStream_t st) {
+    const Range ur = update_range(p, v_component);
+    if (ur.rows() <= 0 || ur.cols() <= 0) return;
+    const dim3 grid((ur.cols() + 31) / 32, (ur.rows() + 7) / 8);
+    k_add_correction<<<grid, dim3(32, 8), 0, st>>>(p, x, e, ur);
+    SGPU_LAUNCH();
+}
+
+void launch_assemble_p_mixed(const DevParams& p, const double* APU, const double* APV,
+                             const double* u, const double* v, double* bfield,
+                             const LevelView32& L0, double* cabs, double* cb, cudaStream_t st) {
+    const dim3 grid((p.NY + 31) / 32, (p.NX + 7) / 8);
+    k_assemble_p_mixed<<<grid, dim3(32, 8), 0, st>>>(p, APU, APV, u, v, bfield, L0, cabs, cb);
+    SGPU_LAUNCH();
+}
+
+void launch_b_to_f32(const DevParams& p, const double* bfield, const double* sum_b,
+                     const LevelView32& L0, cudaStream_t st) {
+    const dim3 grid((p.NY + 31) / 32, (p.NX + 7) / 8);
+    k_b_to_f32<<<grid, dim3(32, 8), 0, st>>>(p, bfield, sum_b, L0);
+    SGPU_LAUNCH();
+}
+
+void launch_correct_mixed(const DevParams& p, const LevelView32& L0, const double* sum_pc,
+                          const double* APU, const double* APV, double* u, double* v, double* pf,
+                          double* pc64, cudaStream_t st) {
+    const dim3 grid((p.NY + 31) / 32, (p.NX + 7) / 8);
+    k_correct_mixed<<<grid, dim3(32, 8), 0, st>>>(p, L0.x, L0.stride, sum_pc, APU, APV, u, v, pf, pc64);
+    SGPU_LAUNCH();
+}
+
+void init_mixed_kernels() {
+    const int smem = kRing * 256 * static_cast<int>(sizeof(float));
+    SGPU_CUDA(cudaFuncSetAttribute(k_corr_stream<5, false, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    SGPU_CUDA(cudaFuncSetAttribute(k_corr_stream<5, true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    SGPU_CUDA(cudaFuncSetAttribute(k_corr_stream<2, false, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    SGPU_CUDA(cudaFuncSetAttribute(k_corr_stream<2, true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+}
+
+} // namespace sgpu

@@ -9,7 +9,8 @@
 // memory, filled by cp.async many tiles ahead; each lane then adds its row's 32 values of a tile in
 // column order. A tile costs a lane 32 shared loads and 32 adds for 32 rows' worth of data, so the
 // kernel is bound by the memory stream and the add latency, not by instruction issue. The last CTA
-// to finish adds the row sums in row order.
+// to finish adds the row sums in row order. Inputs may be FP64 or FP32 (widened to FP64 when
+// added); the sums are FP64.
 #include "kernels.hpp"
 
 namespace sgpu {
@@ -20,9 +21,12 @@ constexpr int kTile = 32;   // columns per tile (and rows per warp)
 constexpr int kStages = 12; // tiles in flight per warp
 constexpr int kPitch = kTile + 1; // padded tile row: lanes reading one column hit distinct banks
 
-__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+template <class T> __device__ __forceinline__ void cp_async(T* smem, const T* gmem) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+    if (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_async_wait() {
@@ -30,19 +34,20 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 }
 
 // One warp per CTA (32 rows); the grid covers ceil(nr / 32) x K planes.
+template <class TIn>
 __global__ void __launch_bounds__(32)
-    k_ordered_sum(const double* __restrict__ vals, std::size_t plane_stride, int ld, int nr, int nc,
+    k_ordered_sum(const TIn* __restrict__ vals, std::size_t plane_stride, int ld, int nr, int nc,
                   double* __restrict__ rows, unsigned int* counter, double* __restrict__ out,
                   const int* skip) {
     if (skip && *skip) return;
-    extern __shared__ double tile_mem[];
-    double(*tile)[kTile][kPitch] = reinterpret_cast<double(*)[kTile][kPitch]>(tile_mem);
+    extern __shared__ __align__(16) unsigned char tile_raw[];
+    TIn(*tile)[kTile][kPitch] = reinterpret_cast<TIn(*)[kTile][kPitch]>(tile_raw);
     __shared__ bool last_block;
     const int m = blockIdx.y;
     const int lane = threadIdx.x;
     const int r0 = blockIdx.x * kTile;
     const int nrow = min(kTile, nr - r0);
-    const double* src = vals + m * plane_stride + static_cast<std::size_t>(r0) * ld;
+    const TIn* src = vals + m * plane_stride + static_cast<std::size_t>(r0) * ld;
     const int ntiles = (nc + kTile - 1) / kTile;
 
     // Tile k: rows r0 .. r0 + 31, columns 32k .. 32k + 31; lane = column while loading.
@@ -51,7 +56,7 @@ __global__ void __launch_bounds__(32)
             const int c = k * kTile + lane;
             if (c < nc)
                 for (int rr = 0; rr < nrow; ++rr)
-                    cp_async8(&tile[k % kStages][rr][lane], src + static_cast<std::size_t>(rr) * ld + c);
+                    cp_async(&tile[k % kStages][rr][lane], src + static_cast<std::size_t>(rr) * ld + c);
         }
         cp_async_commit();
     };
@@ -63,12 +68,15 @@ __global__ void __launch_bounds__(32)
         cp_async_wait<kStages - 1>(); // tile k has landed (this lane's copies)
         __syncwarp();                 // ... and everyone's
         const int cnt = min(kTile, nc - k * kTile);
-        const double* t = tile[k % kStages][lane];
+        const TIn* t = tile[k % kStages][lane];
         if (cnt == kTile) {
+            double v[kTile];
 #pragma unroll
-            for (int c = 0; c < kTile; ++c) s += t[c];
+            for (int c = 0; c < kTile; ++c) v[c] = static_cast<double>(t[c]); // loads first
+#pragma unroll
+            for (int c = 0; c < kTile; ++c) s += v[c];
         } else {
-            for (int c = 0; c < cnt; ++c) s += t[c];
+            for (int c = 0; c < cnt; ++c) s += static_cast<double>(t[c]);
         }
         __syncwarp(); // the slot is refilled by the next issue
     }
@@ -94,10 +102,9 @@ __global__ void __launch_bounds__(32)
     if (lane == 0) *counter = 0u; // ready for the next launch on this stream
 }
 
-} // namespace
-
-void launch_ordered_sum(const double* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
-                        double* out, const SumScratch& s, const int* skip, cudaStream_t st) {
+template <class TIn>
+void launch_sum(const TIn* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
+                double* out, const SumScratch& s, const int* skip, cudaStream_t st) {
     if (K < 1 || K > 32 || K > s.max_k || nr > s.max_rows)
         throw Error(SGPU_E_INVALID, "ordered sum: sizes exceed the scratch");
     if (nr <= 0) {
@@ -105,14 +112,26 @@ void launch_ordered_sum(const double* vals, std::size_t plane_stride, int ld, in
         return;
     }
     const dim3 grid((nr + kTile - 1) / kTile, K);
-    constexpr int smem = kStages * kTile * kPitch * static_cast<int>(sizeof(double));
+    constexpr int smem = kStages * kTile * kPitch * static_cast<int>(sizeof(TIn));
     static bool attr = false; // per process
     if (!attr) {
-        SGPU_CUDA(cudaFuncSetAttribute(k_ordered_sum, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        SGPU_CUDA(cudaFuncSetAttribute(k_ordered_sum<TIn>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         attr = true;
     }
-    k_ordered_sum<<<grid, 32, smem, st>>>(vals, plane_stride, ld, nr, nc, s.rows, s.counter, out, skip);
+    k_ordered_sum<TIn><<<grid, 32, smem, st>>>(vals, plane_stride, ld, nr, nc, s.rows, s.counter, out, skip);
     SGPU_LAUNCH();
+}
+
+} // namespace
+
+void launch_ordered_sum(const double* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
+                        double* out, const SumScratch& s, const int* skip, cudaStream_t st) {
+    launch_sum(vals, plane_stride, ld, nr, nc, K, out, s, skip, st);
+}
+
+void launch_ordered_sum(const float* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
+                        double* out, const SumScratch& s, const int* skip, cudaStream_t st) {
+    launch_sum(vals, plane_stride, ld, nr, nc, K, out, s, skip, st);
 }
 
 } // namespace sgpu

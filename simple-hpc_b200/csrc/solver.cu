@@ -35,6 +35,11 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
+// Relative tolerance of the coarsest-level solve: the reference's kCoarseTol (multigrid.cpp:11)
+// in FP64; the FP32 V-cycle of the mixed-precision mode stops at a tolerance FP32 can reach.
+constexpr double kCoarseTol64 = 1e-10;
+constexpr double kCoarseTol32 = 1e-5;
+
 // Host evaluation of diffusive_coefficients (src/coefficients.cpp:41-63) for the two cell kinds.
 static void diffusive_host(const sgpu_params_t& p, bool band_or_order2, double out[9]) {
     const double dx = p.dx, dy = p.dy, nu = p.nu;
@@ -241,8 +246,69 @@ struct Solver {
 
     void iteration_enqueue(double* res3) {
         ev_n = 0;
-        if (fast) fast_iteration_enqueue(res3);
+        if (mixed) mixed_iteration_enqueue(res3);
+        else if (fast) fast_iteration_enqueue(res3);
         else outer_iteration_enqueue(res3);
+    }
+
+    // ---- mixed precision (precision = mixed): FP32 inner solves inside FP64 defect correction ----
+    bool mixed = false;
+    float* r32 = nullptr;             // momentum residual R in FP32
+    Coef9Ptr32 c32{};                 // momentum coefficients in FP32
+    float* e32[2] = {nullptr, nullptr}; // correction ping-pong
+    std::vector<LevelView32> lv32;    // FP32 multigrid hierarchy (level 0: the p' operator)
+    std::vector<float*> mg32_x2;
+    MgLevelsT<float> mgl32{};
+
+    void mixed_momentum(bool vcomp, double* res) {
+        double* x = vcomp ? v : u;
+        const double* oth = vcomp ? u : v;
+        double* AP = vcomp ? cv.a[8] : cu.a[8];
+        mark(vcomp ? SGPU_PH_BC_V : SGPU_PH_BC_U);
+        if (vcomp) launch_bc_v(dp, v, st);
+        else launch_bc_u(dp, u, st);
+        mark(vcomp ? SGPU_PH_ASSEMBLE_V : SGPU_PH_ASSEMBLE_U);
+        launch_mom_prep_mixed(dp, vcomp, x, oth, pf, AP, cells, r32, c32, st);
+        mark(vcomp ? SGPU_PH_RESIDUAL_V : SGPU_PH_RESIDUAL_U);
+        if (vcomp) launch_ordered_sum(cells, 0, prm.NY, prm.NX - 1, prm.NY, 1, res, ss, nullptr, st);
+        else launch_ordered_sum(cells, 0, prm.NY - 1, prm.NX, prm.NY - 1, 1, res, ss, nullptr, st);
+        mark(vcomp ? SGPU_PH_SWEEP_V : SGPU_PH_SWEEP_U);
+        const int n = vcomp ? prm.maxit_inner_v : prm.maxit_inner_u;
+        int cur = 0; // e32[cur] holds the current correction (zero before the first sweep)
+        for (int k = 0; k < n; ++k) {
+            launch_corr_sweep(dp, vcomp, e32[cur], e32[1 - cur], r32, c32, k == 0, seg_rows, st);
+            cur = 1 - cur;
+        }
+        if (n > 0) launch_add_correction(dp, vcomp, x, e32[cur], st);
+    }
+
+    void mixed_iteration_enqueue(double* res3) {
+        mixed_momentum(false, res3 + 0);
+        mixed_momentum(true, res3 + 1);
+        mark(SGPU_PH_ASSEMBLE_P);
+        launch_assemble_p_mixed(dp, cu.a[8], cv.a[8], u, v, w.b, lv32[0], cells, cells + plane, st);
+        launch_ordered_sum(cells, plane, prm.NY, prm.NX, prm.NY, 2, sums + 24, ss, nullptr, st);
+        SGPU_CUDA(cudaMemcpyAsync(res3 + 2, sums + 24, sizeof(double), cudaMemcpyDeviceToDevice, st));
+        mark(SGPU_PH_SOLVE_P);
+        for (std::size_t l = 1; l < lv32.size(); ++l) launch_mg_build<float>(lv32[l - 1], lv32[l], st);
+        launch_b_to_f32(dp, w.b, sums + 25, lv32[0], st);
+        const LevelView32& L0 = lv32[0];
+        SGPU_CUDA(cudaMemsetAsync(L0.x - (L0.stride + 1), 0,
+                                  sizeof(float) * (L0.nx + 2) * static_cast<std::size_t>(L0.stride), st));
+        for (int c = 0; c < prm.mg_cycles; ++c) {
+            for (int l = 0; l < mg_tail; ++l)
+                launch_mg_down<float>(lv32[l], lv32[l + 1], mg32_x2[l], prm.mg_pre, c == 0 || l > 0, sms, st);
+            launch_mg_tail<float>(mgl32, mg_tail, prm.mg_pre, prm.mg_post, prm.mg_omega, kCoarseTol32,
+                                  coarse_rowbuf, stats, st);
+            for (int l = mg_tail - 1; l >= 0; --l)
+                launch_mg_up<float>(lv32[l + 1], lv32[l], mg32_x2[l], lv32[l].x, prm.mg_omega,
+                                    prm.mg_post, sms, st);
+        }
+        launch_ordered_sum(L0.x, 0, L0.stride, L0.nx, L0.ny, 1, sums + 26, ss, nullptr, st);
+        mark(SGPU_PH_CORRECT);
+        launch_correct_mixed(dp, L0, sums + 26, cu.a[8], cv.a[8], u, v, pf, w.pc, st);
+        mark(SGPU_PH_COUNT);
+        last_vcycles = prm.mg_cycles;
     }
 
     void outer_iteration_enqueue(double* res3) {
@@ -436,6 +502,44 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
         for (int l = 0; l < nl && l < 24; ++l) mgl.L[l] = lv[l];
     }
 
+    if (p.precision == SGPU_PREC_MIXED) {
+        if (p.momentum_solver != SGPU_MOM_GS_MULTICOLOUR || p.pressure_solver != SGPU_P_MG ||
+            !mg_fast)
+            throw Error(SGPU_E_INVALID,
+                        "precision = mixed needs momentum_solver = gs_multicolour, pressure_solver = "
+                        "mg and 1 <= mg_pre <= 4, 0 <= mg_post <= 4");
+        mixed = true;
+        init_mixed_kernels();
+        r32 = dalloc<float>(g.elems());
+        for (int k = 0; k < 9; ++k) c32.a[k] = dalloc<float>(g.elems());
+        e32[0] = dalloc<float>(g.elems());
+        e32[1] = dalloc<float>(g.elems());
+        const int nl = static_cast<int>(lv.size());
+        lv32.resize(nl);
+        mg32_x2.assign(nl, nullptr);
+        for (int l = 0; l < nl; ++l) {
+            LevelView32& L = lv32[l];
+            L.nx = lv[l].nx;
+            L.ny = lv[l].ny;
+            L.stride = L.ny + 2;
+            const std::size_t n = static_cast<std::size_t>(L.nx + 2) * L.stride;
+            const std::size_t base = static_cast<std::size_t>(L.stride) + 1;
+            float* a[8];
+            for (int k = 0; k < 8; ++k) a[k] = dalloc<float>(n) + base;
+            L.AE = a[0];
+            L.AW = a[1];
+            L.AN = a[2];
+            L.AS = a[3];
+            L.AP = a[4];
+            L.b = a[5];
+            L.x = a[6];
+            L.r = a[7];
+            if (l < mg_tail) mg32_x2[l] = dalloc<float>(n) + base;
+        }
+        mgl32.n = nl;
+        for (int l = 0; l < nl && l < 24; ++l) mgl32.L[l] = lv32[l];
+    }
+
     if (hu) upload(u, hu);
     if (hv) upload(v, hv);
     if (hp) upload(pf, hp);
@@ -557,7 +661,7 @@ void Solver::mg_vcycle() {
         launch_mg_residual(lv[l], st);
         launch_mg_restrict(lv[l], lv[l + 1], st);
     }
-    launch_mg_coarse(lv[nl - 1], coarse_rowbuf, stats, st);
+    launch_mg_coarse(lv[nl - 1], coarse_rowbuf, kCoarseTol64, stats, st);
     for (int l = nl - 2; l >= 0; --l) {
         launch_mg_prolong(lv[l + 1], lv[l], prm.mg_omega, st);
         for (int s = 0; s < prm.mg_post; ++s) {
@@ -586,7 +690,8 @@ void Solver::mg_vcycle_fast(bool x_is_zero) {
     const int nl = static_cast<int>(lv.size());
     for (int l = 0; l < mg_tail; ++l)
         launch_mg_down(lv[l], lv[l + 1], mg_x2[l], prm.mg_pre, x_is_zero || l > 0, sms, st);
-    launch_mg_tail(mgl, mg_tail, prm.mg_pre, prm.mg_post, prm.mg_omega, coarse_rowbuf, stats, st);
+    launch_mg_tail(mgl, mg_tail, prm.mg_pre, prm.mg_post, prm.mg_omega, kCoarseTol64, coarse_rowbuf,
+                   stats, st);
     for (int l = mg_tail - 1; l >= 0; --l)
         launch_mg_up(lv[l + 1], lv[l], mg_x2[l], lv[l].x, prm.mg_omega, prm.mg_post, sms, st);
     (void)nl;

@@ -1,0 +1,95 @@
+"""Mixed precision (precision = mixed): FP32 inner solves inside FP64 defect correction.
+
+The mixed path is not bit-identical to the reference by design; these tests bound its distance from
+the FP64 oracle and check that it converges like the FP64 method:
+* the 32 x 32, Re 100, QUICK / 2, gs_multicolour + mg case (494 FP64 iterations to 1e-5) converges
+  in about as many iterations and to the FP64 fields within a small relative error;
+* fixed work on the 32 x 40 snapshot case stays close to the FP64 trajectory;
+* the residuals the stopping test reads are computed in FP64 (the first iteration's res_u and res_v,
+  which do not depend on any inner solve, are bit-identical to the oracle's).
+Errors are reported as max |a - b| / max |b| (relative to the field's scale) and L2 relative.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import config_text, cuda_available, load_golden, snapshot_config
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
+
+
+def rel_errors(a: np.ndarray, b: np.ndarray) -> tuple[float, float]:
+    scale = np.max(np.abs(b))
+    mx = float(np.max(np.abs(a - b)) / scale) if scale > 0 else float(np.max(np.abs(a - b)))
+    l2 = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    return mx, l2
+
+
+def test_mixed_converges_like_fp64(sgpu_mod):
+    g = load_golden("run_cavity32_re100_mc_mg.npz")
+    cfg = dict(g["config"])
+    cfg["precision"] = "mixed"
+    p = sgpu_mod.params_from_config(config_text(cfg))
+    with sgpu_mod.Solver(p) as s:
+        res, log = s.run(p.maxit)
+        fields = {k: s.download(f) for k, f in (("u", 0), ("v", 1), ("p", 2))}
+    n64 = g["log"].shape[0]
+    print(f"mixed: {res.iterations} iterations (FP64: {n64})")
+    assert res.converged
+    assert abs(res.iterations - n64) <= max(5, n64 // 50)
+    for k in ("u", "v", "p"):
+        mx, l2 = rel_errors(fields[k], g[k])
+        print(f"{k}: max rel {mx:.3e}, L2 rel {l2:.3e}")
+        assert mx < 1e-6 and l2 < 1e-6
+
+
+def test_mixed_fixed_work_close_to_fp64(sgpu_mod, oracle_mod):
+    cfg = snapshot_config("converged_32x40")
+    cfg.update(momentum_solver="gs_multicolour", pressure_solver="mg", error_tolerance="0",
+               maxit="60")
+    p64 = sgpu_mod.params_from_config(config_text(cfg))
+    o = oracle_mod.Oracle(p64)
+    _, _, olog = o.run(60)
+    cfg["precision"] = "mixed"
+    p = sgpu_mod.params_from_config(config_text(cfg))
+    with sgpu_mod.Solver(p) as s:
+        res, log = s.run(60)
+        fields = {k: s.download(f) for k, f in (("u", 0), ("v", 1), ("p", 2))}
+    # The first iteration's momentum residuals are computed before any inner solve: FP64, exact.
+    assert log[0, 1] == olog[0, 1] and log[0, 2] == olog[0, 2]
+    for k, f in (("u", 0), ("v", 1), ("p", 2)):
+        mx, l2 = rel_errors(fields[k], o.get(f))
+        print(f"{k}: max rel {mx:.3e}, L2 rel {l2:.3e}")
+        assert mx < 1e-6 and l2 < 1e-6
+    rel = np.abs(log[:, 1:] - olog[:, 1:]) / np.maximum(np.abs(olog[:, 1:]), 1e-300)
+    print(f"residual log max rel {rel.max():.3e}")
+    assert rel.max() < 1e-4
+
+
+@pytest.mark.parametrize("nx,ny,scheme,order", [(96, 160, "QUICK", 4), (130, 600, "UDS", 2)])
+def test_mixed_large_grids_close_to_fp64(sgpu_mod, nx, ny, scheme, order):
+    base = snapshot_config("short_16")
+    base.update(N_cells_x=str(nx), N_cells_y=str(ny), Re="1000", convection_scheme=scheme,
+                diffusion_order=str(order), momentum_solver="gs_multicolour", pressure_solver="mg",
+                maxit="20", error_tolerance="0")
+    p64 = sgpu_mod.params_from_config(config_text(base))
+    with sgpu_mod.Solver(p64) as s:
+        s.run(20)
+        ref = {f: s.download(f) for f in (0, 1, 2)}
+    base["precision"] = "mixed"
+    p = sgpu_mod.params_from_config(config_text(base))
+    with sgpu_mod.Solver(p) as s:
+        s.run(20)
+        for f in (0, 1, 2):
+            mx, l2 = rel_errors(s.download(f), ref[f])
+            print(f"field {f}: max rel {mx:.3e}, L2 rel {l2:.3e}")
+            assert mx < 1e-6 and l2 < 1e-6
+
+
+def test_mixed_rejects_other_solvers(sgpu_mod):
+    cfg = snapshot_config("short_16")
+    cfg.update(momentum_solver="gs_multicolour", pressure_solver="gs_redblack", precision="mixed")
+    with pytest.raises(sgpu_mod.SgpuError, match="precision = mixed needs"):
+        sgpu_mod.Solver(sgpu_mod.params_from_config(config_text(cfg)))

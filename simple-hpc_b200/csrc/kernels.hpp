@@ -125,18 +125,15 @@ void launch_cg_update(const DevParams& p, PressurePtr w, CgPtr cg, const CgScala
 void launch_cg_dir(const DevParams& p, CgPtr cg, const CgScalars* sc, cudaStream_t st);
 
 // ---- mixed precision (mixed.cu) ----
-struct Coef9Ptr32 {
-    float* a[9]; // AE AW AN AS AEE AWW ANN ASS AP
-};
 void init_mixed_kernels();
-// FP64 prep: |R| into cells, AP (FP64), R and the 9 coefficients in FP32, over the update range.
+// FP64 prep: |R| into cells, AP (FP64), and per cell a 48-byte FP32 record (3 float4:
+// AE AW AN AS | AEE AWW ANN ASS | 1/AP R 0 0) at rec + 3 * (i * pitch + j), over the update range.
 void launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x, const double* oth,
-                           const double* pf, double* AP, double* cells, float* r32,
-                           const Coef9Ptr32& c32, cudaStream_t st);
+                           const double* pf, double* AP, double* cells, float4* rec,
+                           cudaStream_t st);
 // One FP32 multicolour correction sweep e_in -> e_out (e_zero: e_in is zero and not read).
 void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, float* eout,
-                       const float* r32, const Coef9Ptr32& c32, bool e_zero, int seg_rows,
-                       cudaStream_t st);
+                       const float4* rec, bool e_zero, int seg_rows, cudaStream_t st);
 // x += e over the component's update range.
 void launch_add_correction(const DevParams& p, bool v_component, double* x, const float* e,
                            cudaStream_t st);

@@ -4,11 +4,12 @@
 // depend on stays FP64:
 //  * Momentum. The FP64 prep pass computes each cell's coefficients and the residual
 //    R = nb(u) + pressure term - AP u exactly as the FP64 path does (momentum_u.cpp:43-59), so
-//    res_u / res_v and their ordered sums are FP64. It also stores R and the 9 coefficients in
-//    FP32. The maxit_inner multicolour sweeps then run on the correction e = u_new - u in FP32:
-//    the reference's update u <- a (nb(u) + pt) / AP + (1 - a) u (momentum_u.cpp:136-137) is, for
-//    u = u0 + e, exactly e <- e + a (R(u0) + nb(e) - AP e) / AP, applied in the same colour order by
-//    the same time-skewed streaming kernel. The field update u += e is FP64.
+//    res_u / res_v and their ordered sums are FP64. It also stores, per cell, one 48-byte FP32
+//    record: the 8 neighbour coefficients, 1/AP and R. The maxit_inner multicolour sweeps then run
+//    on the correction e = u_new - u in FP32: the reference's update
+//    u <- a (nb(u) + pt) / AP + (1 - a) u (momentum_u.cpp:136-137) is, for u = u0 + e, exactly
+//    e <- e + a ((R(u0) + nb(e)) / AP - e), applied in the same colour order by the same
+//    time-skewed streaming scheme as the FP64 sweep. The field update u += e is FP64.
 //  * Pressure correction. assemble_p (pressure.cpp:14-54) stays FP64 for b, its |b| sum (res_p)
 //    and its mean; the p' system's operator is stored in FP32 and solved by the FP32 V-cycle
 //    (mg_fast.cu / mg.cu, float instantiation). The mean of p' and the velocity / pressure
@@ -39,12 +40,12 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 }
 
 // FP64 prep over the update range: |R| for the ordered residual sum, AP (FP64, for assemble_p and
-// correct), R and the 9 coefficients in FP32 for the correction sweeps.
+// correct), and the cell's FP32 record {AE AW AN AS | AEE AWW ANN ASS | 1/AP R 0 0}.
 template <bool V>
 __global__ void k_mom_prep_mixed(DevParams p, const double* __restrict__ x,
                                  const double* __restrict__ oth, const double* __restrict__ pf,
                                  double* __restrict__ AP, double* __restrict__ cells,
-                                 float* __restrict__ r32, Coef9Ptr32 c32, Range ur) {
+                                 float4* __restrict__ rec, Range ur) {
     const int j = ur.j0 + static_cast<int>(blockIdx.x * 32 + threadIdx.x);
     const int i = ur.i0 + static_cast<int>(blockIdx.y * 8 + threadIdx.y);
     if (i > ur.i1 || j > ur.j1) return;
@@ -69,29 +70,29 @@ __global__ void k_mom_prep_mixed(DevParams p, const double* __restrict__ x,
     const double R = nb + pt - c.AP * x[q];
     cells[static_cast<std::size_t>(i - ur.i0) * ur.cols() + (j - ur.j0)] = fabs(R);
     AP[q] = c.AP;
-    r32[q] = static_cast<float>(R);
-    c32.a[0][q] = static_cast<float>(c.AE);
-    c32.a[1][q] = static_cast<float>(c.AW);
-    c32.a[2][q] = static_cast<float>(c.AN);
-    c32.a[3][q] = static_cast<float>(c.AS);
-    c32.a[4][q] = static_cast<float>(c.AEE);
-    c32.a[5][q] = static_cast<float>(c.AWW);
-    c32.a[6][q] = static_cast<float>(c.ANN);
-    c32.a[7][q] = static_cast<float>(c.ASS);
-    c32.a[8][q] = static_cast<float>(c.AP);
+    float4* r = rec + 3 * q;
+    r[0] = make_float4(static_cast<float>(c.AE), static_cast<float>(c.AW), static_cast<float>(c.AN),
+                       static_cast<float>(c.AS));
+    r[1] = make_float4(static_cast<float>(c.AEE), static_cast<float>(c.AWW),
+                       static_cast<float>(c.ANN), static_cast<float>(c.ASS));
+    r[2] = make_float4(static_cast<float>(1.0 / c.AP), static_cast<float>(R), 0.0f, 0.0f);
 }
 
 constexpr int kRing = 32;
 constexpr int kPrefetch = 8;
 
-// One FP32 multicolour correction sweep e_in -> e_out with stored FP32 coefficients; the same
-// time-skewed streaming as k_mom_stream (fused.cu): cell (r, j) of colour c at step r + 2c, two
-// steps per barrier for five colours, strip halo 2 per colour. e_zero: e_in is all zero (first
-// sweep) and is not read.
+struct Rec {
+    float4 a, b, c;
+};
+
+// One FP32 multicolour correction sweep e_in -> e_out from the stored records; the time-skewed
+// streaming of k_mom_stream (fused.cu): cell (r, j) of colour c at step r + 2c, two steps per
+// barrier for five colours, strip halo 2 per colour. The next super-step's records are loaded one
+// super-step ahead into the other of two register sets. e_zero: e_in is zero and is not read.
 template <int NCOL, bool V, int NT>
 __global__ void __launch_bounds__(NT, 3)
     k_corr_stream(DevParams p, const float* __restrict__ ein, float* __restrict__ eout,
-                  const float* __restrict__ r32, Coef9Ptr32 c32, int e_zero, int seg_rows) {
+                  const float4* __restrict__ rec, int e_zero, int seg_rows) {
     constexpr int SPB = NCOL == 5 ? 2 : 1;
     constexpr int HC = 2 * NCOL;
     constexpr int W = NT - 2 * HC;
@@ -131,6 +132,7 @@ __global__ void __launch_bounds__(NT, 3)
     }
     const float relax = static_cast<float>(V ? p.av : p.au);
     float* ringc = ring_mem + tid;
+    const float4* recc = rec + 3 * col;
     int next = L0;
     auto issue = [&]() {
         if (next < L1 && col_in) {
@@ -145,27 +147,26 @@ __global__ void __launch_bounds__(NT, 3)
         r = t - 2 * c;
         return ((colmask >> c) & 1u) && r >= s_rmin[c] && r <= s_rmax[c];
     };
-    // Inputs of one cell: AE AW AN AS AEE AWW ANN ASS AP, then R.
-    auto load_in = [&](int r, float a[10]) {
-        const int q = r * ld + col;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) a[k] = __ldg(c32.a[k] + q);
-        a[9] = __ldg(r32 + q);
+    auto load_rec = [&](int r, Rec& x) {
+        const float4* q = recc + 3 * r * ld;
+        x.a = __ldg(q);
+        x.b = __ldg(q + 1);
+        x.c = __ldg(q + 2);
     };
-    auto update = [&](int r, const float a[10]) {
+    auto update = [&](int r, const Rec& x) {
         float* rc = ringc + (r & (kRing - 1)) * NT;
         const float ee = rc[1], ew = rc[-1];
         const float en = ringc[((r - 1) & (kRing - 1)) * NT];
         const float es = ringc[((r + 1) & (kRing - 1)) * NT];
-        float nb = a[0] * ee + a[1] * ew + a[2] * en + a[3] * es;
+        float nb = x.a.x * ee + x.a.y * ew + x.a.z * en + x.a.w * es;
         if (NCOL == 5) {
             const float eee = rc[2], eww = rc[-2];
             const float enn = ringc[((r - 2) & (kRing - 1)) * NT];
             const float ess = ringc[((r + 2) & (kRing - 1)) * NT];
-            nb += a[4] * eee + a[5] * eww + a[6] * enn + a[7] * ess;
+            nb += x.b.x * eee + x.b.y * eww + x.b.z * enn + x.b.w * ess;
         }
         const float e0 = rc[0];
-        rc[0] = e0 + relax * (a[9] + nb - a[8] * e0) / a[8];
+        rc[0] = e0 + relax * ((x.c.y + nb) * x.c.x - e0);
     };
     auto next_colour = [&](int c, int steps) {
         return NCOL == 5 ? (c + 2 * steps) % 5 : (c + steps) & 1;
@@ -175,45 +176,42 @@ __global__ void __launch_bounds__(NT, 3)
     __syncthreads();
     const int c_start = NCOL == 5 ? (2 * L0 + col + 1000) % 5 : (L0 + col + 1000) & 1;
     const int t_last = R1 + 2 * NCOL - 2 + (SPB - 1);
-    float in[SPB][10];
-    int rr[SPB];
-    bool okk[SPB];
+
+    Rec bufA[SPB], bufB[SPB];
+    int rA[SPB], rB[SPB];
+    bool okA[SPB], okB[SPB];
 #pragma unroll
     for (int s = 0; s < SPB; ++s) {
-        okk[s] = step_cell(next_colour(c_start, s), L0 + s, rr[s]);
-        if (okk[s]) load_in(rr[s], in[s]);
+        okA[s] = step_cell(next_colour(c_start, s), L0 + s, rA[s]);
+        if (okA[s]) load_rec(rA[s], bufA[s]);
     }
-    int c0 = c_start;
-    for (int t = L0; t <= t_last; t += SPB) {
+    auto super_step = [&](int t, int c0, const Rec (&cur)[SPB], const int (&rcur)[SPB],
+                          const bool (&okcur)[SPB], Rec (&nxt)[SPB], int (&rnxt)[SPB],
+                          bool (&oknxt)[SPB]) {
         cp_async_wait<kPrefetch>();
         __syncthreads();
 #pragma unroll
         for (int s = 0; s < SPB; ++s) issue();
-        float cur[SPB][10];
-        int rc_[SPB];
-        bool okc[SPB];
-#pragma unroll
-        for (int s = 0; s < SPB; ++s) {
-            okc[s] = okk[s];
-            rc_[s] = rr[s];
-#pragma unroll
-            for (int m = 0; m < 10; ++m) cur[s][m] = in[s][m];
-        }
         const int cn = next_colour(c0, SPB);
 #pragma unroll
         for (int s = 0; s < SPB; ++s) {
-            okk[s] = step_cell(next_colour(cn, s), t + SPB + s, rr[s]);
-            if (okk[s]) load_in(rr[s], in[s]);
+            oknxt[s] = step_cell(next_colour(cn, s), t + SPB + s, rnxt[s]);
+            if (oknxt[s]) load_rec(rnxt[s], nxt[s]);
         }
 #pragma unroll
         for (int s = 0; s < SPB; ++s)
-            if (okc[s]) update(rc_[s], cur[s]);
+            if (okcur[s]) update(rcur[s], cur[s]);
 #pragma unroll
         for (int s = 0; s < SPB; ++s) {
             const int rw = t - 2 * NCOL + 1 - (SPB - 1) + s;
             if (rw >= R0 && rw < R1 && col_out) eout[col + rw * ld] = ringc[(rw & (kRing - 1)) * NT];
         }
-        c0 = cn;
+        return cn;
+    };
+    int c0 = c_start;
+    for (int t = L0; t <= t_last; t += 2 * SPB) {
+        c0 = super_step(t, c0, bufA, rA, okA, bufB, rB, okB);
+        if (t + SPB <= t_last) c0 = super_step(t + SPB, c0, bufB, rB, okB, bufA, rA, okA);
     }
     cp_async_wait<0>();
 }
@@ -296,12 +294,12 @@ __global__ void k_correct_mixed(DevParams p, const float* __restrict__ pc32, int
 }
 
 template <int NCOL, bool V, int NT>
-void launch_corr(const DevParams& p, const float* ein, float* eout, const float* r32,
-                 const Coef9Ptr32& c32, bool e_zero, int seg_rows, cudaStream_t st) {
+void launch_corr(const DevParams& p, const float* ein, float* eout, const float4* rec, bool e_zero,
+                 int seg_rows, cudaStream_t st) {
     constexpr int W = NT - 4 * NCOL;
     const dim3 grid((p.ncols + W - 1) / W, (p.nrows + seg_rows - 1) / seg_rows);
     constexpr int smem = kRing * NT * static_cast<int>(sizeof(float));
-    k_corr_stream<NCOL, V, NT><<<grid, NT, smem, st>>>(p, ein, eout, r32, c32, e_zero ? 1 : 0, seg_rows);
+    k_corr_stream<NCOL, V, NT><<<grid, NT, smem, st>>>(p, ein, eout, rec, e_zero ? 1 : 0, seg_rows);
     SGPU_LAUNCH();
 }
 
@@ -313,25 +311,24 @@ Range update_range(const DevParams& p, bool v) {
 } // namespace
 
 void launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x, const double* oth,
-                           const double* pf, double* AP, double* cells, float* r32,
-                           const Coef9Ptr32& c32, cudaStream_t st) {
+                           const double* pf, double* AP, double* cells, float4* rec,
+                           cudaStream_t st) {
     const Range ur = update_range(p, v_component);
     if (ur.rows() <= 0 || ur.cols() <= 0) return;
     const dim3 grid((ur.cols() + 31) / 32, (ur.rows() + 7) / 8);
-    if (v_component) k_mom_prep_mixed<true><<<grid, dim3(32, 8), 0, st>>>(p, x, oth, pf, AP, cells, r32, c32, ur);
-    else k_mom_prep_mixed<false><<<grid, dim3(32, 8), 0, st>>>(p, x, oth, pf, AP, cells, r32, c32, ur);
+    if (v_component) k_mom_prep_mixed<true><<<grid, dim3(32, 8), 0, st>>>(p, x, oth, pf, AP, cells, rec, ur);
+    else k_mom_prep_mixed<false><<<grid, dim3(32, 8), 0, st>>>(p, x, oth, pf, AP, cells, rec, ur);
     SGPU_LAUNCH();
 }
 
 void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, float* eout,
-                       const float* r32, const Coef9Ptr32& c32, bool e_zero, int seg_rows,
-                       cudaStream_t st) {
+                       const float4* rec, bool e_zero, int seg_rows, cudaStream_t st) {
     if (p.ncol == 5) {
-        if (v_component) launch_corr<5, true, 256>(p, ein, eout, r32, c32, e_zero, seg_rows, st);
-        else launch_corr<5, false, 256>(p, ein, eout, r32, c32, e_zero, seg_rows, st);
+        if (v_component) launch_corr<5, true, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
+        else launch_corr<5, false, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
     } else {
-        if (v_component) launch_corr<2, true, 256>(p, ein, eout, r32, c32, e_zero, seg_rows, st);
-        else launch_corr<2, false, 256>(p, ein, eout, r32, c32, e_zero, seg_rows, st);
+        if (v_component) launch_corr<2, true, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
+        else launch_corr<2, false, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
     }
 }
 

@@ -253,8 +253,7 @@ struct Solver {
 
     // ---- mixed precision (precision = mixed): FP32 inner solves inside FP64 defect correction ----
     bool mixed = false;
-    float* r32 = nullptr;             // momentum residual R in FP32
-    Coef9Ptr32 c32{};                 // momentum coefficients in FP32
+    float4* rec32 = nullptr;          // per-cell FP32 records: coefficients, 1/AP, R
     float* e32[2] = {nullptr, nullptr}; // correction ping-pong
     std::vector<LevelView32> lv32;    // FP32 multigrid hierarchy (level 0: the p' operator)
     std::vector<float*> mg32_x2;
@@ -268,7 +267,7 @@ struct Solver {
         if (vcomp) launch_bc_v(dp, v, st);
         else launch_bc_u(dp, u, st);
         mark(vcomp ? SGPU_PH_ASSEMBLE_V : SGPU_PH_ASSEMBLE_U);
-        launch_mom_prep_mixed(dp, vcomp, x, oth, pf, AP, cells, r32, c32, st);
+        launch_mom_prep_mixed(dp, vcomp, x, oth, pf, AP, cells, rec32, st);
         mark(vcomp ? SGPU_PH_RESIDUAL_V : SGPU_PH_RESIDUAL_U);
         if (vcomp) launch_ordered_sum(cells, 0, prm.NY, prm.NX - 1, prm.NY, 1, res, ss, nullptr, st);
         else launch_ordered_sum(cells, 0, prm.NY - 1, prm.NX, prm.NY - 1, 1, res, ss, nullptr, st);
@@ -276,7 +275,7 @@ struct Solver {
         const int n = vcomp ? prm.maxit_inner_v : prm.maxit_inner_u;
         int cur = 0; // e32[cur] holds the current correction (zero before the first sweep)
         for (int k = 0; k < n; ++k) {
-            launch_corr_sweep(dp, vcomp, e32[cur], e32[1 - cur], r32, c32, k == 0, seg_rows, st);
+            launch_corr_sweep(dp, vcomp, e32[cur], e32[1 - cur], rec32, k == 0, seg_rows, st);
             cur = 1 - cur;
         }
         if (n > 0) launch_add_correction(dp, vcomp, x, e32[cur], st);
@@ -510,8 +509,7 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
                         "mg and 1 <= mg_pre <= 4, 0 <= mg_post <= 4");
         mixed = true;
         init_mixed_kernels();
-        r32 = dalloc<float>(g.elems());
-        for (int k = 0; k < 9; ++k) c32.a[k] = dalloc<float>(g.elems());
+        rec32 = dalloc<float4>(3 * g.elems());
         e32[0] = dalloc<float>(g.elems());
         e32[1] = dalloc<float>(g.elems());
         const int nl = static_cast<int>(lv.size());

@@ -6,6 +6,10 @@ time-to-1e-5 metric is quoted on. Time to 1e-5 = (outer iterations to 1e-5) / (o
 second); the benchmark measures the second factor, a step being one SIMPLE outer iteration. Inputs
 are the cavity's own initial state (u = v = p = 0, lid u = 1), so the data are synthetic by nature.
 
+The headline arm is the mixed-precision solve (FP32 inner solves inside FP64 defect correction,
+precision = mixed); the plain FP64 GPU solve (bit-identical to the reference) is timed in the same
+run on the same K steps, and the line reports both and their ratio.
+
 Output: one JSON line (rank 0). ``value`` is device-timed throughput with the fields resident in HBM;
 ``e2e`` is the same metric through the C ABI from pinned host buffers (initial fields uploaded, every
 iteration's residuals read back for the stopping test, final fields downloaded); ``roofline`` covers
@@ -23,19 +27,16 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 from pathlib import Path
-
-import numpy as np
 
 REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO / "simple-hpc_b200"))
 sys.path.insert(0, str(REPO / "oracle"))
 
-METRIC = "SIMPLE outer iterations per second, cavity 4096x4096 Re1000 QUICK/4 (time-to-1e-5 = iterations / this)"
+METRIC = ("SIMPLE outer iterations per second, cavity 4096x4096 Re1000 QUICK/4 gs_multicolour+mg "
+          "(time-to-1e-5 = iterations / this)")
 UNIT = "outer_iterations/s"
 
 
@@ -87,44 +88,61 @@ def allmax(x: float, world: int) -> float:
 # ---- clocks during the timed region ----
 
 class Clocks:
-    def __init__(self, index: int):
-        self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and throttle reasons of this process's GPU, sampled every 10 ms by an NVML thread
+    while the timed region runs (read-only queries). The GPU is found by its UUID, so the sample is
+    of the same device under CUDA_VISIBLE_DEVICES."""
+
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
+
+    def __init__(self, index: int, period: float = 0.01):
+        import threading
+        self.sm, self.smax, self.reasons, self.err = [], [], set(), None
+        self._stop = threading.Event()
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(index).uuid)
+            self.h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            self.nv = pynvml
+            self.smax.append(float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)))
+        except Exception as e:  # no NVML: the line says so
+            self.h, self.err = None, f"nvml unavailable: {type(e).__name__}: {e}"
+            return
+        self.period = period
+        self._sample()
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+
+    def _sample(self):
+        nv = self.nv
+        self.sm.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+        mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        for name, bit in self.REASONS.items():
+            if mask & bit:
+                self.reasons.add(name)
+
+    def _run(self):
+        while not self._stop.wait(self.period):
+            try:
+                self._sample()
+            except Exception as e:
+                self.err = f"{type(e).__name__}: {e}"
+                return
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.path.read_text().splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
-            except ValueError:
-                continue
-            for name, val in zip(names, f[5:9]):
-                if val.lower() == "active":
-                    reasons.add(name)
-        self.path.unlink(missing_ok=True)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None, "samples": len(sm),
-                "reasons": sorted(reasons)}
+        if self.h is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "samples": 0, "reasons": [self.err]}
+        self._stop.set()
+        self.t.join(timeout=2)
+        self._sample()
+        out = {"sm_mhz": statistics.median(self.sm), "sm_min_mhz": min(self.sm),
+               "sm_max_mhz": max(self.smax), "samples": len(self.sm), "reasons": sorted(self.reasons),
+               "source": "NVML, every 10 ms during the timed region"}
+        if self.err:
+            out["error"] = self.err
+        return out
 
 
 def measured_peaks() -> dict:
@@ -196,6 +214,61 @@ def cpu_baseline(n: int, seconds_budget: float) -> dict:
 
 # ---- GPU arm ----
 
+def measure(sgpu, torch, n: int, precision: str, steps: int, warmup: int, world: int, local: int,
+            clocks: bool) -> dict:
+    """Device-timed K outer iterations (fields resident in HBM), per-phase times, launch count."""
+    p = sgpu.params_from_config(workload_config(n, precision))
+    solver = sgpu.Solver(p)
+    stream = torch.cuda.ExternalStream(solver.stream())
+    for _ in range(warmup):
+        solver.outer_iteration()
+    solver.set_profiling(True)
+    ph0 = solver.phase_seconds()
+    launches0 = sgpu.launch_count()
+    clk = Clocks(local) if clocks else None
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    res, _ = solver.run(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk_info = clk.stop() if clk else None
+    launches = sgpu.launch_count() - launches0
+    ph1 = solver.phase_seconds()
+    solver.close()
+    secs = allmax(e0.elapsed_time(e1) * 1e-3, world)
+    iters = res.iterations
+    return {"p": p, "iters": iters, "secs": secs, "value": world * iters / secs,
+            "ms_per_step": 1e3 * secs / max(iters, 1), "launches": launches, "clocks": clk_info,
+            "phases": {k: (ph1[k] - ph0[k]) for k in ph1 if k != "output"},
+            "converged": bool(res.converged)}
+
+
+def e2e_measure(sgpu, torch, p, steps: int, world: int) -> dict:
+    """The same K iterations through the C ABI from pinned host buffers, copies included."""
+    shape = (p.nrows, p.ncols)
+    pinned = [torch.zeros(shape, dtype=torch.float64).pin_memory() for _ in range(3)]
+    hu, hv, hp = (t.numpy() for t in pinned)
+    solver = sgpu.Solver(p)  # allocation outside the timed region
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    solver.upload(sgpu.F_U, hu)
+    solver.upload(sgpu.F_V, hv)
+    solver.upload(sgpu.F_P, hp)
+    res, _ = solver.run(steps)
+    for f in (sgpu.F_U, sgpu.F_V, sgpu.F_P):
+        solver.download(f)
+    t = allmax(time.perf_counter() - t0, world)
+    solver.close()
+    fb = 8 * p.nrows * p.ncols
+    return {"value": world * res.iterations / t, "unit": UNIT,
+            "h2d_bytes_per_step": 3 * fb / res.iterations,
+            "d2h_bytes_per_step": 24 + 3 * fb / res.iterations}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -203,9 +276,10 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=4096)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-arm", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -221,102 +295,63 @@ def main() -> None:
 
     torch.cuda.set_device(local)
     n = args.size
-    p = sgpu.params_from_config(workload_config(n, args.precision))
-    solver = sgpu.Solver(p)
-    stream = torch.cuda.ExternalStream(solver.stream())
+    head = measure(sgpu, torch, n, args.precision, args.steps, args.warmup, world, local, True)
+    p = head["p"]
+    plain = None
+    if args.precision != "fp64" and not args.no_fp64_arm:
+        plain = measure(sgpu, torch, n, "fp64", args.steps, args.warmup, world, local, False)
 
-    # warm-up (untimed)
-    for _ in range(args.warmup):
-        solver.outer_iteration()
-
-    # ---- device-timed region: K outer iterations, fields resident in HBM ----
-    solver.set_profiling(True)
-    ph0 = solver.phase_seconds()
-    launches0 = sgpu.launch_count()
-    clocks = Clocks(local)
-    barrier(world)
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    res, log = solver.run(args.steps)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier(world)
-    clk = clocks.stop()
-    launches = sgpu.launch_count() - launches0
-    ph1 = solver.phase_seconds()
-    solver.set_profiling(False)
-    secs = e0.elapsed_time(e1) * 1e-3
-    secs_max = allmax(secs, world)
-    iters = res.iterations
-    value = world * iters / secs_max
-
-    # ---- roofline of the dominant kernel (the streaming sweep, 2 x maxit_inner launches) ----
-    sweep_s = (ph1["sweep_u"] - ph0["sweep_u"]) + (ph1["sweep_v"] - ph0["sweep_v"])
-    sweep_launches = iters * (p.maxit_inner_u + p.maxit_inner_v)
+    # Roofline of the dominant kernel: the streaming sweep (2 x maxit_inner launches per step).
+    ph = head["phases"]
+    sweep_s = ph["sweep_u"] + ph["sweep_v"]
+    sweep_launches = head["iters"] * (p.maxit_inner_u + p.maxit_inner_v)
     cells = p.nrows * p.ncols
-    bytes_per_launch = 5 * 8 * cells  # read x_in, frozen x, other velocity, p; write x_out
+    if args.precision == "mixed":
+        kernel = "k_corr_stream (one FP32 multicolour correction sweep)"
+        bytes_per_cell = 48 + 4 + 4  # record read, e_in read, e_out written
+    else:
+        kernel = "k_mom_stream (one FP64 multicolour sweep)"
+        bytes_per_cell = 5 * 8  # x_in, frozen x, other velocity, p read; x_out written
+    bytes_per_launch = bytes_per_cell * cells
     per_launch_s = sweep_s / max(sweep_launches, 1)
     peaks = measured_peaks()
     achieved = bytes_per_launch / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
     traffic = None
     prof = REPO / "profiles" / "sweep_traffic.json"
     if prof.exists():
-        t = json.loads(prof.read_text())
-        traffic = t.get("bytes_per_cell", 0) * cells if t.get("bytes_per_cell") else None
+        t = json.loads(prof.read_text()).get(args.precision, {})
+        if t.get("bytes_per_cell"):
+            traffic = t["bytes_per_cell"] * cells
 
-    phases_ms = {k: 1e3 * (ph1[k] - ph0[k]) / max(iters, 1) for k in ph1 if k != "output"}
-
-    # ---- end to end through the C ABI from pinned host memory ----
-    e2e = None
-    if rank == 0 or world > 1:
-        shape = (p.nrows, p.ncols)
-        pinned = [torch.zeros(shape, dtype=torch.float64).pin_memory() for _ in range(3)]
-        hu, hv, hp = (t.numpy() for t in pinned)
-        solver2 = sgpu.Solver(p)  # allocation outside the timed region
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        solver2.upload(sgpu.F_U, hu)
-        solver2.upload(sgpu.F_V, hv)
-        solver2.upload(sgpu.F_P, hp)
-        r2, _ = solver2.run(args.steps)
-        out_u, out_v, out_p = (solver2.download(f) for f in (sgpu.F_U, sgpu.F_V, sgpu.F_P))
-        t_e2e = time.perf_counter() - t0
-        solver2.close()
-        t_e2e = allmax(t_e2e, world)
-        fb = 8 * p.nrows * p.ncols
-        e2e = {"value": world * r2.iterations / t_e2e, "unit": UNIT,
-               "h2d_bytes_per_step": 3 * fb / r2.iterations,
-               "d2h_bytes_per_step": 24 + 3 * fb / r2.iterations}
-        del out_u, out_v, out_p
-
-    solver.close()
+    e2e = e2e_measure(sgpu, torch, p, args.steps, world)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(n, args.cpu_seconds)
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": iters,
-            "warmup": args.warmup, "ms_per_step": 1e3 * secs_max / max(iters, 1),
+            "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world,
+            "steps": head["iters"], "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+            "dtype": "f64" if args.precision == "fp64" else "f64 (outer) + f32 (inner solves)",
             "data": "synthetic (cavity initial state u=v=p=0, lid u=1)",
             "config": {"workload": workload_name(n, args.precision), "cells": n * n,
                        "grid": f"{n}x{n}", "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (each field 134 MB at 4096^2; ~30 fields per step)",
-                       "converged_in_timed_region": bool(res.converged)},
+                       "l2": "inputs larger than L2 (each FP64 field 135 MB at 4096^2; ~40 arrays per step)",
+                       "converged_in_timed_region": head["converged"]},
+            "plain_fp64": None if plain is None else {
+                "value": plain["value"], "ms_per_step": plain["ms_per_step"],
+                "note": "bit-identical to the reference; same K steps, same run"},
+            "mixed_vs_fp64": None if plain is None else head["value"] / plain["value"],
             "e2e": e2e,
-            "gpu_launches": launches,
-            "clocks": clk,
-            "roofline": {"bound": "hbm", "kernel": "k_mom_stream (one multicolour sweep)",
-                         "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                         "peak_source": peaks["source"],
+            "gpu_launches": head["launches"],
+            "clocks": head["clocks"],
+            "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved,
+                         "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                         "traffic": traffic, "peak_source": peaks["source"],
                          "algorithmic_bytes_per_launch": bytes_per_launch,
                          "avg_launch_ms": per_launch_s * 1e3},
-            "phases_ms_per_step": phases_ms,
+            "phases_ms_per_step": {k: 1e3 * v / max(head["iters"], 1) for k, v in ph.items()},
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

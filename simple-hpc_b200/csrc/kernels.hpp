@@ -58,6 +58,10 @@ void launch_sweep_v_jacobi(const DevParams& p, Coef9Ptr cv, const double* src, d
 void launch_assemble_p(const DevParams& p, const double* APU, const double* APV, const double* u,
                        const double* v, PressurePtr w, double* cells_absb, double* cells_b,
                        cudaStream_t st);
+// The links and APP of assemble_p without b (the mixed path keeps its p' operator in FP32 and forms
+// the FP64 one only when a caller downloads it).
+void launch_p_links_app(const DevParams& p, const double* APU, const double* APV, PressurePtr w,
+                        cudaStream_t st);
 void launch_pc_redblack(const DevParams& p, PressurePtr w, int colour, cudaStream_t st);
 void launch_pc_jacobi(const DevParams& p, PressurePtr w, const double* src, double* dst,
                       cudaStream_t st);
@@ -75,6 +79,10 @@ template <class T> void launch_mg_residual(const LevelViewT<T>& L, cudaStream_t 
 template <class T> void launch_mg_restrict(const LevelViewT<T>& F, const LevelViewT<T>& C, cudaStream_t st);
 template <class T>
 void launch_mg_prolong(const LevelViewT<T>& C, const LevelViewT<T>& F, double omega, cudaStream_t st);
+// (b - A x)^2 and b^2 per cell of the level into a compact nx x ny plane (FP64), for the ordered
+// norms of the tolerance-driven V-cycle loop (mg_mode = tolerance).
+template <class T> void launch_mg_residual_sq(const LevelViewT<T>& L, double* cells, cudaStream_t st);
+template <class T> void launch_mg_b_sq(const LevelViewT<T>& L, double* cells, cudaStream_t st);
 // x[I, J] -= *sum / (nx * ny) over the level interior (the mean removal after an ordered sum).
 void launch_mg_sub_mean(const LevelView& L, double* x, const double* sum, cudaStream_t st);
 // Coarsest-level solve in one CTA (coarse_solve, multigrid.cpp:120-140) with relative tolerance

@@ -69,6 +69,28 @@ template <class T> __global__ void k_mg_prolong(LevelViewT<T> C, LevelViewT<T> F
     F.x[i * F.stride + j] += static_cast<T>(omega) * C.x[(i / 2) * C.stride + j / 2];
 }
 
+// Squares of the level residual r = b - A x (multigrid.cpp:84-85 form), in FP64, one per cell of a
+// compact nx x ny plane, for the ordered norm of the tolerance-driven V-cycle loop.
+template <class T> __global__ void k_mg_residual_sq(LevelViewT<T> L, double* cells) {
+    const int J = blockIdx.x * BX + threadIdx.x, I = blockIdx.y * BY + threadIdx.y;
+    if (I >= L.nx || J >= L.ny) return;
+    const int s = L.stride, q = I * s + J;
+    const T* x = L.x;
+    const double r = static_cast<double>(L.b[q]) -
+                     (static_cast<double>(L.AP[q]) * x[q] -
+                      (static_cast<double>(L.AE[q]) * x[q + 1] + static_cast<double>(L.AW[q]) * x[q - 1] +
+                       static_cast<double>(L.AS[q]) * x[q + s] + static_cast<double>(L.AN[q]) * x[q - s]));
+    cells[static_cast<std::size_t>(I) * L.ny + J] = r * r;
+}
+
+// Squares of b, for ||b|| of the same loop.
+template <class T> __global__ void k_mg_b_sq(LevelViewT<T> L, double* cells) {
+    const int J = blockIdx.x * BX + threadIdx.x, I = blockIdx.y * BY + threadIdx.y;
+    if (I >= L.nx || J >= L.ny) return;
+    const double b = L.b[I * L.stride + J];
+    cells[static_cast<std::size_t>(I) * L.ny + J] = b * b;
+}
+
 __global__ void k_mg_sub_mean(LevelView L, double* x, const double* sum) {
     const int J = blockIdx.x * BX + threadIdx.x, I = blockIdx.y * BY + threadIdx.y;
     if (I >= L.nx || J >= L.ny) return;
@@ -258,6 +280,19 @@ void launch_mg_coarse(const LevelViewT<T>& L, double* rowbuf, double tol, int* s
     k_mg_coarse<T><<<1, kCoarseThreads, 0, st>>>(L, rowbuf, tol, sweeps_out);
     SGPU_LAUNCH();
 }
+template <class T> void launch_mg_residual_sq(const LevelViewT<T>& L, double* cells, cudaStream_t st) {
+    k_mg_residual_sq<T><<<grid2(L.nx, L.ny), dim3(BX, BY), 0, st>>>(L, cells);
+    SGPU_LAUNCH();
+}
+template <class T> void launch_mg_b_sq(const LevelViewT<T>& L, double* cells, cudaStream_t st) {
+    k_mg_b_sq<T><<<grid2(L.nx, L.ny), dim3(BX, BY), 0, st>>>(L, cells);
+    SGPU_LAUNCH();
+}
+template void launch_mg_residual_sq<double>(const LevelViewT<double>&, double*, cudaStream_t);
+template void launch_mg_residual_sq<float>(const LevelViewT<float>&, double*, cudaStream_t);
+template void launch_mg_b_sq<double>(const LevelViewT<double>&, double*, cudaStream_t);
+template void launch_mg_b_sq<float>(const LevelViewT<float>&, double*, cudaStream_t);
+
 void launch_mg_sub_mean(const LevelView& L, double* x, const double* sum, cudaStream_t st) {
     k_mg_sub_mean<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, st>>>(L, x, sum);
     SGPU_LAUNCH();

@@ -239,6 +239,14 @@ __global__ void k_correct(DevParams p, PressurePtr w, const double* __restrict__
     pf[q] += p.ap * w.pc[q];
 }
 
+// APP alone (pressure.cpp:42): the links' sum, without touching b.
+__global__ void k_p_app(DevParams p, PressurePtr w, Range r) {
+    int i, j;
+    if (!cell_of(r, i, j)) return;
+    const std::size_t q = ix(p, i, j);
+    w.APP[q] = w.AEP[q] + w.AWP[q] + w.ANP[q] + w.ASP[q];
+}
+
 __global__ void k_copy(const double* __restrict__ src, double* __restrict__ dst, std::size_t n) {
     for (std::size_t k = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; k < n;
          k += static_cast<std::size_t>(gridDim.x) * blockDim.x)
@@ -326,6 +334,17 @@ void launch_assemble_p(const DevParams& p, const double* APU, const double* APV,
     k_p_zero<<<(n + 255) / 256, 256, 0, st>>>(p, w);
     SGPU_LAUNCH();
     k_p_rhs<<<grid_of(r), dim3(BX, BY), 0, st>>>(p, u, v, w, cells_absb, cells_b, r);
+    SGPU_LAUNCH();
+}
+void launch_p_links_app(const DevParams& p, const double* APU, const double* APV, PressurePtr w,
+                        cudaStream_t st) {
+    const Range r = r_p(p);
+    k_p_links<<<grid_of(r), dim3(BX, BY), 0, st>>>(p, APU, APV, w, r);
+    SGPU_LAUNCH();
+    const int n = p.nrows > p.ncols ? p.nrows : p.ncols;
+    k_p_zero<<<(n + 255) / 256, 256, 0, st>>>(p, w);
+    SGPU_LAUNCH();
+    k_p_app<<<grid_of(r), dim3(BX, BY), 0, st>>>(p, w, r);
     SGPU_LAUNCH();
 }
 void launch_pc_redblack(const DevParams& p, PressurePtr w, int colour, cudaStream_t st) {

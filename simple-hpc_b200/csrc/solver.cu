@@ -168,6 +168,7 @@ struct Solver {
     void sweep_v(int n);
     void assemble_p(double* out) {
         launch_assemble_p(dp, cu.a[8], cv.a[8], u, v, w, cells, nullptr, st);
+        p_links_stale = false;
         launch_ordered_sum(cells, 0, prm.NY, prm.NX, prm.NY, 1, out, ss, nullptr, st);
     }
     void solve_p();
@@ -253,6 +254,14 @@ struct Solver {
 
     // ---- mixed precision (precision = mixed): FP32 inner solves inside FP64 defect correction ----
     bool mixed = false;
+    // The mixed iteration keeps the p' operator in FP32 only; the FP64 links and APP are formed from
+    // APU / APV when a caller downloads one of them.
+    bool p_links_stale = false;
+    void form_p_links_if_stale(int id) {
+        if (!p_links_stale || id < SGPU_F_AEP || id > SGPU_F_APP) return;
+        launch_p_links_app(dp, cu.a[8], cv.a[8], w, st);
+        p_links_stale = false;
+    }
     float4* rec32 = nullptr;          // per-cell FP32 records: coefficients, 1/AP, R
     float* e32[2] = {nullptr, nullptr}; // correction ping-pong
     std::vector<LevelView32> lv32;    // FP32 multigrid hierarchy (level 0: the p' operator)
@@ -282,6 +291,7 @@ struct Solver {
     }
 
     void mixed_iteration_enqueue(double* res3) {
+        p_links_stale = true;
         mixed_momentum(false, res3 + 0);
         mixed_momentum(true, res3 + 1);
         mark(SGPU_PH_ASSEMBLE_P);
@@ -294,21 +304,65 @@ struct Solver {
         const LevelView32& L0 = lv32[0];
         SGPU_CUDA(cudaMemsetAsync(L0.x - (L0.stride + 1), 0,
                                   sizeof(float) * (L0.nx + 2) * static_cast<std::size_t>(L0.stride), st));
-        for (int c = 0; c < prm.mg_cycles; ++c) {
+        const bool guess = apply_warm_start(L0);
+        auto vcycle32 = [&](bool x_zero) {
             for (int l = 0; l < mg_tail; ++l)
-                launch_mg_down<float>(lv32[l], lv32[l + 1], mg32_x2[l], prm.mg_pre, c == 0 || l > 0, sms, st);
+                launch_mg_down<float>(lv32[l], lv32[l + 1], mg32_x2[l], prm.mg_pre, x_zero || l > 0, sms, st);
             launch_mg_tail<float>(mgl32, mg_tail, prm.mg_pre, prm.mg_post, prm.mg_omega, kCoarseTol32,
                                   coarse_rowbuf, stats, st);
             for (int l = mg_tail - 1; l >= 0; --l)
                 launch_mg_up<float>(lv32[l + 1], lv32[l], mg32_x2[l], lv32[l].x, prm.mg_omega,
                                     prm.mg_post, sms, st);
-        }
+        };
+        last_vcycles = run_cycles(L0, !guess, vcycle32);
         launch_ordered_sum(L0.x, 0, L0.stride, L0.nx, L0.ny, 1, sums + 26, ss, nullptr, st);
         mark(SGPU_PH_CORRECT);
         launch_correct_mixed(dp, L0, sums + 26, cu.a[8], cv.a[8], u, v, pf, w.pc, st);
         mark(SGPU_PH_COUNT);
-        last_vcycles = prm.mg_cycles;
     }
+
+    // V-cycles on level 0 (iterate L0.x, right-hand side L0.b). mg_mode = fixed: mg_cycles cycles
+    // (the reference, multigrid.cpp:349-354). mg_mode = tolerance: cycles until the FP64 norm
+    // ||b - A x|| <= pressure_tolerance ||b||, at most pressure_maxit; each norm is an ordered sum
+    // read back by the host. Returns the number of cycles run. first_zero: L0.x is zero on entry.
+    template <class T, class Cycle>
+    int run_cycles(const LevelViewT<T>& L0, bool first_zero, Cycle&& vcycle) {
+        if (prm.mg_mode != SGPU_MG_TOLERANCE) {
+            for (int c = 0; c < prm.mg_cycles; ++c) vcycle(first_zero && c == 0);
+            return prm.mg_cycles;
+        }
+        const std::size_t nr = static_cast<std::size_t>(L0.nx);
+        launch_mg_b_sq(L0, cells, st);
+        launch_ordered_sum(cells, 0, L0.ny, static_cast<int>(nr), L0.ny, 1, sums + 28, ss, nullptr, st);
+        const double bb = fetch(sums + 28);
+        if (!(bb > 0.0)) return 0;
+        const double target = prm.pressure_tolerance * std::sqrt(bb);
+        int c = 0;
+        if (!first_zero) { // a warm start may already meet the tolerance
+            launch_mg_residual_sq(L0, cells, st);
+            launch_ordered_sum(cells, 0, L0.ny, static_cast<int>(nr), L0.ny, 1, sums + 29, ss, nullptr, st);
+            last_rel_initial = std::sqrt(fetch(sums + 29)) / std::sqrt(bb);
+            if (std::sqrt(fetch(sums + 29)) <= target) return 0;
+        } else {
+            last_rel_initial = 1.0;
+        }
+        while (c < prm.pressure_maxit) {
+            vcycle(first_zero && c == 0);
+            ++c;
+            launch_mg_residual_sq(L0, cells, st);
+            launch_ordered_sum(cells, 0, L0.ny, static_cast<int>(nr), L0.ny, 1, sums + 29, ss, nullptr, st);
+            const double rr = fetch(sums + 29);
+            last_rel = std::sqrt(rr) / std::sqrt(bb);
+            if (std::sqrt(rr) <= target) break;
+        }
+        return c;
+    }
+
+    // Learned warm start (warm_start = cnn): writes the network's p' guess into L0.x. Returns whether
+    // a guess was written (false: L0.x stays zero).
+    double last_rel_initial = 1.0;
+    bool apply_warm_start(const LevelViewT<double>& L0);
+    bool apply_warm_start(const LevelViewT<float>& L0);
 
     void outer_iteration_enqueue(double* res3) {
         mark(SGPU_PH_ASSEMBLE_U);
@@ -674,13 +728,16 @@ void Solver::solve_mg() {
     for (std::size_t l = 1; l < lv.size(); ++l) launch_mg_build(lv[l - 1], lv[l], st);
     SGPU_CUDA(cudaMemsetAsync(w.pc, 0, g.bytes(), st));
     remove_mean0(w.b);
-    for (int c = 0; c < prm.mg_cycles; ++c) {
-        if (mg_fast) mg_vcycle_fast(c == 0);
+    const bool guess = apply_warm_start(lv[0]);
+    last_vcycles = run_cycles(lv[0], !guess, [&](bool x_zero) {
+        if (mg_fast) mg_vcycle_fast(x_zero);
         else mg_vcycle();
-    }
+    });
     remove_mean0(w.pc);
-    last_vcycles = prm.mg_cycles;
 }
+
+bool Solver::apply_warm_start(const LevelViewT<double>&) { return false; }
+bool Solver::apply_warm_start(const LevelViewT<float>&) { return false; }
 
 // mg_vcycle with the streaming level kernels: levels [0, mg_tail) go down and up in one pass
 // each, the rest (and the coarse solve) in the single-CTA tail kernel.
@@ -899,6 +956,7 @@ int sgpu_download(sgpu_handle* h, int id, double* host) {
     return guarded([&] {
         double* f = h->s->field_ptr(id);
         if (!f) throw sgpu::Error(SGPU_E_INVALID, "sgpu_download: unknown field id " + std::to_string(id));
+        h->s->form_p_links_if_stale(id);
         h->s->download(f, host);
     });
 }

@@ -1,0 +1,130 @@
+"""Tolerance-driven multigrid (mg_mode = tolerance): V-cycles until ||b - A p'|| <= tol ||b||.
+
+The reference runs a fixed mg_cycles V-cycles (multigrid.cpp:347-357); mg_mode = tolerance is an
+option of this implementation. These tests recompute the residual of the downloaded p' system in
+numpy (pressure.cpp:70-75's stencil: APP p = AEP pE + AWP pW + ASP pS + ANP pN + b) and check it
+against the tolerance and against the solver's own reported norm, and that mg_mode = fixed is
+unchanged (bit-identical to the oracle: the parity suite covers it).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import bit_equal, config_text, cuda_available, snapshot_config
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
+
+F_AEP, F_AWP, F_ANP, F_ASP, F_APP, F_B, F_PC = range(21, 28)
+
+
+def p_residual(s, p, b_minus_mean: bool, fp32_operator: bool = False) -> tuple[float, float]:
+    """(||b - A p'||, ||b||) over the p' cells i in [H, NX+H), j in [H+1, NY+H]. fp32_operator:
+    the coefficients and b rounded to FP32 first (the operator the mixed V-cycle solves)."""
+    H, NX, NY = p.H, p.NX, p.NY
+    f = {k: s.download(k) for k in (F_AEP, F_AWP, F_ANP, F_ASP, F_APP, F_B, F_PC)}
+    i0, i1, j0, j1 = H, NX + H, H + 1, NY + H + 1
+    pc = f[F_PC]
+    c = (slice(i0, i1), slice(j0, j1))
+    b = f[F_B][c].copy()
+    if b_minus_mean:
+        b -= b.mean()
+    if fp32_operator:
+        for k in (F_AEP, F_AWP, F_ANP, F_ASP, F_APP):
+            f[k] = f[k].astype(np.float32).astype(np.float64)
+        b = b.astype(np.float32).astype(np.float64)
+    ap = (f[F_AEP][c] * pc[i0:i1, j0 + 1:j1 + 1] + f[F_AWP][c] * pc[i0:i1, j0 - 1:j1 - 1]
+          + f[F_ASP][c] * pc[i0 + 1:i1 + 1, j0:j1] + f[F_ANP][c] * pc[i0 - 1:i1 - 1, j0:j1])
+    r = b + ap - f[F_APP][c] * pc[c]
+    return float(np.linalg.norm(r)), float(np.linalg.norm(b))
+
+
+def cavity(n: int, **kw) -> dict:
+    cfg = snapshot_config("short_16")
+    cfg.update(N_cells_x=str(n), N_cells_y=str(n), Re="1000", convection_scheme="QUICK",
+               diffusion_order="4", momentum_solver="gs_multicolour", pressure_solver="mg",
+               error_tolerance="0", maxit="10")
+    cfg.update({k: str(v) for k, v in kw.items()})
+    return cfg
+
+
+@pytest.mark.parametrize("n,tol", [(64, 1e-8), (200, 1e-6)])
+def test_tolerance_mode_fp64_meets_tolerance(sgpu_mod, n, tol):
+    cfg = cavity(n, mg_mode="tolerance", pressure_tolerance=tol, pressure_maxit=200)
+    p = sgpu_mod.params_from_config(config_text(cfg))
+    with sgpu_mod.Solver(p) as s:
+        cycles = []
+        for it in range(4):
+            s.outer_iteration()
+            st = s.last_solve_stats()
+            rn, bn = p_residual(s, p, b_minus_mean=False)
+            print(f"it {it}: {st['mg_vcycles']} V-cycles, reported {st['rel_residual']:.3e}, "
+                  f"numpy {rn / bn:.3e}")
+            assert 1 <= st["mg_vcycles"] <= 200
+            assert st["rel_residual"] <= tol
+            assert rn / bn <= tol * 1.01
+            # the reported norm is the same quantity (up to the mean removal of p')
+            assert abs(rn / bn - st["rel_residual"]) <= 1e-3 * tol + 1e-14
+            cycles.append(st["mg_vcycles"])
+    # a tighter tolerance needs more cycles than the default fixed count of 1
+    assert max(cycles) > 1
+
+
+def test_tolerance_mode_more_cycles_for_tighter_tol(sgpu_mod):
+    got = {}
+    for tol in (1e-4, 1e-9):
+        cfg = cavity(96, mg_mode="tolerance", pressure_tolerance=tol, pressure_maxit=300)
+        p = sgpu_mod.params_from_config(config_text(cfg))
+        with sgpu_mod.Solver(p) as s:
+            s.outer_iteration()
+            got[tol] = s.last_solve_stats()["mg_vcycles"]
+    print(got)
+    assert got[1e-9] > got[1e-4] >= 1
+
+
+def test_tolerance_mode_maxit_caps_cycles(sgpu_mod):
+    cfg = cavity(96, mg_mode="tolerance", pressure_tolerance=1e-14, pressure_maxit=3)
+    p = sgpu_mod.params_from_config(config_text(cfg))
+    with sgpu_mod.Solver(p) as s:
+        s.outer_iteration()
+        st = s.last_solve_stats()
+    assert st["mg_vcycles"] == 3
+    assert st["rel_residual"] > 1e-14
+
+
+def test_fixed_mode_equals_tolerance_mode_with_same_cycle_count(sgpu_mod):
+    """With a tolerance no cycle can meet and pressure_maxit = mg_cycles, both modes run the same
+    V-cycles on the same data: the fields are bit-identical."""
+    out = []
+    for mode in ("fixed", "tolerance"):
+        cfg = cavity(64, mg_mode=mode, mg_cycles=2, pressure_tolerance=1e-30, pressure_maxit=2)
+        p = sgpu_mod.params_from_config(config_text(cfg))
+        with sgpu_mod.Solver(p) as s:
+            for _ in range(3):
+                s.outer_iteration()
+            out.append([s.download(f) for f in (0, 1, 2)])
+    for a, b in zip(*out):
+        assert bit_equal(a, b)
+
+
+def test_tolerance_mode_mixed(sgpu_mod):
+    tol = 1e-5
+    cfg = cavity(128, mg_mode="tolerance", pressure_tolerance=tol, pressure_maxit=100,
+                 precision="mixed")
+    p = sgpu_mod.params_from_config(config_text(cfg))
+    with sgpu_mod.Solver(p) as s:
+        for it in range(3):
+            s.outer_iteration()
+            st = s.last_solve_stats()
+            rn32, bn32 = p_residual(s, p, b_minus_mean=True, fp32_operator=True)
+            rn, bn = p_residual(s, p, b_minus_mean=True)
+            print(f"it {it}: {st['mg_vcycles']} V-cycles, reported {st['rel_residual']:.3e}, "
+                  f"numpy FP32 operator {rn32 / bn32:.3e}, FP64 operator {rn / bn:.3e}")
+            assert 1 <= st["mg_vcycles"] <= 100
+            assert st["rel_residual"] <= tol
+            # the FP32 operator's residual, recomputed in FP64 from the stored p' (its FP64 mean
+            # removed, which that operator's rows do not sum away exactly)
+            assert rn32 / bn32 <= 1.5 * tol
+            # against the FP64 operator the FP32 rounding of the coefficients shows as well
+            assert rn / bn <= 1e-2

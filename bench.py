@@ -224,6 +224,7 @@ def measure(sgpu, torch, n: int, precision: str, steps: int, warmup: int, world:
         solver.outer_iteration()
     solver.set_profiling(True)
     ph0 = solver.phase_seconds()
+    sw0 = solver.sweep_seconds()
     launches0 = sgpu.launch_count()
     clk = Clocks(local) if clocks else None
     barrier(world)
@@ -238,12 +239,14 @@ def measure(sgpu, torch, n: int, precision: str, steps: int, warmup: int, world:
     clk_info = clk.stop() if clk else None
     launches = sgpu.launch_count() - launches0
     ph1 = solver.phase_seconds()
+    sw1 = solver.sweep_seconds()
     solver.close()
     secs = allmax(e0.elapsed_time(e1) * 1e-3, world)
     iters = res.iterations
     return {"p": p, "iters": iters, "secs": secs, "value": world * iters / secs,
             "ms_per_step": 1e3 * secs / max(iters, 1), "launches": launches, "clocks": clk_info,
             "phases": {k: (ph1[k] - ph0[k]) for k in ph1 if k != "output"},
+            "sweep_s": sw1[0] - sw0[0], "sweep_launches": sw1[1] - sw0[1],
             "converged": bool(res.converged)}
 
 
@@ -301,11 +304,11 @@ def main() -> None:
     if args.precision != "fp64" and not args.no_fp64_arm:
         plain = measure(sgpu, torch, n, "fp64", args.steps, args.warmup, world, local, False)
 
-    # Roofline of the dominant kernel: the streaming sweep (2 x maxit_inner launches per step).
+    # Roofline of the dominant kernel: the streaming sweep (2 x maxit_inner launches per step), timed
+    # alone by the solver's own events around its back-to-back launches.
     ph = head["phases"]
-    sweep_s = ph["sweep_u"] + ph["sweep_v"]
-    sweep_launches = head["iters"] * (p.maxit_inner_u + p.maxit_inner_v)
-    cells = p.nrows * p.ncols
+    sweep_s, sweep_launches = head["sweep_s"], head["sweep_launches"]
+    cells = (p.NX - 1) * p.NY  # cells one sweep updates: u NX x (NY-1), v (NX-1) x NY (square grid)
     if args.precision == "mixed":
         kernel = "k_corr_stream (one FP32 multicolour correction sweep)"
         bytes_per_cell = 48 + 4 + 4  # record read, e_in read, e_out written

@@ -219,9 +219,13 @@ int sgpu_ordered_sum_noalloc(const double* values, int nrows_v, int ncols_v, int
  * SGPU_PH_*), the way the reference's PhaseTimers accumulate wall time (include/simple/timer.hpp).
  * sgpu_stream returns the handle's cudaStream_t (as void*) so a caller can time on it.
  * sgpu_launch_count returns the number of kernel launches this library has issued in the process.
+ * sgpu_sweep_seconds returns the device time of the streaming momentum sweep kernels alone (the
+ * FP64 sweep, or the FP32 correction sweep with precision = mixed) and how many were launched, both
+ * accumulated over the profiled iterations: the per-launch time of the dominant kernel.
  */
 int sgpu_set_profiling(sgpu_handle* h, int on);
 int sgpu_phase_seconds(sgpu_handle* h, double* out /* SGPU_PH_COUNT */);
+int sgpu_sweep_seconds(sgpu_handle* h, double* seconds, long long* launches);
 int sgpu_stream(sgpu_handle* h, void** stream);
 long long sgpu_launch_count(void);
 

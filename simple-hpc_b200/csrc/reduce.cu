@@ -13,6 +13,8 @@
 // added); the sums are FP64.
 #include "kernels.hpp"
 
+#include <algorithm>
+
 namespace sgpu {
 
 namespace {
@@ -38,7 +40,7 @@ template <class TIn>
 __global__ void __launch_bounds__(32)
     k_ordered_sum(const TIn* __restrict__ vals, std::size_t plane_stride, int ld, int nr, int nc,
                   double* __restrict__ rows, unsigned int* counter, double* __restrict__ out,
-                  const int* skip) {
+                  const int* skip, int chunk) {
     if (skip && *skip) return;
     extern __shared__ __align__(16) unsigned char tile_raw[];
     TIn(*tile)[kTile][kPitch] = reinterpret_cast<TIn(*)[kTile][kPitch]>(tile_raw);
@@ -93,12 +95,36 @@ __global__ void __launch_bounds__(32)
     __syncwarp();
     if (!last_block) return;
     __threadfence();
-    if (lane < static_cast<int>(gridDim.y)) {
-        const double* rs = rows + static_cast<std::size_t>(lane) * nr;
-        double acc = 0.0;
-        for (int k = 0; k < nr; ++k) acc += __ldcg(rs + k); // L2: written by other CTAs
-        out[lane] = acc;
+    // The chain over the rows is serial, so it must not wait on L2 for each term: the warp stages
+    // chunks of every plane's row sums in shared memory (the tile ring is free now; many
+    // independent loads per lane in flight), then lane m adds plane m's chunk from registers.
+    const int K = static_cast<int>(gridDim.y);
+    double* buf = reinterpret_cast<double*>(tile_raw);
+    const int cs = chunk + 1; // plane stride in buf: lanes reading one row index hit distinct banks
+    double acc = 0.0;
+    for (int c0 = 0; c0 < nr; c0 += chunk) {
+        const int n = min(chunk, nr - c0);
+        __syncwarp();
+        for (int m2 = 0; m2 < K; ++m2) {
+            const double* rs = rows + static_cast<std::size_t>(m2) * nr + c0;
+#pragma unroll 16
+            for (int r = lane; r < n; r += kTile) buf[m2 * cs + r] = __ldcg(rs + r); // L2: other CTAs wrote them
+        }
+        __syncwarp();
+        if (lane < K) {
+            const double* b = buf + lane * cs;
+            int r = 0;
+            for (; r + kTile <= n; r += kTile) {
+                double v[kTile];
+#pragma unroll
+                for (int t = 0; t < kTile; ++t) v[t] = b[r + t];
+#pragma unroll
+                for (int t = 0; t < kTile; ++t) acc += v[t];
+            }
+            for (; r < n; ++r) acc += b[r];
+        }
     }
+    if (lane < K) out[lane] = acc;
     if (lane == 0) *counter = 0u; // ready for the next launch on this stream
 }
 
@@ -118,7 +144,10 @@ void launch_sum(const TIn* vals, std::size_t plane_stride, int ld, int nr, int n
         SGPU_CUDA(cudaFuncSetAttribute(k_ordered_sum<TIn>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         attr = true;
     }
-    k_ordered_sum<TIn><<<grid, 32, smem, st>>>(vals, plane_stride, ld, nr, nc, s.rows, s.counter, out, skip);
+    // Rows per staged chunk of the final pass: K planes of (chunk + 1) doubles fit the tile ring.
+    const int chunk = std::min(2048, (smem / (static_cast<int>(sizeof(double)) * K) - 1) / kTile * kTile);
+    k_ordered_sum<TIn><<<grid, 32, smem, st>>>(vals, plane_stride, ld, nr, nc, s.rows, s.counter, out,
+                                                skip, chunk);
     SGPU_LAUNCH();
 }
 

@@ -199,10 +199,12 @@ struct Solver {
         const int n = vcomp ? prm.maxit_inner_v : prm.maxit_inner_u;
         double* in = x;
         double* out = tmp;
+        sweep_mark(vcomp, 0, n);
         for (int k = 0; k < n; ++k) {
             launch_mom_sweep(dp, vcomp, in, out, xF, oth, pf, seg_rows, st);
             std::swap(in, out);
         }
+        sweep_mark(vcomp, 1, n);
         if (in != x) launch_copy(in, x, g.elems(), st);
     }
 
@@ -233,9 +235,30 @@ struct Solver {
         SGPU_CUDA(cudaEventRecord(ev[ph], st));
         ev_order[ev_n++] = ph;
     }
+    // The streaming sweep kernels alone (k_mom_stream or k_corr_stream, back to back on the stream):
+    // events before the first and after the last sweep of each component.
+    cudaEvent_t sw_ev[4] = {};
+    int sw_pending[2] = {0, 0};
+    double sweep_acc = 0.0;
+    long long sweep_launches = 0;
+    void sweep_mark(bool vcomp, int end, int n) {
+        if (!profiling || n <= 0) return;
+        cudaEvent_t& e = sw_ev[2 * (vcomp ? 1 : 0) + end];
+        if (!e) SGPU_CUDA(cudaEventCreate(&e));
+        SGPU_CUDA(cudaEventRecord(e, st));
+        if (end) sw_pending[vcomp ? 1 : 0] = n;
+    }
     // After the stream is synchronised: add each phase's time to phase_acc (and to out if given).
     void collect_phases(double* out) {
         if (!profiling) return;
+        for (int c = 0; c < 2; ++c) {
+            if (!sw_pending[c]) continue;
+            float ms = 0.0f;
+            SGPU_CUDA(cudaEventElapsedTime(&ms, sw_ev[2 * c], sw_ev[2 * c + 1]));
+            sweep_acc += ms * 1e-3;
+            sweep_launches += sw_pending[c];
+            sw_pending[c] = 0;
+        }
         for (int k = 0; k + 1 < ev_n; ++k) {
             float ms = 0.0f;
             SGPU_CUDA(cudaEventElapsedTime(&ms, ev[ev_order[k]], ev[ev_order[k + 1]]));
@@ -283,10 +306,12 @@ struct Solver {
         mark(vcomp ? SGPU_PH_SWEEP_V : SGPU_PH_SWEEP_U);
         const int n = vcomp ? prm.maxit_inner_v : prm.maxit_inner_u;
         int cur = 0; // e32[cur] holds the current correction (zero before the first sweep)
+        sweep_mark(vcomp, 0, n);
         for (int k = 0; k < n; ++k) {
             launch_corr_sweep(dp, vcomp, e32[cur], e32[1 - cur], rec32, k == 0, seg_rows, st);
             cur = 1 - cur;
         }
+        sweep_mark(vcomp, 1, n);
         if (n > 0) launch_add_correction(dp, vcomp, x, e32[cur], st);
     }
 
@@ -600,6 +625,10 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
 
 Solver::~Solver() {
     if (st) cudaStreamSynchronize(st);
+    for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : sw_ev)
+        if (e) cudaEventDestroy(e);
     for (void* q : allocs) cudaFree(q);
     if (host_res) cudaFreeHost(host_res);
     if (st) cudaStreamDestroy(st);
@@ -1062,6 +1091,13 @@ int sgpu_phase_seconds(sgpu_handle* h, double* out) {
     SGPU_NEED_HANDLE(h);
     if (!out) return sgpu::fail(SGPU_E_INVALID, "sgpu_phase_seconds: null output");
     for (int k = 0; k < SGPU_PH_COUNT; ++k) out[k] = h->s->phase_acc[k];
+    return SGPU_OK;
+}
+
+int sgpu_sweep_seconds(sgpu_handle* h, double* seconds, long long* launches) {
+    SGPU_NEED_HANDLE(h);
+    if (seconds) *seconds = h->s->sweep_acc;
+    if (launches) *launches = h->s->sweep_launches;
     return SGPU_OK;
 }
 

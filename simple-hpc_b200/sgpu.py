@@ -110,6 +110,7 @@ def lib() -> C.CDLL:
             "sgpu_last_solve_stats": (I, [H, C.POINTER(I), C.POINTER(I), C.POINTER(I), D]),
             "sgpu_ordered_sum": (I, [D, I, I, D]),
             "sgpu_set_profiling": (I, [H, I]), "sgpu_phase_seconds": (I, [H, D]),
+            "sgpu_sweep_seconds": (I, [H, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
             "sgpu_stream": (I, [H, C.POINTER(C.c_void_p)]), "sgpu_launch_count": (C.c_longlong, []),
             "sgpu_write_outputs": (I, [P, D, D, D, D, I, C.POINTER(Result), C.c_char_p, C.c_char_p,
                                        C.c_char_p]),
@@ -275,6 +276,12 @@ class Solver:
         out = np.zeros(12)
         _check(lib().sgpu_phase_seconds(self._h, _dptr(out)))
         return dict(zip(PHASES, out.tolist()))
+
+    def sweep_seconds(self) -> tuple[float, int]:
+        """(device seconds, launches) of the streaming sweep kernels while profiling was on."""
+        sec, n = C.c_double(), C.c_longlong()
+        _check(lib().sgpu_sweep_seconds(self._h, C.byref(sec), C.byref(n)))
+        return sec.value, n.value
 
     def stream(self) -> int:
         s = C.c_void_p()

@@ -239,9 +239,55 @@ int sgpu_write_outputs(const sgpu_params_t* p, const double* u, const double* v,
                        const double* log, int iterations, const sgpu_result_t* result,
                        const char* cfg_path, const char* git_hash, const char* compiler);
 
-/* ---- learned warm start for p' (keys warm_start, cnn_weights) ---- */
-/* Load or replace the network weights of a handle from a file written by sgpu_cnn_save. */
+/* ---- learned warm start for p' (keys warm_start, cnn_weights) ----
+ *
+ * The reference has no learned part: p' starts at zero before every solve (multigrid.cpp:349-354,
+ * pressure.cpp:114-134). With a network attached (warm_start = cnn, sgpu_cnn_load or
+ * sgpu_attach_cnn) and pressure_solver = mg, each p' solve first runs the network on the finest
+ * multigrid level of at most max_size x max_size cells (inputs: that level's restricted b and its
+ * diagonal AP), injects the guess down to the fine grid and starts the V-cycles from it. The
+ * multigrid is unchanged: with mg_mode = tolerance it iterates to the same tolerance as from zero.
+ * A guess whose residual is not below ||b|| is discarded (the cycles start from zero, counted as a
+ * fallback).
+ *
+ * Network: U-Net of `levels` levels, `base` channels on the finest (doubling per level), 3x3
+ * convolutions with ReLU, 2x2 average pooling, nearest upsampling with skip concatenation, 1x1
+ * head; BF16 weights and activations, FP32 accumulation on the tensor cores; FP32 master weights
+ * trained with Adam on the mean-squared error. Images are n x height x width with 2 FP32 input
+ * channels interleaved per pixel (b / rms(b), AP / mean(AP) - 1) and 1 FP32 output channel (p' *
+ * mean(AP) / rms(b)); height and width must be multiples of 2^(levels-1).
+ */
+typedef struct sgpu_cnn sgpu_cnn;
+/* Load or replace the network of a handle from a weights file (sgpu_cnn_write), cnn_max 256. */
 int sgpu_cnn_load(sgpu_handle* h, const char* path);
+int sgpu_cnn_create(int base, int levels, unsigned seed, sgpu_cnn** out);
+int sgpu_cnn_read(const char* path, sgpu_cnn** out);
+int sgpu_cnn_write(sgpu_cnn* c, const char* path);
+int sgpu_cnn_destroy(sgpu_cnn* c);
+int sgpu_cnn_info(sgpu_cnn* c, int* base, int* levels, long long* num_params, double* flops_per_pixel);
+/* FP32 master parameters: per convolution W[cout][9][cin] then bias[cout], in network order (encoder
+ * levels finest first, two convolutions each; decoder levels coarsest first, the first of each pair
+ * with cin = its upsampled input + the skip); then the head's base weights and its bias. */
+int sgpu_cnn_get_params(sgpu_cnn* c, float* host);
+int sgpu_cnn_set_params(sgpu_cnn* c, const float* host);
+int sgpu_cnn_forward(sgpu_cnn* c, const float* in, int n, int height, int width, float* out);
+/* Loss (mean-squared error against target) and, if grads is not null, its gradient with respect to
+ * every parameter (layout of sgpu_cnn_get_params). */
+int sgpu_cnn_loss_grad(sgpu_cnn* c, const float* in, const float* target, int n, int height, int width,
+                       float* loss, float* grads);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on one batch; *loss = the batch loss before the step. */
+int sgpu_cnn_train_step(sgpu_cnn* c, const float* in, const float* target, int n, int height, int width,
+                        float lr, float* loss);
+/* Attach a network to a handle (not owned: keep it alive while attached; NULL detaches). */
+int sgpu_attach_cnn(sgpu_handle* h, sgpu_cnn* c, int max_size);
+/* Warm starts applied, guesses discarded, and the last guess's ||b - A p'|| / ||b||. */
+int sgpu_warm_start_stats(sgpu_handle* h, long long* used, long long* fallbacks, double* rel_initial);
+/* Training pair from the handle's last p' solve (precision = fp64, pressure_solver = mg): the
+ * network input of the finest level of at most max_size x max_size cells (nx x ny x 2) and the
+ * normalised block mean of the solved p' on it (nx x ny). With in or target NULL only *nx, *ny and
+ * *level are returned. Run the solves with mg_mode = tolerance and a tight pressure_tolerance so
+ * the target is the converged p'. */
+int sgpu_cnn_sample(sgpu_handle* h, int max_size, float* in, float* target, int* nx, int* ny, int* level);
 
 #ifdef __cplusplus
 }

@@ -42,6 +42,7 @@ SOURCES = {
     "mixed.cu": EXACT,
     "io.cpp": EXACT,
     "noalloc.cu": EXACT,
+    "cnn.cu": FAST,
 }
 DRIVER = ["driver.cpp"]
 

@@ -9,6 +9,7 @@
 //    GPU backend accepts gs_multicolour + gs_redblack only, solver_hip.hip:373-377);
 //  - one CUDA stream per handle; an outer iteration ends with one device->host copy of the three
 //    residuals instead of a device synchronisation per phase.
+#include "cnn.hpp"
 #include "kernels.hpp"
 
 #include <atomic>
@@ -103,6 +104,21 @@ struct Solver {
     int seg_rows = 64;
 
     int ncol = 5;
+
+    // learned warm start (warm_start = cnn, or a network attached through the C ABI)
+    std::unique_ptr<UNet> own_net;
+    UNet* net = nullptr;
+    int cnn_max = 256; // the network runs on the finest level of at most cnn_max x cnn_max cells
+    long long ws_used = 0, ws_fallbacks = 0;
+    float* pair_buf = nullptr; // training pair of the last sgpu_cnn_sample (input 2 planes, target)
+    template <class T> int cnn_level(const std::vector<LevelViewT<T>>& L) const {
+        int l = 0;
+        while (l + 1 < static_cast<int>(L.size()) && std::max(L[l].nx, L[l].ny) > cnn_max) ++l;
+        return l;
+    }
+    template <class T> bool warm_start_on(std::vector<LevelViewT<T>>& L);
+    template <class T> void sample_pair(std::vector<LevelViewT<T>>& L, float* hin, float* htarget);
+
     int last_cg_iterations = 0, last_vcycles = 0, last_coarse_sweeps = 0;
     double last_rel = 0.0;
     bool cg_stats_pending = false;
@@ -350,37 +366,57 @@ struct Solver {
     // (the reference, multigrid.cpp:349-354). mg_mode = tolerance: cycles until the FP64 norm
     // ||b - A x|| <= pressure_tolerance ||b||, at most pressure_maxit; each norm is an ordered sum
     // read back by the host. Returns the number of cycles run. first_zero: L0.x is zero on entry.
+    // Otherwise L0.x is a warm start. It is judged after its first cycle, not before: a network guess
+    // carries rounding noise at the grid scale that the operator amplifies but the first smoothing
+    // removes. If the residual after that cycle is still not below ||b|| (what a zero start has
+    // before any cycle), the guess is discarded and the cycles start again from zero.
     template <class T, class Cycle>
     int run_cycles(const LevelViewT<T>& L0, bool first_zero, Cycle&& vcycle) {
-        if (prm.mg_mode != SGPU_MG_TOLERANCE) {
-            for (int c = 0; c < prm.mg_cycles; ++c) vcycle(first_zero && c == 0);
+        const bool tol_mode = prm.mg_mode == SGPU_MG_TOLERANCE;
+        const bool judge = !first_zero;
+        const int nr = L0.nx;
+        auto norm2 = [&](bool residual, double* slot) {
+            if (residual) launch_mg_residual_sq(L0, cells, st);
+            else launch_mg_b_sq(L0, cells, st);
+            launch_ordered_sum(cells, 0, L0.ny, nr, L0.ny, 1, slot, ss, nullptr, st);
+            return fetch(slot);
+        };
+        if (!tol_mode && !judge) { // the reference's fixed cycle count from zero
+            for (int c = 0; c < prm.mg_cycles; ++c) vcycle(c == 0);
             return prm.mg_cycles;
         }
-        const std::size_t nr = static_cast<std::size_t>(L0.nx);
-        launch_mg_b_sq(L0, cells, st);
-        launch_ordered_sum(cells, 0, L0.ny, static_cast<int>(nr), L0.ny, 1, sums + 28, ss, nullptr, st);
-        const double bb = fetch(sums + 28);
-        if (!(bb > 0.0)) return 0;
+        const double bb = norm2(false, sums + 28);
+        if (!(bb > 0.0)) { // b = 0: p' = 0
+            if (!first_zero) launch_zero_x(L0, st);
+            last_rel = 0.0;
+            return 0;
+        }
+        const int maxc = tol_mode ? prm.pressure_maxit : prm.mg_cycles;
         const double target = prm.pressure_tolerance * std::sqrt(bb);
-        int c = 0;
-        if (!first_zero) { // a warm start may already meet the tolerance
-            launch_mg_residual_sq(L0, cells, st);
-            launch_ordered_sum(cells, 0, L0.ny, static_cast<int>(nr), L0.ny, 1, sums + 29, ss, nullptr, st);
-            last_rel_initial = std::sqrt(fetch(sums + 29)) / std::sqrt(bb);
-            if (std::sqrt(fetch(sums + 29)) <= target) return 0;
-        } else {
-            last_rel_initial = 1.0;
-        }
-        while (c < prm.pressure_maxit) {
-            vcycle(first_zero && c == 0);
+        last_rel_initial = 1.0;
+        int c = 0, run = 0;
+        bool zero = first_zero;
+        while (c < maxc) {
+            vcycle(zero && c == 0);
             ++c;
-            launch_mg_residual_sq(L0, cells, st);
-            launch_ordered_sum(cells, 0, L0.ny, static_cast<int>(nr), L0.ny, 1, sums + 29, ss, nullptr, st);
-            const double rr = fetch(sums + 29);
+            ++run;
+            const bool need = tol_mode || (judge && c == 1);
+            if (!need) continue;
+            const double rr = norm2(true, sums + 29);
             last_rel = std::sqrt(rr) / std::sqrt(bb);
-            if (std::sqrt(rr) <= target) break;
+            if (judge && c == 1 && !zero) {
+                last_rel_initial = last_rel;
+                if (!(rr < bb)) { // no better than a zero start: discard the guess
+                    launch_zero_x(L0, st);
+                    ++ws_fallbacks;
+                    zero = true;
+                    c = 0;
+                    continue;
+                }
+            }
+            if (tol_mode && std::sqrt(rr) <= target) break;
         }
-        return c;
+        return run;
     }
 
     // Learned warm start (warm_start = cnn): writes the network's p' guess into L0.x. Returns whether
@@ -617,6 +653,15 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
         for (int l = 0; l < nl && l < 24; ++l) mgl32.L[l] = lv32[l];
     }
 
+    if (p.warm_start == 1) {
+        if (p.pressure_solver != SGPU_P_MG)
+            throw Error(SGPU_E_INVALID, "warm_start = cnn needs pressure_solver = mg");
+        if (!p.cnn_weights[0])
+            throw Error(SGPU_E_INVALID, "warm_start = cnn needs cnn_weights = <file written by sgpu_cnn_write>");
+        own_net = UNet::load(p.cnn_weights);
+        net = own_net.get();
+    }
+
     if (hu) upload(u, hu);
     if (hv) upload(v, hv);
     if (hp) upload(pf, hp);
@@ -765,8 +810,34 @@ void Solver::solve_mg() {
     remove_mean0(w.pc);
 }
 
-bool Solver::apply_warm_start(const LevelViewT<double>&) { return false; }
-bool Solver::apply_warm_start(const LevelViewT<float>&) { return false; }
+bool Solver::apply_warm_start(const LevelViewT<double>&) { return net && warm_start_on(lv); }
+bool Solver::apply_warm_start(const LevelViewT<float>&) { return net && warm_start_on(lv32); }
+
+// The network's guess on the finest level of at most cnn_max^2 cells (its b restricted from level 0
+// by 2x2 sums, its operator the multigrid one), injected back to level 0 as the initial iterate.
+template <class T> bool Solver::warm_start_on(std::vector<LevelViewT<T>>& L) {
+    const int l = cnn_level(L);
+    for (int k = 0; k < l; ++k) launch_restrict_b(L[k], L[k + 1], st);
+    net->predict_level(L[l], cells, plane, sums + 30, ss, st);
+    for (int k = l - 1; k >= 0; --k) launch_inject_x(L[k + 1], L[k], st);
+    ++ws_used;
+    return true;
+}
+
+// Training pair from the last p' solve: the network input of the warm-start level and the block
+// mean of the solved p' there (both normalised as the network sees them).
+template <class T> void Solver::sample_pair(std::vector<LevelViewT<T>>& L, float* hin, float* htarget) {
+    const int l = cnn_level(L);
+    for (int k = 0; k < l; ++k) launch_restrict_b(L[k], L[k + 1], st);
+    launch_level_stats(L[l], cells, plane, st);
+    launch_ordered_sum(cells, plane, L[l].ny, L[l].nx, L[l].ny, 2, sums + 30, ss, nullptr, st);
+    const std::size_t n = static_cast<std::size_t>(L[l].nx) * L[l].ny;
+    if (!pair_buf) pair_buf = dalloc<float>(3 * plane);
+    launch_make_pair(L[l], L[0], l, sums + 30, pair_buf, pair_buf + 2 * n, st);
+    SGPU_CUDA(cudaMemcpyAsync(hin, pair_buf, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost, st));
+    SGPU_CUDA(cudaMemcpyAsync(htarget, pair_buf + 2 * n, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    SGPU_CUDA(cudaStreamSynchronize(st));
+}
 
 // mg_vcycle with the streaming level kernels: levels [0, mg_tail) go down and up in one pass
 // each, the rest (and the coarse solve) in the single-CTA tail kernel.
@@ -795,6 +866,10 @@ void Solver::solve_p() {
 
 struct sgpu_handle {
     std::unique_ptr<sgpu::Solver> s;
+};
+struct sgpu_cnn {
+    std::unique_ptr<sgpu::UNet> net;
+    cudaStream_t st = nullptr;
 };
 
 namespace {
@@ -1112,8 +1187,168 @@ long long sgpu_launch_count(void) { return sgpu::g_launches.load(); }
 
 int sgpu_cnn_load(sgpu_handle* h, const char* path) {
     SGPU_NEED_HANDLE(h);
-    (void)path;
-    return sgpu::fail(SGPU_E_INVALID, "sgpu_cnn_load: not available in this build");
+    if (!path) return sgpu::fail(SGPU_E_INVALID, "sgpu_cnn_load: null path");
+    return guarded([&] {
+        sgpu::Solver& s = *h->s;
+        if (s.prm.pressure_solver != SGPU_P_MG)
+            throw sgpu::Error(SGPU_E_INVALID, "sgpu_cnn_load: the warm start needs pressure_solver = mg");
+        s.sync();
+        s.own_net = sgpu::UNet::load(path);
+        s.net = s.own_net.get();
+    });
+}
+
+int sgpu_cnn_create(int base, int levels, unsigned seed, sgpu_cnn** out) {
+    if (!out) return sgpu::fail(SGPU_E_INVALID, "sgpu_cnn_create: null output");
+    *out = nullptr;
+    return guarded([&] {
+        auto c = std::make_unique<sgpu_cnn>();
+        c->net = std::make_unique<sgpu::UNet>(base, levels, seed);
+        SGPU_CUDA(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+        *out = c.release();
+    });
+}
+
+int sgpu_cnn_read(const char* path, sgpu_cnn** out) {
+    if (!out || !path) return sgpu::fail(SGPU_E_INVALID, "sgpu_cnn_read: null argument");
+    *out = nullptr;
+    return guarded([&] {
+        auto c = std::make_unique<sgpu_cnn>();
+        c->net = sgpu::UNet::load(path);
+        SGPU_CUDA(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+        *out = c.release();
+    });
+}
+
+int sgpu_cnn_destroy(sgpu_cnn* c) {
+    if (!c) return SGPU_OK;
+    const int rc = guarded([&] {
+        if (c->st) cudaStreamSynchronize(c->st);
+        c->net.reset();
+        if (c->st) cudaStreamDestroy(c->st);
+    });
+    delete c;
+    return rc;
+}
+
+#define SGPU_NEED_CNN(c)                                                                           \
+    do {                                                                                           \
+        if (!(c) || !(c)->net) return sgpu::fail(SGPU_E_INVALID, "null network");                  \
+    } while (0)
+
+int sgpu_cnn_write(sgpu_cnn* c, const char* path) {
+    SGPU_NEED_CNN(c);
+    if (!path) return sgpu::fail(SGPU_E_INVALID, "sgpu_cnn_write: null path");
+    return guarded([&] {
+        SGPU_CUDA(cudaStreamSynchronize(c->st));
+        c->net->save(path);
+    });
+}
+
+int sgpu_cnn_info(sgpu_cnn* c, int* base, int* levels, long long* num_params, double* flops_per_pixel) {
+    SGPU_NEED_CNN(c);
+    if (base) *base = c->net->base();
+    if (levels) *levels = c->net->levels();
+    if (num_params) *num_params = c->net->num_params();
+    if (flops_per_pixel) *flops_per_pixel = c->net->flops_per_pixel();
+    return SGPU_OK;
+}
+
+int sgpu_cnn_get_params(sgpu_cnn* c, float* host) {
+    SGPU_NEED_CNN(c);
+    if (!host) return sgpu::fail(SGPU_E_INVALID, "sgpu_cnn_get_params: null buffer");
+    return guarded([&] { c->net->get_params(host); });
+}
+
+int sgpu_cnn_set_params(sgpu_cnn* c, const float* host) {
+    SGPU_NEED_CNN(c);
+    if (!host) return sgpu::fail(SGPU_E_INVALID, "sgpu_cnn_set_params: null buffer");
+    return guarded([&] { c->net->set_params(host); });
+}
+
+int sgpu_cnn_forward(sgpu_cnn* c, const float* in, int n, int height, int width, float* out) {
+    SGPU_NEED_CNN(c);
+    if (!in || !out) return sgpu::fail(SGPU_E_INVALID, "sgpu_cnn_forward: null buffer");
+    return guarded([&] {
+        c->net->set_input(in, n, height, width, c->st);
+        c->net->forward(c->st);
+        c->net->get_output(out, c->st);
+    });
+}
+
+int sgpu_cnn_loss_grad(sgpu_cnn* c, const float* in, const float* target, int n, int height, int width,
+                       float* loss, float* grads) {
+    SGPU_NEED_CNN(c);
+    if (!in || !target) return sgpu::fail(SGPU_E_INVALID, "sgpu_cnn_loss_grad: null buffer");
+    return guarded([&] {
+        c->net->set_input(in, n, height, width, c->st);
+        c->net->set_target(target, c->st);
+        c->net->forward(c->st);
+        c->net->backward(c->st);
+        const float l = c->net->loss(c->st);
+        if (loss) *loss = l;
+        if (grads) c->net->get_grads(grads);
+    });
+}
+
+int sgpu_cnn_train_step(sgpu_cnn* c, const float* in, const float* target, int n, int height, int width,
+                        float lr, float* loss) {
+    SGPU_NEED_CNN(c);
+    if (!in || !target) return sgpu::fail(SGPU_E_INVALID, "sgpu_cnn_train_step: null buffer");
+    if (!(lr > 0.0f)) return sgpu::fail(SGPU_E_INVALID, "sgpu_cnn_train_step: learning rate must be positive");
+    return guarded([&] {
+        c->net->set_input(in, n, height, width, c->st);
+        c->net->set_target(target, c->st);
+        c->net->forward(c->st);
+        c->net->backward(c->st);
+        c->net->adam(lr, c->st);
+        const float l = c->net->loss(c->st);
+        if (loss) *loss = l;
+    });
+}
+
+int sgpu_attach_cnn(sgpu_handle* h, sgpu_cnn* c, int max_size) {
+    SGPU_NEED_HANDLE(h);
+    return guarded([&] {
+        sgpu::Solver& s = *h->s;
+        if (c && s.prm.pressure_solver != SGPU_P_MG)
+            throw sgpu::Error(SGPU_E_INVALID, "sgpu_attach_cnn: the warm start needs pressure_solver = mg");
+        if (max_size < 8) throw sgpu::Error(SGPU_E_INVALID, "sgpu_attach_cnn: max_size must be >= 8");
+        s.sync();
+        if (c) SGPU_CUDA(cudaStreamSynchronize(c->st));
+        s.own_net.reset();
+        s.net = c ? c->net.get() : nullptr;
+        s.cnn_max = max_size;
+    });
+}
+
+int sgpu_warm_start_stats(sgpu_handle* h, long long* used, long long* fallbacks, double* rel_initial) {
+    SGPU_NEED_HANDLE(h);
+    sgpu::Solver& s = *h->s;
+    if (used) *used = s.ws_used;
+    if (fallbacks) *fallbacks = s.ws_fallbacks;
+    if (rel_initial) *rel_initial = s.last_rel_initial;
+    return SGPU_OK;
+}
+
+int sgpu_cnn_sample(sgpu_handle* h, int max_size, float* in, float* target, int* nx, int* ny, int* level) {
+    SGPU_NEED_HANDLE(h);
+    return guarded([&] {
+        sgpu::Solver& s = *h->s;
+        if (s.prm.pressure_solver != SGPU_P_MG || s.lv.empty())
+            throw sgpu::Error(SGPU_E_INVALID, "sgpu_cnn_sample: needs pressure_solver = mg");
+        if (max_size < 8) throw sgpu::Error(SGPU_E_INVALID, "sgpu_cnn_sample: max_size must be >= 8");
+        s.cnn_max = max_size;
+        const int l = s.cnn_level(s.lv);
+        if (nx) *nx = s.lv[l].nx;
+        if (ny) *ny = s.lv[l].ny;
+        if (level) *level = l;
+        if (!in || !target) return; // size query
+        if (s.mixed)
+            throw sgpu::Error(SGPU_E_INVALID, "sgpu_cnn_sample: generate training pairs with precision = fp64");
+        s.sync();
+        s.sample_pair(s.lv, in, target);
+    });
 }
 
 } // extern "C"

@@ -90,6 +90,7 @@ def lib() -> C.CDLL:
             raise ImportError(f"{LIB_PATH} is missing: build it with simple-hpc_b200/build.py")
         L = C.CDLL(str(LIB_PATH))
         P, D, I, H = C.POINTER(Params), C.POINTER(C.c_double), C.c_int, C.c_void_p
+        F = C.POINTER(C.c_float)
         sig = {
             "sgpu_params_from_config": (I, [C.c_char_p, P]),
             "sgpu_params_default": (I, [P]),
@@ -114,6 +115,20 @@ def lib() -> C.CDLL:
             "sgpu_stream": (I, [H, C.POINTER(C.c_void_p)]), "sgpu_launch_count": (C.c_longlong, []),
             "sgpu_write_outputs": (I, [P, D, D, D, D, I, C.POINTER(Result), C.c_char_p, C.c_char_p,
                                        C.c_char_p]),
+            # learned warm start
+            "sgpu_cnn_load": (I, [H, C.c_char_p]),
+            "sgpu_cnn_create": (I, [I, I, C.c_uint, C.POINTER(H)]),
+            "sgpu_cnn_read": (I, [C.c_char_p, C.POINTER(H)]),
+            "sgpu_cnn_write": (I, [H, C.c_char_p]),
+            "sgpu_cnn_destroy": (I, [H]),
+            "sgpu_cnn_info": (I, [H, C.POINTER(I), C.POINTER(I), C.POINTER(C.c_longlong), D]),
+            "sgpu_cnn_get_params": (I, [H, F]), "sgpu_cnn_set_params": (I, [H, F]),
+            "sgpu_cnn_forward": (I, [H, F, I, I, I, F]),
+            "sgpu_cnn_loss_grad": (I, [H, F, F, I, I, I, F, F]),
+            "sgpu_cnn_train_step": (I, [H, F, F, I, I, I, C.c_float, F]),
+            "sgpu_attach_cnn": (I, [H, H, I]),
+            "sgpu_warm_start_stats": (I, [H, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), D]),
+            "sgpu_cnn_sample": (I, [H, I, F, F, C.POINTER(I), C.POINTER(I), C.POINTER(I)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -132,6 +147,90 @@ def _dptr(a: np.ndarray | None):
     if a is None:
         return None
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _fptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Cnn:
+    """The warm-start network (sgpu_cnn_*): U-Net with BF16 tensor-core kernels, trained on the GPU.
+
+    Images are (n, height, width, 2) FP32 inputs and (n, height, width) FP32 targets / outputs;
+    height and width must be multiples of 2^(levels - 1)."""
+
+    def __init__(self, base: int = 16, levels: int = 4, seed: int = 0, path: str | None = None):
+        h = C.c_void_p()
+        if path is not None:
+            _check(lib().sgpu_cnn_read(str(path).encode(), C.byref(h)))
+        else:
+            _check(lib().sgpu_cnn_create(base, levels, seed, C.byref(h)))
+        self._h = h
+        b, l, n, f = C.c_int(), C.c_int(), C.c_longlong(), C.c_double()
+        _check(lib().sgpu_cnn_info(h, C.byref(b), C.byref(l), C.byref(n), C.byref(f)))
+        self.base, self.levels, self.num_params, self.flops_per_pixel = b.value, l.value, n.value, f.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().sgpu_cnn_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def write(self, path) -> None:
+        _check(lib().sgpu_cnn_write(self._h, str(path).encode()))
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.num_params, np.float32)
+        _check(lib().sgpu_cnn_get_params(self._h, _fptr(out)))
+        return out
+
+    def set_params(self, w: np.ndarray) -> None:
+        w = np.ascontiguousarray(w, np.float32)
+        if w.shape != (self.num_params,):
+            raise ValueError(f"expected {self.num_params} parameters, got {w.shape}")
+        _check(lib().sgpu_cnn_set_params(self._h, _fptr(w)))
+
+    @staticmethod
+    def _images(x: np.ndarray) -> tuple[np.ndarray, int, int, int]:
+        x = np.ascontiguousarray(x, np.float32)
+        if x.ndim != 4 or x.shape[3] != 2:
+            raise ValueError(f"input must be (n, height, width, 2), got {x.shape}")
+        return x, x.shape[0], x.shape[1], x.shape[2]
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x, n, hh, ww = self._images(x)
+        out = np.empty((n, hh, ww), np.float32)
+        _check(lib().sgpu_cnn_forward(self._h, _fptr(x), n, hh, ww, _fptr(out)))
+        return out
+
+    def loss_grad(self, x: np.ndarray, t: np.ndarray) -> tuple[float, np.ndarray]:
+        x, n, hh, ww = self._images(x)
+        t = np.ascontiguousarray(t, np.float32).reshape(n, hh, ww)
+        g = np.empty(self.num_params, np.float32)
+        loss = C.c_float()
+        _check(lib().sgpu_cnn_loss_grad(self._h, _fptr(x), _fptr(t), n, hh, ww, C.byref(loss), _fptr(g)))
+        return loss.value, g
+
+    def train_step(self, x: np.ndarray, t: np.ndarray, lr: float) -> float:
+        x, n, hh, ww = self._images(x)
+        t = np.ascontiguousarray(t, np.float32).reshape(n, hh, ww)
+        loss = C.c_float()
+        _check(lib().sgpu_cnn_train_step(self._h, _fptr(x), _fptr(t), n, hh, ww, lr, C.byref(loss)))
+        return loss.value
 
 
 def params_from_config(text: str, **overrides) -> Params:
@@ -287,6 +386,29 @@ class Solver:
         s = C.c_void_p()
         _check(lib().sgpu_stream(self._h, C.byref(s)))
         return s.value or 0
+
+    def attach_cnn(self, net: "Cnn | None", max_size: int = 256) -> None:
+        """Use net as the p' warm start (not owned: keep it alive; None detaches)."""
+        _check(lib().sgpu_attach_cnn(self._h, None if net is None else net._h, max_size))
+        self._net = net  # keep the network alive while attached
+
+    def load_cnn(self, path) -> None:
+        _check(lib().sgpu_cnn_load(self._h, str(path).encode()))
+
+    def warm_start_stats(self) -> dict:
+        u, f, r = C.c_longlong(), C.c_longlong(), C.c_double()
+        _check(lib().sgpu_warm_start_stats(self._h, C.byref(u), C.byref(f), C.byref(r)))
+        return {"used": u.value, "fallbacks": f.value, "rel_initial": r.value}
+
+    def cnn_sample(self, max_size: int = 256) -> tuple[np.ndarray, np.ndarray, int]:
+        """Training pair from the last p' solve: (input (nx, ny, 2), target (nx, ny), level)."""
+        nx, ny, lvl = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().sgpu_cnn_sample(self._h, max_size, None, None, C.byref(nx), C.byref(ny), C.byref(lvl)))
+        x = np.empty((nx.value, ny.value, 2), np.float32)
+        t = np.empty((nx.value, ny.value), np.float32)
+        _check(lib().sgpu_cnn_sample(self._h, max_size, _fptr(x), _fptr(t), C.byref(nx), C.byref(ny),
+                                     C.byref(lvl)))
+        return x, t, lvl.value
 
     def last_solve_stats(self) -> dict:
         a, b, c, r = C.c_int(), C.c_int(), C.c_int(), C.c_double()

@@ -289,6 +289,35 @@ int sgpu_warm_start_stats(sgpu_handle* h, long long* used, long long* fallbacks,
  * the target is the converged p'. */
 int sgpu_cnn_sample(sgpu_handle* h, int max_size, float* in, float* target, int* nx, int* ny, int* level);
 
+/* ---- batched cavities (sgpu_batch_*) ----
+ *
+ * Many independent cavities, each with its own parameters (size, Re, schemes, precision), solved in
+ * one graph launch: a WHILE node repeats one batch iteration while any cavity is active; inside it
+ * each cavity's outer iteration (captured from its own solver) sits under an IF node that runs it
+ * only while that cavity is active, and a final kernel applies the reference's stopping rule
+ * (run_outer_loop, solver.cpp:117-129) to every cavity on the device. A cavity therefore stops at
+ * exactly the iteration a single sgpu_run would, with the same fields. Supported per cavity: every
+ * momentum solver; pressure_solver gs_redblack, jacobi or mg with mg_mode = fixed; no warm start.
+ * The reference has no batched mode; a batch of one behaves like sgpu_run.
+ */
+typedef struct sgpu_batch sgpu_batch;
+int sgpu_batch_create(const sgpu_params_t* params /* count */, int count, sgpu_batch** out);
+int sgpu_batch_destroy(sgpu_batch* b);
+int sgpu_batch_count(sgpu_batch* b, int* count);
+/* Autotuner: per distinct grid, times the candidate row-segment heights of the streaming momentum
+ * sweep and keeps the fastest (chosen[count], 0 for cavities without that sweep; may be NULL). The
+ * segment height changes no result bit. Call before sgpu_batch_run. */
+int sgpu_batch_autotune(sgpu_batch* b, int* chosen);
+/* Run every cavity to its tolerance or maxit iterations from its current fields. log_cap > 0 keeps
+ * the first log_cap (iteration, res_u, res_v, res_p) rows of every cavity (sgpu_batch_log).
+ * *seconds = device time of the launch. */
+int sgpu_batch_run(sgpu_batch* b, int maxit, int log_cap, double* seconds);
+/* Per cavity: iterations run, converged flag, last res_u, res_v, res_p (3 per cavity). */
+int sgpu_batch_results(sgpu_batch* b, int* iterations, int* converged, double* residuals);
+/* count x log_cap x 4 doubles; rows past a cavity's iteration count are zero. */
+int sgpu_batch_log(sgpu_batch* b, double* host);
+int sgpu_batch_download(sgpu_batch* b, int index, int field_id, double* host);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,8 +17,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <string>
+#include <tuple>
 #include <vector>
 
 namespace sgpu {
@@ -864,8 +866,106 @@ void Solver::solve_p() {
 
 } // namespace sgpu
 
+namespace sgpu {
+
+// ---- batched cavities: device-side stopping test inside one graph launch ----
+
+struct BatchDev {
+    int n, maxit;
+    double* const* res;         // per cavity: its res_u, res_v, res_p of the current iteration
+    const double* tol;          // error_tolerance per cavity
+    const int* runmax;          // residual_normalisation = running_max per cavity
+    double* maxr;               // 3 running maxima per cavity
+    int* iters;                 // iterations done per cavity
+    int* active;                // 1 while a cavity iterates
+    int* converged;
+    double* last;               // 3 residuals of the last iteration per cavity
+    double* log;                // log_cap x 4 per cavity (iteration, res_u, res_v, res_p), or null
+    int log_cap;
+    cudaGraphConditionalHandle* h; // the IF node of each cavity
+    cudaGraphConditionalHandle hw; // the WHILE node around the batch iteration
+};
+
+// Start of a batch iteration: each cavity's IF node runs iff the cavity is still active.
+__global__ void k_batch_pre(BatchDev b) {
+    for (int c = threadIdx.x; c < b.n; c += blockDim.x) cudaGraphSetConditional(b.h[c], b.active[c] ? 1u : 0u);
+}
+
+// End of a batch iteration: the stopping rule of run_outer_loop (solver.cpp:117-129) per active
+// cavity, with the same arithmetic as the host loop of sgpu_run; the loop continues while any
+// cavity is active.
+__global__ void k_batch_step(BatchDev b) {
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int c = threadIdx.x; c < b.n; c += blockDim.x) {
+        if (!b.active[c]) continue;
+        const int it = ++b.iters[c];
+        const double ru = b.res[c][0], rv = b.res[c][1], rp = b.res[c][2];
+        b.last[3 * c + 0] = ru;
+        b.last[3 * c + 1] = rv;
+        b.last[3 * c + 2] = rp;
+        if (b.log && it <= b.log_cap) {
+            double* l = b.log + (static_cast<std::size_t>(c) * b.log_cap + (it - 1)) * 4;
+            l[0] = it;
+            l[1] = ru;
+            l[2] = rv;
+            l[3] = rp;
+        }
+        double tu = ru, tv = rv, tp = rp;
+        if (b.runmax[c]) {
+            double* m = b.maxr + 3 * c;
+            m[0] = m[0] < ru ? ru : m[0];
+            m[1] = m[1] < rv ? rv : m[1];
+            m[2] = m[2] < rp ? rp : m[2];
+            tu = m[0] > 0.0 ? ru / m[0] : 0.0;
+            tv = m[1] > 0.0 ? rv / m[1] : 0.0;
+            tp = m[2] > 0.0 ? rp / m[2] : 0.0;
+        }
+        double m = tu;
+        if (m < tv) m = tv;
+        if (m < tp) m = tp;
+        const bool conv = m <= b.tol[c] && it > 1;
+        if (conv || it >= b.maxit) {
+            b.active[c] = 0;
+            b.converged[c] = conv ? 1 : 0;
+        } else {
+            any = 1;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) cudaGraphSetConditional(b.hw, any ? 1u : 0u);
+}
+
+} // namespace sgpu
+
 struct sgpu_handle {
     std::unique_ptr<sgpu::Solver> s;
+};
+struct sgpu_batch {
+    std::vector<std::unique_ptr<sgpu::Solver>> s;
+    cudaStream_t st = nullptr;
+    std::vector<void*> dev; // device allocations of the batch state
+    double* d_last = nullptr;
+    double* d_log = nullptr;
+    int* d_iters = nullptr;
+    int* d_conv = nullptr;
+    int log_cap = 0;
+    int ran = 0; // 1 after sgpu_batch_run
+    std::vector<int> seg_tuned; // autotuned row segment per cavity (0: heuristic)
+    ~sgpu_batch() {
+        if (st) cudaStreamSynchronize(st);
+        s.clear();
+        for (void* p : dev) cudaFree(p);
+        if (st) cudaStreamDestroy(st);
+    }
+    template <class T> T* alloc(std::size_t n) {
+        void* p = nullptr;
+        SGPU_CUDA(cudaMalloc(&p, sizeof(T) * (n ? n : 1)));
+        SGPU_CUDA(cudaMemset(p, 0, sizeof(T) * (n ? n : 1)));
+        dev.push_back(p);
+        return static_cast<T*>(p);
+    }
 };
 struct sgpu_cnn {
     std::unique_ptr<sgpu::UNet> net;
@@ -1348,6 +1448,274 @@ int sgpu_cnn_sample(sgpu_handle* h, int max_size, float* in, float* target, int*
             throw sgpu::Error(SGPU_E_INVALID, "sgpu_cnn_sample: generate training pairs with precision = fp64");
         s.sync();
         s.sample_pair(s.lv, in, target);
+    });
+}
+
+
+// ---- batched cavities ----
+
+#define SGPU_NEED_BATCH(b)                                                                         \
+    do {                                                                                           \
+        if (!(b) || (b)->s.empty()) return sgpu::fail(SGPU_E_INVALID, "null batch");               \
+    } while (0)
+
+int sgpu_batch_create(const sgpu_params_t* params, int count, sgpu_batch** out) {
+    if (!params || !out || count < 1) return sgpu::fail(SGPU_E_INVALID, "sgpu_batch_create: bad arguments");
+    *out = nullptr;
+    return guarded([&] {
+        auto b = std::make_unique<sgpu_batch>();
+        for (int c = 0; c < count; ++c) {
+            const sgpu_params_t& p = params[c];
+            const std::string who = "sgpu_batch_create: cavity " + std::to_string(c) + ": ";
+            if (p.pressure_solver == SGPU_P_CG)
+                throw sgpu::Error(SGPU_E_INVALID, who + "pressure_solver = cg is not supported in a batch");
+            if (p.mg_mode == SGPU_MG_TOLERANCE)
+                throw sgpu::Error(SGPU_E_INVALID, who + "mg_mode = tolerance is not supported in a batch");
+            if (p.warm_start)
+                throw sgpu::Error(SGPU_E_INVALID, who + "warm_start = cnn is not supported in a batch");
+            b->s.push_back(std::make_unique<sgpu::Solver>(p, nullptr, nullptr, nullptr));
+        }
+        SGPU_CUDA(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+        b->seg_tuned.assign(count, 0);
+        for (auto& sv : b->s) sv->sync();
+        *out = b.release();
+    });
+}
+
+int sgpu_batch_destroy(sgpu_batch* b) {
+    if (!b) return SGPU_OK;
+    const int rc = guarded([&] { b->s.clear(); });
+    delete b;
+    return rc;
+}
+
+int sgpu_batch_count(sgpu_batch* b, int* count) {
+    SGPU_NEED_BATCH(b);
+    if (count) *count = static_cast<int>(b->s.size());
+    return SGPU_OK;
+}
+
+// Autotuner: the row-segment height of the streaming momentum sweep (the tile height of each
+// CTA's strip) per distinct grid, timed on the cavity's own scratch buffers.
+int sgpu_batch_autotune(sgpu_batch* b, int* chosen) {
+    SGPU_NEED_BATCH(b);
+    return guarded([&] {
+        std::map<std::tuple<int, int, int, int>, int> best;
+        for (std::size_t c = 0; c < b->s.size(); ++c) {
+            sgpu::Solver& sv = *b->s[c];
+            if (!sv.fast) continue;
+            const auto key = std::make_tuple(sv.prm.NX, sv.prm.NY, sv.dp.ncol, sv.mixed ? 1 : 0);
+            auto it = best.find(key);
+            if (it == best.end()) {
+                const int heur = sgpu::stream_seg_rows(sv.dp, sv.sms);
+                std::vector<int> cand = {heur};
+                for (int k : {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64})
+                    if (8 * sv.dp.ncol * k <= sv.dp.nrows + 8 * sv.dp.ncol) cand.push_back(8 * sv.dp.ncol * k);
+                cudaEvent_t e0, e1;
+                SGPU_CUDA(cudaEventCreate(&e0));
+                SGPU_CUDA(cudaEventCreate(&e1));
+                auto sweep = [&](int seg) {
+                    if (sv.mixed) sgpu::launch_corr_sweep(sv.dp, false, sv.e32[0], sv.e32[1], sv.rec32, true, seg, sv.st);
+                    else sgpu::launch_mom_sweep(sv.dp, false, sv.u, sv.tmp, sv.xF, sv.v, sv.pf, seg, sv.st);
+                };
+                int pick = heur;
+                float tbest = 1e30f;
+                for (int seg : cand) {
+                    sweep(seg);
+                    SGPU_CUDA(cudaEventRecord(e0, sv.st));
+                    for (int r = 0; r < 5; ++r) sweep(seg);
+                    SGPU_CUDA(cudaEventRecord(e1, sv.st));
+                    SGPU_CUDA(cudaEventSynchronize(e1));
+                    float ms = 0.0f;
+                    SGPU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                    if (ms < tbest) {
+                        tbest = ms;
+                        pick = seg;
+                    }
+                }
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                it = best.emplace(key, pick).first;
+            }
+            sv.seg_rows = it->second;
+            b->seg_tuned[c] = it->second;
+        }
+        if (chosen)
+            for (std::size_t c = 0; c < b->s.size(); ++c) chosen[c] = b->seg_tuned[c];
+    });
+}
+
+// All cavities in one graph launch: WHILE (any cavity active) { per cavity: IF (active) { one outer
+// iteration }; stopping test }. Each cavity's iteration is captured from its own solver into the
+// body of its IF node, so the cavities run as independent branches.
+int sgpu_batch_run(sgpu_batch* b, int maxit, int log_cap, double* seconds) {
+    SGPU_NEED_BATCH(b);
+    if (maxit < 0 || log_cap < 0) return sgpu::fail(SGPU_E_INVALID, "sgpu_batch_run: bad arguments");
+    return guarded([&] {
+        const int n = static_cast<int>(b->s.size());
+        if (!b->d_iters) {
+            b->d_iters = b->alloc<int>(n);
+            b->d_conv = b->alloc<int>(n);
+            b->d_last = b->alloc<double>(3 * static_cast<std::size_t>(n));
+        }
+        if (log_cap != b->log_cap) {
+            b->d_log = log_cap ? b->alloc<double>(static_cast<std::size_t>(n) * log_cap * 4) : nullptr;
+            b->log_cap = log_cap;
+        }
+        for (auto& sv : b->s) sv->sync();
+        SGPU_CUDA(cudaMemsetAsync(b->d_iters, 0, sizeof(int) * n, b->st));
+        SGPU_CUDA(cudaMemsetAsync(b->d_conv, 0, sizeof(int) * n, b->st));
+        SGPU_CUDA(cudaMemsetAsync(b->d_last, 0, sizeof(double) * 3 * n, b->st));
+        b->ran = 1;
+        if (maxit == 0) {
+            if (seconds) *seconds = 0.0;
+            SGPU_CUDA(cudaStreamSynchronize(b->st));
+            return;
+        }
+        std::vector<double*> res(n);
+        std::vector<double> tol(n);
+        std::vector<int> runmax(n), ones(n, 1);
+        for (int c = 0; c < n; ++c) {
+            res[c] = b->s[c]->res_dev;
+            tol[c] = b->s[c]->prm.error_tolerance;
+            runmax[c] = b->s[c]->prm.residual_normalisation == SGPU_NORM_RUNNING_MAX ? 1 : 0;
+        }
+        // per-run state (freed with the batch)
+        sgpu::BatchDev bd{};
+        bd.n = n;
+        bd.maxit = maxit;
+        double** d_res = b->alloc<double*>(n);
+        double* d_tol = b->alloc<double>(n);
+        int* d_runmax = b->alloc<int>(n);
+        int* d_active = b->alloc<int>(n);
+        SGPU_CUDA(cudaMemcpyAsync(d_res, res.data(), sizeof(double*) * n, cudaMemcpyHostToDevice, b->st));
+        SGPU_CUDA(cudaMemcpyAsync(d_tol, tol.data(), sizeof(double) * n, cudaMemcpyHostToDevice, b->st));
+        SGPU_CUDA(cudaMemcpyAsync(d_runmax, runmax.data(), sizeof(int) * n, cudaMemcpyHostToDevice, b->st));
+        SGPU_CUDA(cudaMemcpyAsync(d_active, ones.data(), sizeof(int) * n, cudaMemcpyHostToDevice, b->st));
+        bd.res = d_res;
+        bd.tol = d_tol;
+        bd.runmax = d_runmax;
+        bd.maxr = b->alloc<double>(3 * static_cast<std::size_t>(n));
+        bd.iters = b->d_iters;
+        bd.active = d_active;
+        bd.converged = b->d_conv;
+        bd.last = b->d_last;
+        bd.log = b->d_log;
+        bd.log_cap = b->log_cap;
+
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        auto cleanup = [&] {
+            if (exec) cudaGraphExecDestroy(exec);
+            if (g) cudaGraphDestroy(g);
+        };
+        try {
+            SGPU_CUDA(cudaGraphCreate(&g, 0));
+            SGPU_CUDA(cudaGraphConditionalHandleCreate(&bd.hw, g, 1, cudaGraphCondAssignDefault));
+            cudaGraphNodeParams wp{};
+            wp.type = cudaGraphNodeTypeConditional;
+            wp.conditional.handle = bd.hw;
+            wp.conditional.type = cudaGraphCondTypeWhile;
+            wp.conditional.size = 1;
+            cudaGraphNode_t wnode;
+            SGPU_CUDA(cudaGraphAddNode(&wnode, g, nullptr, 0, &wp));
+            cudaGraph_t body = wp.conditional.phGraph_out[0];
+            std::vector<cudaGraphConditionalHandle> hs(n);
+            for (int c = 0; c < n; ++c) SGPU_CUDA(cudaGraphConditionalHandleCreate(&hs[c], body, 0, 0));
+            auto* d_h = b->alloc<cudaGraphConditionalHandle>(n);
+            SGPU_CUDA(cudaMemcpyAsync(d_h, hs.data(), sizeof(cudaGraphConditionalHandle) * n,
+                                      cudaMemcpyHostToDevice, b->st));
+            bd.h = d_h;
+            void* args[] = {&bd};
+            cudaKernelNodeParams kp{};
+            kp.func = reinterpret_cast<void*>(&sgpu::k_batch_pre);
+            kp.gridDim = dim3(1);
+            kp.blockDim = dim3(256);
+            kp.kernelParams = args;
+            cudaGraphNode_t pre;
+            SGPU_CUDA(cudaGraphAddKernelNode(&pre, body, nullptr, 0, &kp));
+            std::vector<cudaGraphNode_t> ifs(n);
+            for (int c = 0; c < n; ++c) {
+                cudaGraphNodeParams ip{};
+                ip.type = cudaGraphNodeTypeConditional;
+                ip.conditional.handle = hs[c];
+                ip.conditional.type = cudaGraphCondTypeIf;
+                ip.conditional.size = 1;
+                SGPU_CUDA(cudaGraphAddNode(&ifs[c], body, &pre, 1, &ip));
+                cudaGraph_t ib = ip.conditional.phGraph_out[0];
+                sgpu::Solver& sv = *b->s[c];
+                SGPU_CUDA(cudaStreamBeginCaptureToGraph(sv.st, ib, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+                try {
+                    sv.iteration_enqueue(sv.res_dev);
+                } catch (...) {
+                    cudaGraph_t tmp = nullptr;
+                    cudaStreamEndCapture(sv.st, &tmp);
+                    throw;
+                }
+                cudaGraph_t captured = nullptr;
+                SGPU_CUDA(cudaStreamEndCapture(sv.st, &captured));
+            }
+            kp.func = reinterpret_cast<void*>(&sgpu::k_batch_step);
+            cudaGraphNode_t step;
+            SGPU_CUDA(cudaGraphAddKernelNode(&step, body, ifs.data(), ifs.size(), &kp));
+            SGPU_CUDA(cudaGraphInstantiate(&exec, g, 0));
+            cudaEvent_t e0, e1;
+            SGPU_CUDA(cudaEventCreate(&e0));
+            SGPU_CUDA(cudaEventCreate(&e1));
+            SGPU_CUDA(cudaEventRecord(e0, b->st));
+            SGPU_CUDA(cudaGraphLaunch(exec, b->st));
+            SGPU_CUDA(cudaEventRecord(e1, b->st));
+            SGPU_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.0f;
+            SGPU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            if (seconds) *seconds = ms * 1e-3;
+            sgpu::count_launch(); // the batch graph: one launch from the host
+        } catch (...) {
+            cleanup();
+            throw;
+        }
+        cleanup();
+    });
+}
+
+int sgpu_batch_results(sgpu_batch* b, int* iterations, int* converged, double* residuals) {
+    SGPU_NEED_BATCH(b);
+    if (!b->ran) return sgpu::fail(SGPU_E_INVALID, "sgpu_batch_results: the batch has not run");
+    return guarded([&] {
+        const int n = static_cast<int>(b->s.size());
+        if (iterations)
+            SGPU_CUDA(cudaMemcpyAsync(iterations, b->d_iters, sizeof(int) * n, cudaMemcpyDeviceToHost, b->st));
+        if (converged)
+            SGPU_CUDA(cudaMemcpyAsync(converged, b->d_conv, sizeof(int) * n, cudaMemcpyDeviceToHost, b->st));
+        if (residuals)
+            SGPU_CUDA(cudaMemcpyAsync(residuals, b->d_last, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, b->st));
+        SGPU_CUDA(cudaStreamSynchronize(b->st));
+    });
+}
+
+int sgpu_batch_log(sgpu_batch* b, double* host) {
+    SGPU_NEED_BATCH(b);
+    if (!host || !b->d_log) return sgpu::fail(SGPU_E_INVALID, "sgpu_batch_log: no log (run with log_cap > 0)");
+    return guarded([&] {
+        const std::size_t n = b->s.size() * static_cast<std::size_t>(b->log_cap) * 4;
+        SGPU_CUDA(cudaMemcpyAsync(host, b->d_log, sizeof(double) * n, cudaMemcpyDeviceToHost, b->st));
+        SGPU_CUDA(cudaStreamSynchronize(b->st));
+    });
+}
+
+int sgpu_batch_download(sgpu_batch* b, int index, int field_id, double* host) {
+    SGPU_NEED_BATCH(b);
+    if (index < 0 || index >= static_cast<int>(b->s.size()) || !host)
+        return sgpu::fail(SGPU_E_INVALID, "sgpu_batch_download: bad arguments");
+    return guarded([&] {
+        SGPU_CUDA(cudaStreamSynchronize(b->st));
+        sgpu::Solver& sv = *b->s[index];
+        double* f = sv.field_ptr(field_id);
+        if (!f) throw sgpu::Error(SGPU_E_INVALID, "sgpu_batch_download: unknown field id " + std::to_string(field_id));
+        sv.form_p_links_if_stale(field_id);
+        sv.download(f, host);
     });
 }
 

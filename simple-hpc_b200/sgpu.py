@@ -129,6 +129,15 @@ def lib() -> C.CDLL:
             "sgpu_attach_cnn": (I, [H, H, I]),
             "sgpu_warm_start_stats": (I, [H, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), D]),
             "sgpu_cnn_sample": (I, [H, I, F, F, C.POINTER(I), C.POINTER(I), C.POINTER(I)]),
+            # batched cavities
+            "sgpu_batch_create": (I, [P, I, C.POINTER(H)]),
+            "sgpu_batch_destroy": (I, [H]),
+            "sgpu_batch_count": (I, [H, C.POINTER(I)]),
+            "sgpu_batch_autotune": (I, [H, C.POINTER(I)]),
+            "sgpu_batch_run": (I, [H, I, I, D]),
+            "sgpu_batch_results": (I, [H, C.POINTER(I), C.POINTER(I), D]),
+            "sgpu_batch_log": (I, [H, D]),
+            "sgpu_batch_download": (I, [H, I, I, D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -154,6 +163,65 @@ def _fptr(a: np.ndarray | None):
         return None
     assert a.dtype == np.float32 and a.flags.c_contiguous
     return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Batch:
+    """Independent cavities solved in one graph launch (sgpu_batch_*)."""
+
+    def __init__(self, params: list[Params]):
+        arr = (Params * len(params))(*params)
+        h = C.c_void_p()
+        _check(lib().sgpu_batch_create(arr, len(params), C.byref(h)))
+        self._h = h
+        self.params = list(params)
+        self.log_cap = 0
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().sgpu_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def autotune(self) -> list[int]:
+        out = (C.c_int * len(self.params))()
+        _check(lib().sgpu_batch_autotune(self._h, out))
+        return list(out)
+
+    def run(self, maxit: int, log_cap: int = 0) -> float:
+        """Run all cavities; returns the device seconds of the launch."""
+        sec = C.c_double()
+        _check(lib().sgpu_batch_run(self._h, maxit, log_cap, C.byref(sec)))
+        self.log_cap = log_cap
+        return sec.value
+
+    def results(self) -> dict:
+        n = len(self.params)
+        its, conv = (C.c_int * n)(), (C.c_int * n)()
+        res = np.zeros((n, 3))
+        _check(lib().sgpu_batch_results(self._h, its, conv, _dptr(res)))
+        return {"iterations": np.array(its), "converged": np.array(conv, bool), "residuals": res}
+
+    def log(self) -> np.ndarray:
+        out = np.zeros((len(self.params), self.log_cap, 4))
+        _check(lib().sgpu_batch_log(self._h, _dptr(out)))
+        return out
+
+    def download(self, index: int, field_id: int) -> np.ndarray:
+        p = self.params[index]
+        out = np.empty((p.nrows, p.ncols))
+        _check(lib().sgpu_batch_download(self._h, index, field_id, _dptr(out)))
+        return out
 
 
 class Cnn:

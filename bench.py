@@ -272,6 +272,134 @@ def e2e_measure(sgpu, torch, p, steps: int, world: int) -> dict:
             "d2h_bytes_per_step": 24 + 3 * fb / res.iterations}
 
 
+# ---- batched workload: many cavities of uneven size and Re in one graph launch ----
+
+BATCH_SIZES = (64, 96, 128, 192, 256, 384, 512)
+BATCH_METRIC = ("cavities solved to 1e-5 per second: N uniform in {64,96,128,192,256,384,512}, Re "
+                "log-uniform in [100, 5000], QUICK + 2nd-order diffusion, mixed-precision mg, one graph launch")
+
+
+def batch_manifest(count: int, seed: int) -> list[tuple[int, float]]:
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    ns = rng.choice(BATCH_SIZES, count)
+    res = np.exp(rng.uniform(np.log(100.0), np.log(5000.0), count))
+    return [(int(n), float(r)) for n, r in zip(ns, res)]
+
+
+def batch_config(n: int, re: float, precision: str | None, maxit: int) -> str:
+    text = (f"N_cells_x = {n}\nN_cells_y = {n}\nRe = {re!r}\nconvection_scheme = QUICK\n"
+            f"diffusion_order = 2\nmomentum_solver = gs_multicolour\npressure_solver = mg\n"
+            f"error_tolerance = 1e-5\nmaxit = {maxit}\nbackend = gpu\n")
+    return text + (f"precision = {precision}\n" if precision else "")
+
+
+def batch_shard(manifest, world: int, rank: int):
+    """Size-balanced partition (cost ~ N^3: cells x iterations), no collective needed."""
+    load = [0.0] * world
+    mine = []
+    for idx in sorted(range(len(manifest)), key=lambda i: -manifest[i][0]):
+        r = min(range(world), key=lambda k: load[k])
+        load[r] += float(manifest[idx][0]) ** 3
+        if r == rank:
+            mine.append(idx)
+    return sorted(mine)
+
+
+def run_batch_workload(args, rank: int, world: int, local: int) -> None:
+    import numpy as np
+    import torch
+    import sgpu
+    torch.cuda.set_device(local)
+    manifest = batch_manifest(args.cavities, args.seed)
+    mine = batch_shard(manifest, world, rank)
+    params = [sgpu.params_from_config(batch_config(*manifest[i], "mixed", args.batch_maxit)) for i in mine]
+    # warm-up: short runs of a separate batch of the same cavities (module load, graph paths)
+    with sgpu.Batch(params) as wb:
+        wb.autotune()
+        for _ in range(args.warmup):
+            wb.run(2)
+    t_wall0 = time.perf_counter()
+    b = sgpu.Batch(params)
+    chosen = b.autotune()
+    barrier(world)
+    torch.cuda.synchronize()
+    secs = b.run(args.batch_maxit)
+    torch.cuda.synchronize()
+    barrier(world)
+    r = b.results()
+    fields = {i: [b.download(k, f) for f in (0, 1, 2)] for k, i in enumerate(mine)}
+    wall = time.perf_counter() - t_wall0
+    secs_max = allmax(secs, world)
+    wall_max = allmax(wall, world)
+    converged = int(r["converged"].sum())
+    its = {i: int(r["iterations"][k]) for k, i in enumerate(mine)}
+    b.close()
+    out_bytes = sum(3 * 8 * p.nrows * p.ncols for p in params)
+    # per-cavity error against individual FP64 runs, on the smallest cavities of this rank
+    errs = []
+    for i in sorted(mine, key=lambda i: manifest[i][0])[:args.batch_check]:
+        p64 = sgpu.params_from_config(batch_config(*manifest[i], None, args.batch_maxit))
+        with sgpu.Solver(p64) as s:
+            res, _ = s.run(args.batch_maxit)
+            ref = [s.download(f) for f in (0, 1, 2)]
+        e = {"cavity": i, "N": manifest[i][0], "Re": round(manifest[i][1], 1), "iterations_fp64": res.iterations,
+             "iterations_batch": its[i]}
+        for name, a, x in zip("uvp", fields[i], ref):
+            e[f"max_rel_{name}"] = float(np.max(np.abs(a - x)) / np.max(np.abs(x)))
+            e[f"l2_rel_{name}"] = float(np.linalg.norm(a - x) / np.linalg.norm(x))
+        errs.append(e)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = batch_cpu_estimate(manifest, its, args.cpu_seconds)
+    if rank == 0:
+        line = {
+            "metric": BATCH_METRIC, "value": len(manifest) / secs_max, "unit": "cavities/s",
+            "n_gpus": world, "steps": 1, "warmup": args.warmup, "ms_per_step": 1e3 * secs_max,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64 (outer) + f32 (inner solves)",
+            "data": f"synthetic (seeded manifest, seed {args.seed}; cavity initial state)",
+            "config": {"workload": f"{len(manifest)} cavities, batch to 1e-5 (maxit {args.batch_maxit}), "
+                                   "one CUDA graph launch per rank (WHILE over per-cavity IF branches)",
+                       "cavities": len(manifest), "sizes": list(BATCH_SIZES),
+                       "parallelism": f"size-balanced shard x{world}", "step": "the whole batched solve",
+                       "autotuned_row_segments": sorted(set(chosen))},
+            "converged": converged if world == 1 else None,
+            "iterations": {"min": min(its.values()), "max": max(its.values()),
+                           "sum": sum(its.values())} if world == 1 else None,
+            "e2e": {"value": len(manifest) / wall_max, "unit": "cavities/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": out_bytes,
+                    "note": "batch creation, autotune, graph build, launch and download of every u, v, p"},
+            "gpu_launches": 1,
+            "errors_vs_fp64_single_runs": errs,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def batch_cpu_estimate(manifest, its: dict, budget: float) -> dict:
+    """The reference's OpenMP outer iteration timed per distinct N (bounded sample), times the
+    batch's iteration counts: the CPU time the reference would need for the same cavities."""
+    per_n = {}
+    spent = 0.0
+    cores, kind = 1, "port"
+    for n in sorted({m[0] for m in manifest}):
+        engine, kind, cores = reference_engine(batch_config(n, 1000.0, None, 10), n)
+        engine.outer_iteration()
+        k, secs = 0, 0.0
+        while k < 3 and (k == 0 or spent + secs < budget):
+            secs += time_cpu_iterations(engine, 1)
+            k += 1
+        engine.close()
+        spent += secs
+        per_n[n] = secs / k
+    est = sum(its[i] * per_n[manifest[i][0]] for i in its)
+    return {"value": len(manifest) / est, "unit": "cavities/s", "cores": cores, "kind": kind,
+            "sample": "outer iterations timed per N ({}); estimate = sum over cavities of the batch's "
+                      "iteration count x that time ({:.0f} s)".format(
+                          ", ".join(f"{n}: {1e3 * t:.2f} ms" for n, t in per_n.items()), est)}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -283,14 +411,34 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-arm", action="store_true")
+    ap.add_argument("--workload", default="cavity", choices=["cavity", "batch"])
+    ap.add_argument("--cavities", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--batch-maxit", type=int, default=60000)
+    ap.add_argument("--batch-check", type=int, default=8)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
 
     rank, world, local = dist_init()
+    if args.impl == "reference" and args.workload == "batch":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched mode and "
+                              "needs hours per 512^2 cavity; the batch line's cpu_baseline times its outer "
+                              "iteration per size and scales by the batch's iteration counts"}), flush=True)
+        barrier(world)
+        return
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
         barrier(world)
+        return
+
+    if args.workload == "batch":
+        run_batch_workload(args, rank, world, local)
+        barrier(world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
 
     import torch

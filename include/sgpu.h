@@ -280,7 +280,11 @@ int sgpu_cnn_train_step(sgpu_cnn* c, const float* in, const float* target, int n
                         float lr, float* loss);
 /* Attach a network to a handle (not owned: keep it alive while attached; NULL detaches). */
 int sgpu_attach_cnn(sgpu_handle* h, sgpu_cnn* c, int max_size);
-/* Warm starts applied, guesses discarded, and the last guess's ||b - A p'|| / ||b||. */
+/* Switch the handle's multigrid stopping mode (keys mg_mode, pressure_tolerance, pressure_maxit)
+ * between outer iterations, e.g. to solve p' tightly only where a training pair is sampled. */
+int sgpu_set_mg_mode(sgpu_handle* h, int mg_mode, double pressure_tolerance, int pressure_maxit);
+/* Warm starts applied, guesses discarded, and the residual ||b - A p'|| / ||b|| after the first
+ * V-cycle from the last guess. */
 int sgpu_warm_start_stats(sgpu_handle* h, long long* used, long long* fallbacks, double* rel_initial);
 /* Training pair from the handle's last p' solve (precision = fp64, pressure_solver = mg): the
  * network input of the finest level of at most max_size x max_size cells (nx x ny x 2) and the

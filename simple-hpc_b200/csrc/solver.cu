@@ -16,6 +16,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -599,9 +600,10 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
             }
         }
         coarse_rowbuf = dalloc<double>(static_cast<std::size_t>(maxnx) + 1);
-        // Streaming V-cycle: levels above kTailCells cells get a second iterate buffer; the rest
-        // run in the single-CTA tail kernel.
-        constexpr int kTailCells = 1024;
+        // Streaming V-cycle: levels above tail_cells cells get a second iterate buffer; the rest
+        // run in the single-CTA tail kernel. SGPU_MG_TAIL_CELLS overrides the split (tuning).
+        int kTailCells = 1024;
+        if (const char* e = std::getenv("SGPU_MG_TAIL_CELLS")) kTailCells = std::max(16, std::atoi(e));
         mg_fast = mg_fast_supported(p.mg_pre, p.mg_post) && p.mg_pre >= 1 && nl <= 24;
         mg_tail = 0;
         while (mg_tail < nl - 1 && lv[mg_tail].nx * lv[mg_tail].ny > kTailCells) ++mg_tail;
@@ -1419,6 +1421,20 @@ int sgpu_attach_cnn(sgpu_handle* h, sgpu_cnn* c, int max_size) {
         s.own_net.reset();
         s.net = c ? c->net.get() : nullptr;
         s.cnn_max = max_size;
+    });
+}
+
+int sgpu_set_mg_mode(sgpu_handle* h, int mg_mode, double pressure_tolerance, int pressure_maxit) {
+    SGPU_NEED_HANDLE(h);
+    if ((mg_mode != SGPU_MG_FIXED && mg_mode != SGPU_MG_TOLERANCE) || !(pressure_tolerance > 0.0) ||
+        pressure_maxit < 1)
+        return sgpu::fail(SGPU_E_INVALID, "sgpu_set_mg_mode: bad arguments");
+    return guarded([&] {
+        sgpu::Solver& s = *h->s;
+        s.sync();
+        s.prm.mg_mode = mg_mode;
+        s.prm.pressure_tolerance = pressure_tolerance;
+        s.prm.pressure_maxit = pressure_maxit;
     });
 }
 

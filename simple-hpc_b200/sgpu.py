@@ -128,6 +128,7 @@ def lib() -> C.CDLL:
             "sgpu_cnn_train_step": (I, [H, F, F, I, I, I, C.c_float, F]),
             "sgpu_attach_cnn": (I, [H, H, I]),
             "sgpu_warm_start_stats": (I, [H, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), D]),
+            "sgpu_set_mg_mode": (I, [H, I, C.c_double, I]),
             "sgpu_cnn_sample": (I, [H, I, F, F, C.POINTER(I), C.POINTER(I), C.POINTER(I)]),
             # batched cavities
             "sgpu_batch_create": (I, [P, I, C.POINTER(H)]),
@@ -462,6 +463,9 @@ class Solver:
 
     def load_cnn(self, path) -> None:
         _check(lib().sgpu_cnn_load(self._h, str(path).encode()))
+
+    def set_mg_mode(self, tolerance: bool, pressure_tolerance: float = 1e-6, pressure_maxit: int = 1000) -> None:
+        _check(lib().sgpu_set_mg_mode(self._h, 1 if tolerance else 0, pressure_tolerance, pressure_maxit))
 
     def warm_start_stats(self) -> dict:
         u, f, r = C.c_longlong(), C.c_longlong(), C.c_double()

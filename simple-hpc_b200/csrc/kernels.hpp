@@ -134,6 +134,8 @@ void launch_cg_dir(const DevParams& p, CgPtr cg, const CgScalars* sc, cudaStream
 
 // ---- mixed precision (mixed.cu) ----
 void init_mixed_kernels();
+// Resident CTAs per SM of the FP32 correction sweep (its register and shared-memory footprint).
+int corr_blocks_per_sm(int ncol);
 // FP64 prep: |R| into cells, AP (FP64), and per cell a 48-byte FP32 record (3 float4:
 // AE AW AN AS | AEE AWW ANN ASS | 1/AP R 0 0) at rec + 3 * (i * pitch + j), over the update range.
 void launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x, const double* oth,
@@ -155,7 +157,8 @@ void launch_correct_mixed(const DevParams& p, const LevelView32& L0, const doubl
                           double* pc64, cudaStream_t st);
 
 // ---- fused fast path (fused.cu) ----
-int stream_seg_rows(const DevParams& p, int sms);
+// Rows per CTA segment of the streaming sweeps: one wave of blocks_per_sm resident CTAs per SM.
+int stream_seg_rows(const DevParams& p, int sms, int blocks_per_sm = 2);
 // Momentum prep: |R| into cells, AP over the update range, frozen copy xF of x.
 void launch_mom_prep(const DevParams& p, bool v_component, const double* x, const double* oth,
                      const double* pf, double* xF, double* AP, double* cells, cudaStream_t st);

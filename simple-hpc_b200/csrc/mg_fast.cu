@@ -88,9 +88,18 @@ __device__ __forceinline__ void rb_update(T (*ring)[NT], int I, int tid, const T
     row[tid] = x;
 }
 
+// The coefficient loads of a step are issued PD steps before the step runs, into one of PD
+// register sets used in rotation (the step loop is unrolled by PD so every set index is a
+// compile-time constant): a step then waits on loads issued PD steps earlier, not on a memory round
+// trip of its own.
+template <int NC, class T> struct StepRegs {
+    int I[NC];
+    bool ok[NC];
+    T a[NC][6];
+};
+
 // PRE red-black sweeps, residual and restriction in one streaming pass (see the file comment).
-// Each step prefetches the next step's coefficients into registers.
-template <int NT, int PRE, class T>
+template <int NT, int PRE, int PD, class T>
 __global__ void __launch_bounds__(NT, 2)
     k_mg_down(LevelViewT<T> L, LevelViewT<T> C, T* __restrict__ xout, int x_zero, int seg_rows,
               int HC) {
@@ -114,58 +123,43 @@ __global__ void __launch_bounds__(NT, 2)
         cp_async_commit();
         ++next;
     };
-    // Cells of step t: PRE updates (rows t - 2c - 4 sw) and the residual (row t - 4 PRE).
+    // Cells of step t: PRE updates (rows t - 2c - 4 sw) and the residual (row t - 4 PRE), with
+    // their six inputs loaded.
     constexpr int NC = PRE + 1;
-    auto cells = [&](int t, int* I, bool* ok) {
+    auto prepare = [&](int t, StepRegs<NC, T>& r) {
         const int cpar = (t + Jc + 4) & 1;
 #pragma unroll
         for (int sw = 0; sw < PRE; ++sw) {
-            I[sw] = t - 2 * cpar - 4 * sw;
-            ok[sw] = cint && I[sw] >= 0 && I[sw] < L.nx && in_cone(w, I[sw], Jc, 2 * sw + cpar, NT);
+            r.I[sw] = t - 2 * cpar - 4 * sw;
+            r.ok[sw] = cint && r.I[sw] >= 0 && r.I[sw] < L.nx && in_cone(w, r.I[sw], Jc, 2 * sw + cpar, NT);
         }
-        I[PRE] = t - 4 * PRE;
-        ok[PRE] = cint && I[PRE] >= 0 && I[PRE] < L.nx && in_cone(w, I[PRE], Jc, 2 * PRE, NT);
+        r.I[PRE] = t - 4 * PRE;
+        r.ok[PRE] = cint && r.I[PRE] >= 0 && r.I[PRE] < L.nx && in_cone(w, r.I[PRE], Jc, 2 * PRE, NT);
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+            if (r.ok[c]) load6(L, r.I[c] * s + Jc, r.a[c]);
     };
     for (int k = 0; k < kPD + 2; ++k) issue(); // rows L0 .. L0 + 1 + kPD
 
-    int In[NC];
-    bool okn[NC];
-    T an[NC][6];
-    cells(w.L0, In, okn);
+    StepRegs<NC, T> S[PD];
 #pragma unroll
-    for (int c = 0; c < NC; ++c)
-        if (okn[c]) load6(L, In[c] * s + Jc, an[c]);
+    for (int d = 0; d < PD; ++d) prepare(w.L0 + d, S[d]);
 
     const int t_last = w.R1 - 1 + 4 * PRE;
     T r_prev = T(0);
-    for (int t = w.L0; t <= t_last; ++t) {
+    auto step = [&](int t, StepRegs<NC, T>& R) {
         cp_async_wait<kPD>(); // rows <= t + 1 have landed
         __syncthreads();
         issue();
-        int I[NC];
-        bool ok[NC];
-        T a[NC][6];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            I[c] = In[c];
-            ok[c] = okn[c];
-#pragma unroll
-            for (int m = 0; m < 6; ++m) a[c][m] = an[c][m];
-        }
-        cells(t + 1, In, okn);
-#pragma unroll
-        for (int c = 0; c < NC; ++c)
-            if (okn[c]) load6(L, In[c] * s + Jc, an[c]);
-
 #pragma unroll
         for (int sw = 0; sw < PRE; ++sw)
-            if (ok[sw]) rb_update<NT>(ring, I[sw], tid, a[sw]);
+            if (R.ok[sw]) rb_update<NT>(ring, R.I[sw], tid, R.a[sw]);
         // Residual of row Ir = t - 4 PRE (multigrid.cpp:84-85): its neighbours are final.
-        const int Ir = I[PRE];
+        const int Ir = R.I[PRE];
         T r = T(0);
-        if (ok[PRE]) {
+        if (R.ok[PRE]) {
             const T* row = ring[Ir & (kRing - 1)];
-            const T* aa = a[PRE];
+            const T* aa = R.a[PRE];
             r = aa[5] - (aa[4] * row[tid] -
                          (aa[0] * row[tid + 1] + aa[1] * row[tid - 1] +
                           aa[3] * ring[(Ir + 1) & (kRing - 1)][tid] +
@@ -175,9 +169,9 @@ __global__ void __launch_bounds__(NT, 2)
         if ((Ir & 1) && Ir >= 1) { // uniform over the CTA
             const T rp_odd = __shfl_down_sync(0xffffffffu, r_prev, 1);
             const T r_odd = __shfl_down_sync(0xffffffffu, r, 1);
-            const int R = Ir >> 1;
-            if (cown && !(Jc & 1) && Ir - 1 >= w.R0 && Ir < w.R1 && R < C.nx) {
-                const int cq = R * C.stride + (Jc >> 1);
+            const int Rc = Ir >> 1;
+            if (cown && !(Jc & 1) && Ir - 1 >= w.R0 && Ir < w.R1 && Rc < C.nx) {
+                const int cq = Rc * C.stride + (Jc >> 1);
                 C.b[cq] = r_prev + rp_odd + r + r_odd;
                 C.x[cq] = T(0);
             }
@@ -186,12 +180,18 @@ __global__ void __launch_bounds__(NT, 2)
         // The smoothed iterate: row t - 4 PRE + 1 had its last update at step t - 1.
         const int rw = t - 4 * PRE + 1;
         if (cown && rw >= w.R0 && rw < w.R1) xout[rw * s + Jc] = ring[rw & (kRing - 1)][tid];
+        prepare(t + PD, R); // this set's next use is PD steps on
+    };
+    for (int t = w.L0; t <= t_last; t += PD) {
+#pragma unroll
+        for (int d = 0; d < PD; ++d)
+            if (t + d <= t_last) step(t + d, S[d]);
     }
     cp_async_wait<0>();
 }
 
 // Prolongation and POST red-black sweeps in one streaming pass (see the file comment).
-template <int NT, int POST, class T>
+template <int NT, int POST, int PD, class T>
 __global__ void __launch_bounds__(NT, 2)
     k_mg_up(LevelViewT<T> C, LevelViewT<T> L, const T* __restrict__ xin, T* __restrict__ xout,
             double omega, int seg_rows, int HC) {
@@ -212,58 +212,38 @@ __global__ void __launch_bounds__(NT, 2)
         cp_async_commit();
         ++next;
     };
-    auto cells = [&](int t, int* I, bool* ok) {
+    constexpr int NC = POST > 0 ? POST : 1;
+    auto prepare = [&](int t, StepRegs<NC, T>& r) {
         const int cpar = (t + Jc + 4) & 1;
 #pragma unroll
         for (int sw = 0; sw < POST; ++sw) {
-            I[sw] = t - 2 * cpar - 4 * sw;
-            ok[sw] = cint && I[sw] >= 0 && I[sw] < L.nx && in_cone(w, I[sw], Jc, 2 * sw + cpar, NT);
+            r.I[sw] = t - 2 * cpar - 4 * sw;
+            r.ok[sw] = cint && r.I[sw] >= 0 && r.I[sw] < L.nx && in_cone(w, r.I[sw], Jc, 2 * sw + cpar, NT);
+            if (r.ok[sw]) load6(L, r.I[sw] * s + Jc, r.a[sw]);
         }
     };
-    for (int k = 0; k < kPD + 3; ++k) issue(); // rows L0 .. L0 + 2 + kPD
-
-    constexpr int NC = POST > 0 ? POST : 1;
-    int In[NC];
-    bool okn[NC];
-    T an[NC][6];
-    const int t0 = w.L0 - 2;
-    if (POST > 0) {
-        cells(t0, In, okn);
-#pragma unroll
-        for (int c = 0; c < POST; ++c)
-            if (okn[c]) load6(L, In[c] * s + Jc, an[c]);
-    }
     auto coarse_at = [&](int Ip) {
         return (cint && Ip >= 0 && Ip < L.nx && Ip < w.L1)
                    ? __ldg(C.x + (Ip >> 1) * C.stride + (Jc >> 1))
                    : T(0);
     };
-    T cxn = coarse_at(t0 + 2); // coarse correction of the next row to prolong
+    for (int k = 0; k < kPD + 3; ++k) issue(); // rows L0 .. L0 + 2 + kPD
+
+    const int t0 = w.L0 - 2;
+    StepRegs<NC, T> S[PD];
+    T cxs[PD]; // coarse correction of row t + 2 for each set's step
+#pragma unroll
+    for (int d = 0; d < PD; ++d) {
+        prepare(t0 + d, S[d]);
+        cxs[d] = coarse_at(t0 + d + 2);
+    }
 
     const int t_last = w.R1 - 1 + 4 * POST;
-    for (int t = t0; t <= t_last; ++t) {
+    auto step = [&](int t, StepRegs<NC, T>& R, T& cx) {
         if (t >= w.L0) cp_async_wait<kPD>(); // rows <= t + 2 have landed
         else cp_async_wait<kPD + 1>();
         __syncthreads();
         if (t >= w.L0) issue();
-        int I[NC];
-        bool ok[NC];
-        T a[NC][6];
-        if (POST > 0) {
-#pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                I[c] = In[c];
-                ok[c] = okn[c];
-#pragma unroll
-                for (int m = 0; m < 6; ++m) a[c][m] = an[c][m];
-            }
-            cells(t + 1, In, okn);
-#pragma unroll
-            for (int c = 0; c < NC; ++c)
-                if (okn[c]) load6(L, In[c] * s + Jc, an[c]);
-        }
-        const T cx = cxn;
-        cxn = coarse_at(t + 3);
         // Prolongation of row t + 2 (read first at step t + 1): x += omega * coarse x.
         const int Ip = t + 2;
         if (cint && Ip >= 0 && Ip < L.nx && Ip < w.L1) {
@@ -272,14 +252,23 @@ __global__ void __launch_bounds__(NT, 2)
         }
 #pragma unroll
         for (int sw = 0; sw < POST; ++sw)
-            if (ok[sw]) rb_update<NT>(ring, I[sw], tid, a[sw]);
+            if (R.ok[sw]) rb_update<NT>(ring, R.I[sw], tid, R.a[sw]);
         const int rw = t - 4 * POST + 1;
         if (cown && rw >= w.R0 && rw < w.R1) xout[rw * s + Jc] = ring[rw & (kRing - 1)][tid];
+        prepare(t + PD, R);
+        cx = coarse_at(t + PD + 2);
+    };
+    for (int t = t0; t <= t_last; t += PD) {
+#pragma unroll
+        for (int d = 0; d < PD; ++d)
+            if (t + d <= t_last) step(t + d, S[d], cxs[d]);
     }
     cp_async_wait<0>();
 }
 
 constexpr int kNT = 256;
+// Register sets in the coefficient pipeline (steps of prefetch): FP32 cells are half the registers.
+template <class T> constexpr int kStepPrefetch = sizeof(T) == 4 ? 3 : 2;
 
 int seg_for(int nx, int ny, int HC, int sms) {
     const int W = kNT - 2 * HC;
@@ -308,8 +297,9 @@ void down_t(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, bool x_zero
     const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
     constexpr int smem = kRing * kNT * static_cast<int>(sizeof(T));
     static bool attr = false;
-    allow_smem(k_mg_down<kNT, PRE, T>, smem, attr);
-    k_mg_down<kNT, PRE, T><<<grid, kNT, smem, st>>>(F, C, xout, x_zero ? 1 : 0, seg, HC);
+    constexpr int PD = kStepPrefetch<T>;
+    allow_smem(k_mg_down<kNT, PRE, PD, T>, smem, attr);
+    k_mg_down<kNT, PRE, PD, T><<<grid, kNT, smem, st>>>(F, C, xout, x_zero ? 1 : 0, seg, HC);
     SGPU_LAUNCH();
 }
 
@@ -322,8 +312,9 @@ void up_t(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, T* xout,
     const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
     constexpr int smem = kRing * kNT * static_cast<int>(sizeof(T));
     static bool attr = false;
-    allow_smem(k_mg_up<kNT, POST, T>, smem, attr);
-    k_mg_up<kNT, POST, T><<<grid, kNT, smem, st>>>(C, F, xin, xout, omega, seg, HC);
+    constexpr int PD = kStepPrefetch<T>;
+    allow_smem(k_mg_up<kNT, POST, PD, T>, smem, attr);
+    k_mg_up<kNT, POST, PD, T><<<grid, kNT, smem, st>>>(C, F, xin, xout, omega, seg, HC);
     SGPU_LAUNCH();
 }
 

@@ -372,4 +372,14 @@ void init_mixed_kernels() {
     SGPU_CUDA(cudaFuncSetAttribute(k_corr_stream<2, true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
 }
 
+int corr_blocks_per_sm(int ncol) {
+    const int smem = kRing * 256 * static_cast<int>(sizeof(float));
+    int n = 0;
+    if (ncol == 5)
+        SGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_corr_stream<5, false, 256>, 256, smem));
+    else
+        SGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_corr_stream<2, false, 256>, 256, smem));
+    return n > 0 ? n : 1;
+}
+
 } // namespace sgpu

@@ -602,7 +602,7 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
         coarse_rowbuf = dalloc<double>(static_cast<std::size_t>(maxnx) + 1);
         // Streaming V-cycle: levels above tail_cells cells get a second iterate buffer; the rest
         // run in the single-CTA tail kernel. SGPU_MG_TAIL_CELLS overrides the split (tuning).
-        int kTailCells = 1024;
+        int kTailCells = 4096;
         if (const char* e = std::getenv("SGPU_MG_TAIL_CELLS")) kTailCells = std::max(16, std::atoi(e));
         mg_fast = mg_fast_supported(p.mg_pre, p.mg_post) && p.mg_pre >= 1 && nl <= 24;
         mg_tail = 0;
@@ -628,6 +628,7 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
                         "mg and 1 <= mg_pre <= 4, 0 <= mg_post <= 4");
         mixed = true;
         init_mixed_kernels();
+        seg_rows = stream_seg_rows(dp, sms, corr_blocks_per_sm(dp.ncol));
         rec32 = dalloc<float4>(3 * g.elems());
         e32[0] = dalloc<float>(g.elems());
         e32[1] = dalloc<float>(g.elems());
@@ -1523,7 +1524,7 @@ int sgpu_batch_autotune(sgpu_batch* b, int* chosen) {
             const auto key = std::make_tuple(sv.prm.NX, sv.prm.NY, sv.dp.ncol, sv.mixed ? 1 : 0);
             auto it = best.find(key);
             if (it == best.end()) {
-                const int heur = sgpu::stream_seg_rows(sv.dp, sv.sms);
+                const int heur = sv.seg_rows;
                 std::vector<int> cand = {heur};
                 for (int k : {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64})
                     if (8 * sv.dp.ncol * k <= sv.dp.nrows + 8 * sv.dp.ncol) cand.push_back(8 * sv.dp.ncol * k);

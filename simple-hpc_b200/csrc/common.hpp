@@ -87,6 +87,20 @@ struct DevParams {
 // Multigrid level view (the reference's MGView, include/simple/multigrid.hpp:59-66): element
 // (I, J), 0 <= I < nx, 0 <= J < ny, of each array is ptr[I * stride + J]; the pointers address
 // interior cell (0, 0) and every neighbour of an interior cell lies inside the allocation.
+#ifdef __CUDACC__
+// The red-black update value of multigrid.cpp:61-63, x = b / AP; x += nb / AP. The double
+// instances keep the reference's two divisions (bit parity); the float instances (the mixed-precision
+// V-cycle, where no bit parity applies) divide once, (b + nb) / AP, correctly rounded.
+__device__ __forceinline__ double rb_value(double b, double nb, double ap) {
+    double t = b / ap;
+    t += nb / ap;
+    return t;
+}
+__device__ __forceinline__ float rb_value(float b, float nb, float ap) {
+    return __fdiv_rn(b + nb, ap);
+}
+#endif
+
 template <class T> struct LevelViewT {
     int nx, ny, stride;
     T *AE, *AW, *AN, *AS, *AP, *b, *x, *r;

@@ -40,9 +40,8 @@ template <class T> __global__ void k_mg_smooth(LevelViewT<T> L, int colour) {
     if (I >= L.nx || J >= L.ny || ((I + J) & 1) != colour) return;
     const int s = L.stride, q = I * s + J;
     T* x = L.x;
-    T t = L.b[q] / L.AP[q];
-    t += (L.AE[q] * x[q + 1] + L.AW[q] * x[q - 1] + L.AS[q] * x[q + s] + L.AN[q] * x[q - s]) / L.AP[q];
-    x[q] = t;
+    x[q] = rb_value(L.b[q], L.AE[q] * x[q + 1] + L.AW[q] * x[q - 1] + L.AS[q] * x[q + s] + L.AN[q] * x[q - s],
+                    L.AP[q]);
 }
 
 template <class T> __global__ void k_mg_residual(LevelViewT<T> L) {
@@ -142,10 +141,9 @@ template <class T> __device__ void cta_smooth_colour(const LevelViewT<T>& L, int
         const int I = k / L.ny, J = k % L.ny;
         if (((I + J) & 1) != colour) continue;
         const int q = I * s + J;
-        T t = L.b[q] / L.AP[q];
-        t += (L.AE[q] * x[q + 1] + L.AW[q] * x[q - 1] + L.AS[q] * x[q + s] + L.AN[q] * x[q - s]) /
-             L.AP[q];
-        x[q] = t;
+        x[q] = rb_value(L.b[q],
+                        L.AE[q] * x[q + 1] + L.AW[q] * x[q - 1] + L.AS[q] * x[q + s] + L.AN[q] * x[q - s],
+                        L.AP[q]);
     }
     __syncthreads();
 }

@@ -81,11 +81,10 @@ template <class T> __device__ __forceinline__ void load6(const LevelViewT<T>& L,
 template <int NT, class T>
 __device__ __forceinline__ void rb_update(T (*ring)[NT], int I, int tid, const T a[6]) {
     T* row = ring[I & (kRing - 1)];
-    T x = a[5] / a[4];
-    x += (a[0] * row[tid + 1] + a[1] * row[tid - 1] + a[3] * ring[(I + 1) & (kRing - 1)][tid] +
-          a[2] * ring[(I - 1) & (kRing - 1)][tid]) /
-         a[4];
-    row[tid] = x;
+    row[tid] = rb_value(a[5],
+                        a[0] * row[tid + 1] + a[1] * row[tid - 1] + a[3] * ring[(I + 1) & (kRing - 1)][tid] +
+                            a[2] * ring[(I - 1) & (kRing - 1)][tid],
+                        a[4]);
 }
 
 // The coefficient loads of a step are issued PD steps before the step runs, into one of PD

@@ -101,11 +101,43 @@ __device__ __forceinline__ float rb_value(float b, float nb, float ap) {
 }
 #endif
 
+// The four links of one FP32 multigrid cell, read with one 128-bit load.
+struct alignas(16) Link4 {
+    float e, w, n, s;
+};
+
+// One multigrid level (interior origin at AE..r, row stride `stride`). Double levels (the reference's
+// bits) keep the links in the arrays AE, AW, AN, AS; float levels (the mixed-precision V-cycle) keep
+// them in L4, one record per cell, and leave those four arrays null.
 template <class T> struct LevelViewT {
     int nx, ny, stride;
     T *AE, *AW, *AN, *AS, *AP, *b, *x, *r;
+    Link4* L4 = nullptr;
 };
 using LevelView = LevelViewT<double>;
 using LevelView32 = LevelViewT<float>;
+
+#ifdef __CUDACC__
+template <class T> struct Links {
+    T e, w, n, s;
+};
+__device__ __forceinline__ Links<double> links(const LevelViewT<double>& L, int q) {
+    return {__ldg(L.AE + q), __ldg(L.AW + q), __ldg(L.AN + q), __ldg(L.AS + q)};
+}
+__device__ __forceinline__ Links<float> links(const LevelViewT<float>& L, int q) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(L.L4) + q);
+    return {v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ void set_links(const LevelViewT<double>& L, int q, double e, double w, double n,
+                                          double s) {
+    L.AE[q] = e;
+    L.AW[q] = w;
+    L.AN[q] = n;
+    L.AS[q] = s;
+}
+__device__ __forceinline__ void set_links(const LevelViewT<float>& L, int q, float e, float w, float n, float s) {
+    reinterpret_cast<float4*>(L.L4)[q] = make_float4(e, w, n, s);
+}
+#endif
 
 } // namespace sgpu

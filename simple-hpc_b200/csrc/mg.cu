@@ -23,14 +23,12 @@ template <class T> __global__ void k_mg_build(LevelViewT<T> F, LevelViewT<T> C) 
     if (I >= C.nx || J >= C.ny) return;
     const int fs = F.stride;
     const int f = 2 * I * fs + 2 * J, c = I * C.stride + J;
-    const T ae = F.AE[f + 1] + F.AE[f + fs + 1];
-    const T aw = F.AW[f] + F.AW[f + fs];
-    const T an = F.AN[f] + F.AN[f + 1];
-    const T as = F.AS[f + fs] + F.AS[f + fs + 1];
-    C.AE[c] = ae;
-    C.AW[c] = aw;
-    C.AN[c] = an;
-    C.AS[c] = as;
+    const Links<T> k00 = links(F, f), k01 = links(F, f + 1), k10 = links(F, f + fs), k11 = links(F, f + fs + 1);
+    const T ae = k01.e + k11.e;
+    const T aw = k00.w + k10.w;
+    const T an = k00.n + k01.n;
+    const T as = k10.s + k11.s;
+    set_links(C, c, ae, aw, an, as);
     C.AP[c] = ae + aw + an + as;
 }
 
@@ -40,8 +38,8 @@ template <class T> __global__ void k_mg_smooth(LevelViewT<T> L, int colour) {
     if (I >= L.nx || J >= L.ny || ((I + J) & 1) != colour) return;
     const int s = L.stride, q = I * s + J;
     T* x = L.x;
-    x[q] = rb_value(L.b[q], L.AE[q] * x[q + 1] + L.AW[q] * x[q - 1] + L.AS[q] * x[q + s] + L.AN[q] * x[q - s],
-                    L.AP[q]);
+    const Links<T> k = links(L, q);
+    x[q] = rb_value(L.b[q], k.e * x[q + 1] + k.w * x[q - 1] + k.s * x[q + s] + k.n * x[q - s], L.AP[q]);
 }
 
 template <class T> __global__ void k_mg_residual(LevelViewT<T> L) {
@@ -49,9 +47,8 @@ template <class T> __global__ void k_mg_residual(LevelViewT<T> L) {
     if (I >= L.nx || J >= L.ny) return;
     const int s = L.stride, q = I * s + J;
     const T* x = L.x;
-    L.r[q] = L.b[q] - (L.AP[q] * x[q] -
-                       (L.AE[q] * x[q + 1] + L.AW[q] * x[q - 1] + L.AS[q] * x[q + s] +
-                        L.AN[q] * x[q - s]));
+    const Links<T> k = links(L, q);
+    L.r[q] = L.b[q] - (L.AP[q] * x[q] - (k.e * x[q + 1] + k.w * x[q - 1] + k.s * x[q + s] + k.n * x[q - s]));
 }
 
 template <class T> __global__ void k_mg_restrict(LevelViewT<T> F, LevelViewT<T> C) {
@@ -75,10 +72,11 @@ template <class T> __global__ void k_mg_residual_sq(LevelViewT<T> L, double* cel
     if (I >= L.nx || J >= L.ny) return;
     const int s = L.stride, q = I * s + J;
     const T* x = L.x;
+    const Links<T> k = links(L, q);
     const double r = static_cast<double>(L.b[q]) -
                      (static_cast<double>(L.AP[q]) * x[q] -
-                      (static_cast<double>(L.AE[q]) * x[q + 1] + static_cast<double>(L.AW[q]) * x[q - 1] +
-                       static_cast<double>(L.AS[q]) * x[q + s] + static_cast<double>(L.AN[q]) * x[q - s]));
+                      (static_cast<double>(k.e) * x[q + 1] + static_cast<double>(k.w) * x[q - 1] +
+                       static_cast<double>(k.s) * x[q + s] + static_cast<double>(k.n) * x[q - s]));
     cells[static_cast<std::size_t>(I) * L.ny + J] = r * r;
 }
 
@@ -141,9 +139,8 @@ template <class T> __device__ void cta_smooth_colour(const LevelViewT<T>& L, int
         const int I = k / L.ny, J = k % L.ny;
         if (((I + J) & 1) != colour) continue;
         const int q = I * s + J;
-        x[q] = rb_value(L.b[q],
-                        L.AE[q] * x[q + 1] + L.AW[q] * x[q - 1] + L.AS[q] * x[q + s] + L.AN[q] * x[q - s],
-                        L.AP[q]);
+        const Links<T> k4 = links(L, q);
+        x[q] = rb_value(L.b[q], k4.e * x[q + 1] + k4.w * x[q - 1] + k4.s * x[q + s] + k4.n * x[q - s], L.AP[q]);
     }
     __syncthreads();
 }
@@ -153,8 +150,8 @@ template <class T> __device__ void cta_residual(const LevelViewT<T>& L) {
     const T* x = L.x;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const int I = k / L.ny, J = k % L.ny, q = I * s + J;
-        L.r[q] = L.b[q] - (L.AP[q] * x[q] - (L.AE[q] * x[q + 1] + L.AW[q] * x[q - 1] +
-                                             L.AS[q] * x[q + s] + L.AN[q] * x[q - s]));
+        const Links<T> k4 = links(L, q);
+        L.r[q] = L.b[q] - (L.AP[q] * x[q] - (k4.e * x[q + 1] + k4.w * x[q - 1] + k4.s * x[q + s] + k4.n * x[q - s]));
     }
     __syncthreads();
 }

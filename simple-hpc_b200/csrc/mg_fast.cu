@@ -69,10 +69,11 @@ __device__ __forceinline__ bool in_cone(const Win& w, int I, int Jc, int k, int 
 
 // The 6 per-cell inputs of a red-black update or a residual: AE, AW, AN, AS, AP, b.
 template <class T> __device__ __forceinline__ void load6(const LevelViewT<T>& L, int q, T a[6]) {
-    a[0] = __ldg(L.AE + q);
-    a[1] = __ldg(L.AW + q);
-    a[2] = __ldg(L.AN + q);
-    a[3] = __ldg(L.AS + q);
+    const Links<T> k = links(L, q);
+    a[0] = k.e;
+    a[1] = k.w;
+    a[2] = k.n;
+    a[3] = k.s;
     a[4] = __ldg(L.AP + q);
     a[5] = __ldg(L.b + q);
 }

@@ -245,10 +245,8 @@ __global__ void k_assemble_p_mixed(DevParams p, const double* __restrict__ APU,
     const double anp = (i == H) ? 0.0 : dx * dx / APV[q];
     const double asp = (i == p.NX + H - 1) ? 0.0 : dx * dx / APV[q + ld];
     const int lq = I * L0.stride + J;
-    L0.AE[lq] = static_cast<float>(aep);
-    L0.AW[lq] = static_cast<float>(awp);
-    L0.AN[lq] = static_cast<float>(anp);
-    L0.AS[lq] = static_cast<float>(asp);
+    set_links(L0, lq, static_cast<float>(aep), static_cast<float>(awp), static_cast<float>(anp),
+              static_cast<float>(asp));
     L0.AP[lq] = static_cast<float>(aep + awp + anp + asp);
     const double b = -dx * (-v[q + ld] + v[q]) - dy * (-u[q - 1] + u[q]);
     bfield[q] = b;

@@ -212,8 +212,7 @@ struct Solver {
         mark(vcomp ? SGPU_PH_ASSEMBLE_V : SGPU_PH_ASSEMBLE_U);
         launch_mom_prep(dp, vcomp, x, oth, pf, xF, AP, cells, st);
         mark(vcomp ? SGPU_PH_RESIDUAL_V : SGPU_PH_RESIDUAL_U);
-        if (vcomp) launch_ordered_sum(cells, 0, prm.NY, prm.NX - 1, prm.NY, 1, res, ss, nullptr, st);
-        else launch_ordered_sum(cells, 0, prm.NY - 1, prm.NX, prm.NY - 1, 1, res, ss, nullptr, st);
+        momentum_sum(vcomp, res);
         mark(vcomp ? SGPU_PH_SWEEP_V : SGPU_PH_SWEEP_U);
         const int n = vcomp ? prm.maxit_inner_v : prm.maxit_inner_u;
         double* in = x;
@@ -225,6 +224,13 @@ struct Solver {
         }
         sweep_mark(vcomp, 1, n);
         if (in != x) launch_copy(in, x, g.elems(), st);
+    }
+
+    // res_u / res_v: the ordered sum of |R| over the residual range (on the solver's stream: a
+    // concurrent sum would hold shared memory the sweep's single wave of CTAs needs).
+    void momentum_sum(bool vcomp, double* res) {
+        if (vcomp) launch_ordered_sum(cells, 0, prm.NY, prm.NX - 1, prm.NY, 1, res, ss, nullptr, st);
+        else launch_ordered_sum(cells, 0, prm.NY - 1, prm.NX, prm.NY - 1, 1, res, ss, nullptr, st);
     }
 
     void fast_iteration_enqueue(double* res3) {
@@ -320,8 +326,7 @@ struct Solver {
         mark(vcomp ? SGPU_PH_ASSEMBLE_V : SGPU_PH_ASSEMBLE_U);
         launch_mom_prep_mixed(dp, vcomp, x, oth, pf, AP, cells, rec32, st);
         mark(vcomp ? SGPU_PH_RESIDUAL_V : SGPU_PH_RESIDUAL_U);
-        if (vcomp) launch_ordered_sum(cells, 0, prm.NY, prm.NX - 1, prm.NY, 1, res, ss, nullptr, st);
-        else launch_ordered_sum(cells, 0, prm.NY - 1, prm.NX, prm.NY - 1, 1, res, ss, nullptr, st);
+        momentum_sum(vcomp, res);
         mark(vcomp ? SGPU_PH_SWEEP_V : SGPU_PH_SWEEP_U);
         const int n = vcomp ? prm.maxit_inner_v : prm.maxit_inner_u;
         int cur = 0; // e32[cur] holds the current correction (zero before the first sweep)
@@ -642,16 +647,13 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
             L.stride = L.ny + 2;
             const std::size_t n = static_cast<std::size_t>(L.nx + 2) * L.stride;
             const std::size_t base = static_cast<std::size_t>(L.stride) + 1;
-            float* a[8];
-            for (int k = 0; k < 8; ++k) a[k] = dalloc<float>(n) + base;
-            L.AE = a[0];
-            L.AW = a[1];
-            L.AN = a[2];
-            L.AS = a[3];
-            L.AP = a[4];
-            L.b = a[5];
-            L.x = a[6];
-            L.r = a[7];
+            // links as one 16-byte record per cell (AE..AS stay null), AP, b, x, r as arrays
+            L.L4 = dalloc<Link4>(n) + base;
+            L.AE = L.AW = L.AN = L.AS = nullptr;
+            L.AP = dalloc<float>(n) + base;
+            L.b = dalloc<float>(n) + base;
+            L.x = dalloc<float>(n) + base;
+            L.r = dalloc<float>(n) + base;
             if (l < mg_tail) mg32_x2[l] = dalloc<float>(n) + base;
         }
         mgl32.n = nl;
@@ -679,6 +681,7 @@ Solver::~Solver() {
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : sw_ev)
         if (e) cudaEventDestroy(e);
+
     for (void* q : allocs) cudaFree(q);
     if (host_res) cudaFreeHost(host_res);
     if (st) cudaStreamDestroy(st);

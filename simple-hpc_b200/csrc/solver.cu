@@ -32,6 +32,7 @@ std::atomic<long long> g_launches{0};
 }
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 int fail(int code, const std::string& msg) {
@@ -66,6 +67,11 @@ static void diffusive_host(const sgpu_params_t& p, bool band_or_order2, double o
         out[8] = -nu * (-2.5 * dx / dy - 2.5 * dy / dx);
     }
 }
+
+// One CUDA graph that runs outer iterations of one or more solvers with the stopping test on the
+// device (defined with the batch kernels below); sgpu_run and sgpu_batch_run launch it.
+struct IterGraph;
+void destroy_iter_graph(IterGraph* g);
 
 struct Solver {
     sgpu_params_t prm{};
@@ -107,6 +113,7 @@ struct Solver {
     int seg_rows = 64;
 
     int ncol = 5;
+    IterGraph* run_graph = nullptr; // sgpu_run's graph (built on first use)
 
     // learned warm start (warm_start = cnn, or a network attached through the C ABI)
     std::unique_ptr<UNet> own_net;
@@ -677,6 +684,7 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
 
 Solver::~Solver() {
     if (st) cudaStreamSynchronize(st);
+    destroy_iter_graph(run_graph);
     for (cudaEvent_t e : ev)
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : sw_ev)
@@ -877,7 +885,8 @@ namespace sgpu {
 // ---- batched cavities: device-side stopping test inside one graph launch ----
 
 struct BatchDev {
-    int n, maxit;
+    int n;
+    const int* limit;           // a cavity stops after *limit iterations at most
     double* const* res;         // per cavity: its res_u, res_v, res_p of the current iteration
     const double* tol;          // error_tolerance per cavity
     const int* runmax;          // residual_normalisation = running_max per cavity
@@ -892,20 +901,24 @@ struct BatchDev {
     cudaGraphConditionalHandle hw; // the WHILE node around the batch iteration
 };
 
-// Start of a batch iteration: each cavity's IF node runs iff the cavity is still active.
-__global__ void k_batch_pre(BatchDev b) {
-    for (int c = threadIdx.x; c < b.n; c += blockDim.x) cudaGraphSetConditional(b.h[c], b.active[c] ? 1u : 0u);
+// Start of a batch iteration: each cavity's IF node runs iff the cavity is still active and below
+// the iteration limit of this launch.
+__global__ void k_batch_pre(const BatchDev* bp) {
+    const BatchDev& b = *bp;
+    for (int c = threadIdx.x; c < b.n; c += blockDim.x)
+        cudaGraphSetConditional(b.h[c], b.active[c] && b.iters[c] < *b.limit ? 1u : 0u);
 }
 
 // End of a batch iteration: the stopping rule of run_outer_loop (solver.cpp:117-129) per active
 // cavity, with the same arithmetic as the host loop of sgpu_run; the loop continues while any
 // cavity is active.
-__global__ void k_batch_step(BatchDev b) {
+__global__ void k_batch_step(const BatchDev* bp) {
+    const BatchDev& b = *bp;
     __shared__ int any;
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
     for (int c = threadIdx.x; c < b.n; c += blockDim.x) {
-        if (!b.active[c]) continue;
+        if (!b.active[c] || b.iters[c] >= *b.limit) continue; // its IF branch did not run
         const int it = ++b.iters[c];
         const double ru = b.res[c][0], rv = b.res[c][1], rp = b.res[c][2];
         b.last[3 * c + 0] = ru;
@@ -932,15 +945,188 @@ __global__ void k_batch_step(BatchDev b) {
         if (m < tv) m = tv;
         if (m < tp) m = tp;
         const bool conv = m <= b.tol[c] && it > 1;
-        if (conv || it >= b.maxit) {
+        if (conv) { // finished
             b.active[c] = 0;
-            b.converged[c] = conv ? 1 : 0;
-        } else {
+            b.converged[c] = 1;
+        } else if (it < *b.limit) {
             any = 1;
-        }
+        } // else paused at the limit: a later launch with a higher limit continues it
     }
     __syncthreads();
     if (threadIdx.x == 0) cudaGraphSetConditional(b.hw, any ? 1u : 0u);
+}
+
+__global__ void k_set_ints(int* p, int n, int v) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = v;
+}
+
+// WHILE (any solver active) { pre; per solver IF (active) { one outer iteration }; stopping test }.
+// Each solver's iteration is captured from its own stream into the body of its IF node, so several
+// solvers run as independent branches. The graph is reusable: reset() zeroes the counters and
+// launch(limit) runs until every solver has stopped or reached `limit` iterations in total.
+struct IterGraph {
+    std::vector<Solver*> sv;
+    std::vector<void*> dev;
+    BatchDev bd{};                // host mirror of the control block
+    BatchDev* d_bd = nullptr;     // the kernels read this copy (so the log can grow without a new graph)
+    int* d_limit = nullptr;
+    double* d_log = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int log_cap = 0;
+    long long kernels_per_iteration = 0; // launches one captured outer iteration holds, all solvers
+
+    template <class T> T* alloc(std::size_t n) {
+        void* p = nullptr;
+        SGPU_CUDA(cudaMalloc(&p, sizeof(T) * (n ? n : 1)));
+        SGPU_CUDA(cudaMemset(p, 0, sizeof(T) * (n ? n : 1)));
+        dev.push_back(p);
+        return static_cast<T*>(p);
+    }
+
+    IterGraph(std::vector<Solver*> solvers, int cap) : sv(std::move(solvers)) {
+        const int n = static_cast<int>(sv.size());
+        std::vector<double*> res(n);
+        std::vector<double> tol(n);
+        std::vector<int> runmax(n);
+        for (int c = 0; c < n; ++c) {
+            sv[c]->sync();
+            res[c] = sv[c]->res_dev;
+            tol[c] = sv[c]->prm.error_tolerance;
+            runmax[c] = sv[c]->prm.residual_normalisation == SGPU_NORM_RUNNING_MAX ? 1 : 0;
+        }
+        bd.n = n;
+        double** d_res = alloc<double*>(n);
+        double* d_tol = alloc<double>(n);
+        int* d_runmax = alloc<int>(n);
+        SGPU_CUDA(cudaMemcpy(d_res, res.data(), sizeof(double*) * n, cudaMemcpyHostToDevice));
+        SGPU_CUDA(cudaMemcpy(d_tol, tol.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        SGPU_CUDA(cudaMemcpy(d_runmax, runmax.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+        d_limit = alloc<int>(1);
+        bd.limit = d_limit;
+        bd.res = d_res;
+        bd.tol = d_tol;
+        bd.runmax = d_runmax;
+        bd.maxr = alloc<double>(3 * static_cast<std::size_t>(n));
+        bd.iters = alloc<int>(n);
+        bd.active = alloc<int>(n);
+        bd.converged = alloc<int>(n);
+        bd.last = alloc<double>(3 * static_cast<std::size_t>(n));
+        bd.log = nullptr;
+        bd.log_cap = 0;
+        d_bd = alloc<BatchDev>(1);
+
+        cudaGraph_t g = nullptr;
+        try {
+            SGPU_CUDA(cudaGraphCreate(&g, 0));
+            SGPU_CUDA(cudaGraphConditionalHandleCreate(&bd.hw, g, 1, cudaGraphCondAssignDefault));
+            cudaGraphNodeParams wp{};
+            wp.type = cudaGraphNodeTypeConditional;
+            wp.conditional.handle = bd.hw;
+            wp.conditional.type = cudaGraphCondTypeWhile;
+            wp.conditional.size = 1;
+            cudaGraphNode_t wnode;
+            SGPU_CUDA(cudaGraphAddNode(&wnode, g, nullptr, 0, &wp));
+            cudaGraph_t body = wp.conditional.phGraph_out[0];
+            std::vector<cudaGraphConditionalHandle> hs(n);
+            for (int c = 0; c < n; ++c) SGPU_CUDA(cudaGraphConditionalHandleCreate(&hs[c], body, 0, 0));
+            auto* d_h = alloc<cudaGraphConditionalHandle>(n);
+            SGPU_CUDA(cudaMemcpy(d_h, hs.data(), sizeof(cudaGraphConditionalHandle) * n, cudaMemcpyHostToDevice));
+            bd.h = d_h;
+            SGPU_CUDA(cudaMemcpy(d_bd, &bd, sizeof bd, cudaMemcpyHostToDevice));
+            void* args[] = {&d_bd};
+            cudaKernelNodeParams kp{};
+            kp.func = reinterpret_cast<void*>(&k_batch_pre);
+            kp.gridDim = dim3(1);
+            kp.blockDim = dim3(256);
+            kp.kernelParams = args;
+            cudaGraphNode_t pre;
+            SGPU_CUDA(cudaGraphAddKernelNode(&pre, body, nullptr, 0, &kp));
+            std::vector<cudaGraphNode_t> ifs(n);
+            for (int c = 0; c < n; ++c) {
+                cudaGraphNodeParams ip{};
+                ip.type = cudaGraphNodeTypeConditional;
+                ip.conditional.handle = hs[c];
+                ip.conditional.type = cudaGraphCondTypeIf;
+                ip.conditional.size = 1;
+                SGPU_CUDA(cudaGraphAddNode(&ifs[c], body, &pre, 1, &ip));
+                cudaGraph_t ib = ip.conditional.phGraph_out[0];
+                Solver& s = *sv[c];
+                SGPU_CUDA(cudaStreamBeginCaptureToGraph(s.st, ib, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+                try {
+                    const long long before = g_launches.load();
+                    s.iteration_enqueue(s.res_dev);
+                    const long long captured = g_launches.load() - before;
+                    kernels_per_iteration += captured;
+                    count_launches(-captured); // captured, not run: counted when the graph runs
+                } catch (...) {
+                    cudaGraph_t tmp = nullptr;
+                    cudaStreamEndCapture(s.st, &tmp);
+                    throw;
+                }
+                cudaGraph_t captured = nullptr;
+                SGPU_CUDA(cudaStreamEndCapture(s.st, &captured));
+            }
+            kp.func = reinterpret_cast<void*>(&k_batch_step);
+            cudaGraphNode_t step;
+            SGPU_CUDA(cudaGraphAddKernelNode(&step, body, ifs.data(), ifs.size(), &kp));
+            SGPU_CUDA(cudaGraphInstantiate(&exec, g, 0));
+        } catch (...) {
+            if (g) cudaGraphDestroy(g);
+            release();
+            throw;
+        }
+        cudaGraphDestroy(g);
+        ensure_log(cap);
+    }
+    // Residual log of at least cap rows per solver (rows past a solver's iteration count stay zero).
+    void ensure_log(int cap) {
+        if (cap <= log_cap) return;
+        if (d_log) cudaFree(d_log);
+        d_log = nullptr;
+        const std::size_t n = static_cast<std::size_t>(bd.n) * cap * 4;
+        SGPU_CUDA(cudaMalloc(&d_log, sizeof(double) * n));
+        SGPU_CUDA(cudaMemset(d_log, 0, sizeof(double) * n));
+        log_cap = cap;
+        bd.log = d_log;
+        bd.log_cap = cap;
+        SGPU_CUDA(cudaMemcpy(d_bd, &bd, sizeof bd, cudaMemcpyHostToDevice));
+    }
+    ~IterGraph() { release(); }
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        for (void* p : dev) cudaFree(p);
+        dev.clear();
+        if (d_log) cudaFree(d_log);
+        d_log = nullptr;
+    }
+    void reset(cudaStream_t st) {
+        const int n = bd.n;
+        SGPU_CUDA(cudaMemsetAsync(bd.iters, 0, sizeof(int) * n, st));
+        SGPU_CUDA(cudaMemsetAsync(bd.converged, 0, sizeof(int) * n, st));
+        SGPU_CUDA(cudaMemsetAsync(bd.last, 0, sizeof(double) * 3 * n, st));
+        SGPU_CUDA(cudaMemsetAsync(bd.maxr, 0, sizeof(double) * 3 * n, st));
+        if (bd.log) SGPU_CUDA(cudaMemsetAsync(bd.log, 0, sizeof(double) * 4 * n * static_cast<std::size_t>(log_cap), st));
+        k_set_ints<<<1, 256, 0, st>>>(bd.active, n, 1);
+        SGPU_LAUNCH();
+    }
+    void launch(int limit, cudaStream_t st) {
+        k_set_ints<<<1, 32, 0, st>>>(d_limit, 1, limit);
+        SGPU_LAUNCH();
+        SGPU_CUDA(cudaGraphLaunch(exec, st));
+    }
+    // Kernel launches the graph performed for `rounds` WHILE iterations that ran `iterations` solver
+    // iterations in total: the captured kernels of each solver iteration, and 2 per round.
+    void count(long long rounds, long long iterations) const {
+        const long long per = sv.empty() ? 0 : kernels_per_iteration / static_cast<long long>(sv.size());
+        count_launches(2 * rounds + iterations * per);
+    }
+};
+
+void destroy_iter_graph(IterGraph* g) {
+    if (!g) return;
+    cudaDeviceSynchronize();
+    delete g;
 }
 
 } // namespace sgpu
@@ -951,26 +1137,15 @@ struct sgpu_handle {
 struct sgpu_batch {
     std::vector<std::unique_ptr<sgpu::Solver>> s;
     cudaStream_t st = nullptr;
-    std::vector<void*> dev; // device allocations of the batch state
-    double* d_last = nullptr;
-    double* d_log = nullptr;
-    int* d_iters = nullptr;
-    int* d_conv = nullptr;
-    int log_cap = 0;
-    int ran = 0; // 1 after sgpu_batch_run
-    std::vector<int> seg_tuned; // autotuned row segment per cavity (0: heuristic)
+    std::unique_ptr<sgpu::IterGraph> g; // the graph of the last run (its counters are the results)
+    int ran = 0;                        // 1 after sgpu_batch_run
+    int last_log_cap = 0;               // log_cap of the last run
+    std::vector<int> seg_tuned;         // autotuned row segment per cavity (0: heuristic)
     ~sgpu_batch() {
         if (st) cudaStreamSynchronize(st);
+        g.reset();
         s.clear();
-        for (void* p : dev) cudaFree(p);
         if (st) cudaStreamDestroy(st);
-    }
-    template <class T> T* alloc(std::size_t n) {
-        void* p = nullptr;
-        SGPU_CUDA(cudaMalloc(&p, sizeof(T) * (n ? n : 1)));
-        SGPU_CUDA(cudaMemset(p, 0, sizeof(T) * (n ? n : 1)));
-        dev.push_back(p);
-        return static_cast<T*>(p);
     }
 };
 struct sgpu_cnn {
@@ -1102,12 +1277,63 @@ int sgpu_outer_iteration(sgpu_handle* h, double res[3], double* phase_seconds) {
     });
 }
 
+// sgpu_run without per-iteration host round trips: the iterations run inside one graph launch per
+// print interval (sgpu::IterGraph), the stopping rule and the residual log on the device. Used when
+// every outer iteration is a fixed sequence of launches (no CG, no tolerance-driven multigrid, no
+// warm start) and the per-phase timers are off.
+static bool run_graphed(sgpu::Solver& s, int maxit, double* log, int print_every, sgpu_result_t& out) {
+    if (s.profiling || maxit < 1 || s.prm.pressure_solver == SGPU_P_CG || s.prm.mg_mode == SGPU_MG_TOLERANCE ||
+        s.net)
+        return false;
+    if (!s.run_graph) s.run_graph = new sgpu::IterGraph({&s}, maxit);
+    sgpu::IterGraph& g = *s.run_graph;
+    g.ensure_log(maxit);
+    g.reset(s.st);
+    const int chunk = print_every > 0 ? print_every : maxit;
+    int done = 0, conv = 0;
+    std::vector<double> rows;
+    while (done < maxit) {
+        const int lim = std::min(maxit, done + chunk);
+        g.launch(lim, s.st);
+        int it = 0;
+        SGPU_CUDA(cudaMemcpyAsync(&it, g.bd.iters, sizeof(int), cudaMemcpyDeviceToHost, s.st));
+        SGPU_CUDA(cudaMemcpyAsync(&conv, g.bd.converged, sizeof(int), cudaMemcpyDeviceToHost, s.st));
+        s.sync();
+        if (print_every > 0 && it > done) {
+            rows.resize(4 * static_cast<std::size_t>(it - done));
+            SGPU_CUDA(cudaMemcpy(rows.data(), g.bd.log + 4 * static_cast<std::size_t>(done),
+                                 sizeof(double) * rows.size(), cudaMemcpyDeviceToHost));
+            for (int k = done + 1; k <= it; ++k)
+                if (k == 1 || k % print_every == 0) {
+                    const double* r = rows.data() + 4 * static_cast<std::size_t>(k - 1 - done);
+                    std::printf("iter %d  res_u %.6e  res_v %.6e  res_p %.6e\n", k, r[1], r[2], r[3]);
+                }
+        }
+        const bool stopped = conv || it < lim;
+        done = it;
+        if (stopped) break;
+    }
+    if (log && done > 0)
+        SGPU_CUDA(cudaMemcpy(log, g.bd.log, sizeof(double) * 4 * static_cast<std::size_t>(done),
+                             cudaMemcpyDeviceToHost));
+    g.count(done, done);
+    out.iterations = done;
+    out.converged = conv;
+    if (s.prm.pressure_solver == SGPU_P_MG) out.mg_vcycles = done * s.prm.mg_cycles;
+    return true;
+}
+
 int sgpu_run(sgpu_handle* h, int maxit, double* log, int print_every, sgpu_result_t* result) {
     SGPU_NEED_HANDLE(h);
     return guarded([&] {
         sgpu::Solver& s = *h->s;
         sgpu_result_t out{};
         const auto t0 = std::chrono::steady_clock::now();
+        if (run_graphed(s, maxit, log, print_every, out)) {
+            out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            if (result) *result = out;
+            return;
+        }
         double mu = 0.0, mv = 0.0, mp = 0.0;
         for (int iter = 1; iter <= maxit; ++iter) {
             s.iteration_enqueue(s.res_dev);
@@ -1520,6 +1746,7 @@ int sgpu_batch_count(sgpu_batch* b, int* count) {
 int sgpu_batch_autotune(sgpu_batch* b, int* chosen) {
     SGPU_NEED_BATCH(b);
     return guarded([&] {
+        b->g.reset(); // captured launches carry the old segment heights
         std::map<std::tuple<int, int, int, int>, int> best;
         for (std::size_t c = 0; c < b->s.size(); ++c) {
             sgpu::Solver& sv = *b->s[c];
@@ -1572,131 +1799,41 @@ int sgpu_batch_run(sgpu_batch* b, int maxit, int log_cap, double* seconds) {
     SGPU_NEED_BATCH(b);
     if (maxit < 0 || log_cap < 0) return sgpu::fail(SGPU_E_INVALID, "sgpu_batch_run: bad arguments");
     return guarded([&] {
-        const int n = static_cast<int>(b->s.size());
-        if (!b->d_iters) {
-            b->d_iters = b->alloc<int>(n);
-            b->d_conv = b->alloc<int>(n);
-            b->d_last = b->alloc<double>(3 * static_cast<std::size_t>(n));
-        }
-        if (log_cap != b->log_cap) {
-            b->d_log = log_cap ? b->alloc<double>(static_cast<std::size_t>(n) * log_cap * 4) : nullptr;
-            b->log_cap = log_cap;
-        }
-        for (auto& sv : b->s) sv->sync();
-        SGPU_CUDA(cudaMemsetAsync(b->d_iters, 0, sizeof(int) * n, b->st));
-        SGPU_CUDA(cudaMemsetAsync(b->d_conv, 0, sizeof(int) * n, b->st));
-        SGPU_CUDA(cudaMemsetAsync(b->d_last, 0, sizeof(double) * 3 * n, b->st));
+        std::vector<sgpu::Solver*> sv;
+        for (auto& p : b->s) sv.push_back(p.get());
+        if (!b->g) b->g = std::make_unique<sgpu::IterGraph>(sv, log_cap);
+        b->g->ensure_log(log_cap);
+        b->g->reset(b->st);
         b->ran = 1;
+        b->last_log_cap = log_cap;
         if (maxit == 0) {
             if (seconds) *seconds = 0.0;
             SGPU_CUDA(cudaStreamSynchronize(b->st));
             return;
         }
-        std::vector<double*> res(n);
-        std::vector<double> tol(n);
-        std::vector<int> runmax(n), ones(n, 1);
-        for (int c = 0; c < n; ++c) {
-            res[c] = b->s[c]->res_dev;
-            tol[c] = b->s[c]->prm.error_tolerance;
-            runmax[c] = b->s[c]->prm.residual_normalisation == SGPU_NORM_RUNNING_MAX ? 1 : 0;
-        }
-        // per-run state (freed with the batch)
-        sgpu::BatchDev bd{};
-        bd.n = n;
-        bd.maxit = maxit;
-        double** d_res = b->alloc<double*>(n);
-        double* d_tol = b->alloc<double>(n);
-        int* d_runmax = b->alloc<int>(n);
-        int* d_active = b->alloc<int>(n);
-        SGPU_CUDA(cudaMemcpyAsync(d_res, res.data(), sizeof(double*) * n, cudaMemcpyHostToDevice, b->st));
-        SGPU_CUDA(cudaMemcpyAsync(d_tol, tol.data(), sizeof(double) * n, cudaMemcpyHostToDevice, b->st));
-        SGPU_CUDA(cudaMemcpyAsync(d_runmax, runmax.data(), sizeof(int) * n, cudaMemcpyHostToDevice, b->st));
-        SGPU_CUDA(cudaMemcpyAsync(d_active, ones.data(), sizeof(int) * n, cudaMemcpyHostToDevice, b->st));
-        bd.res = d_res;
-        bd.tol = d_tol;
-        bd.runmax = d_runmax;
-        bd.maxr = b->alloc<double>(3 * static_cast<std::size_t>(n));
-        bd.iters = b->d_iters;
-        bd.active = d_active;
-        bd.converged = b->d_conv;
-        bd.last = b->d_last;
-        bd.log = b->d_log;
-        bd.log_cap = b->log_cap;
-
-        cudaGraph_t g = nullptr;
-        cudaGraphExec_t exec = nullptr;
-        auto cleanup = [&] {
-            if (exec) cudaGraphExecDestroy(exec);
-            if (g) cudaGraphDestroy(g);
-        };
-        try {
-            SGPU_CUDA(cudaGraphCreate(&g, 0));
-            SGPU_CUDA(cudaGraphConditionalHandleCreate(&bd.hw, g, 1, cudaGraphCondAssignDefault));
-            cudaGraphNodeParams wp{};
-            wp.type = cudaGraphNodeTypeConditional;
-            wp.conditional.handle = bd.hw;
-            wp.conditional.type = cudaGraphCondTypeWhile;
-            wp.conditional.size = 1;
-            cudaGraphNode_t wnode;
-            SGPU_CUDA(cudaGraphAddNode(&wnode, g, nullptr, 0, &wp));
-            cudaGraph_t body = wp.conditional.phGraph_out[0];
-            std::vector<cudaGraphConditionalHandle> hs(n);
-            for (int c = 0; c < n; ++c) SGPU_CUDA(cudaGraphConditionalHandleCreate(&hs[c], body, 0, 0));
-            auto* d_h = b->alloc<cudaGraphConditionalHandle>(n);
-            SGPU_CUDA(cudaMemcpyAsync(d_h, hs.data(), sizeof(cudaGraphConditionalHandle) * n,
-                                      cudaMemcpyHostToDevice, b->st));
-            bd.h = d_h;
-            void* args[] = {&bd};
-            cudaKernelNodeParams kp{};
-            kp.func = reinterpret_cast<void*>(&sgpu::k_batch_pre);
-            kp.gridDim = dim3(1);
-            kp.blockDim = dim3(256);
-            kp.kernelParams = args;
-            cudaGraphNode_t pre;
-            SGPU_CUDA(cudaGraphAddKernelNode(&pre, body, nullptr, 0, &kp));
-            std::vector<cudaGraphNode_t> ifs(n);
-            for (int c = 0; c < n; ++c) {
-                cudaGraphNodeParams ip{};
-                ip.type = cudaGraphNodeTypeConditional;
-                ip.conditional.handle = hs[c];
-                ip.conditional.type = cudaGraphCondTypeIf;
-                ip.conditional.size = 1;
-                SGPU_CUDA(cudaGraphAddNode(&ifs[c], body, &pre, 1, &ip));
-                cudaGraph_t ib = ip.conditional.phGraph_out[0];
-                sgpu::Solver& sv = *b->s[c];
-                SGPU_CUDA(cudaStreamBeginCaptureToGraph(sv.st, ib, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-                try {
-                    sv.iteration_enqueue(sv.res_dev);
-                } catch (...) {
-                    cudaGraph_t tmp = nullptr;
-                    cudaStreamEndCapture(sv.st, &tmp);
-                    throw;
-                }
-                cudaGraph_t captured = nullptr;
-                SGPU_CUDA(cudaStreamEndCapture(sv.st, &captured));
+        cudaEvent_t e0, e1;
+        SGPU_CUDA(cudaEventCreate(&e0));
+        SGPU_CUDA(cudaEventCreate(&e1));
+        SGPU_CUDA(cudaEventRecord(e0, b->st));
+        b->g->launch(maxit, b->st);
+        SGPU_CUDA(cudaEventRecord(e1, b->st));
+        SGPU_CUDA(cudaEventSynchronize(e1));
+        {
+            const int n = static_cast<int>(b->s.size());
+            std::vector<int> its(n);
+            SGPU_CUDA(cudaMemcpy(its.data(), b->g->bd.iters, sizeof(int) * n, cudaMemcpyDeviceToHost));
+            long long total = 0, rounds = 0;
+            for (int v : its) {
+                total += v;
+                rounds = std::max<long long>(rounds, v);
             }
-            kp.func = reinterpret_cast<void*>(&sgpu::k_batch_step);
-            cudaGraphNode_t step;
-            SGPU_CUDA(cudaGraphAddKernelNode(&step, body, ifs.data(), ifs.size(), &kp));
-            SGPU_CUDA(cudaGraphInstantiate(&exec, g, 0));
-            cudaEvent_t e0, e1;
-            SGPU_CUDA(cudaEventCreate(&e0));
-            SGPU_CUDA(cudaEventCreate(&e1));
-            SGPU_CUDA(cudaEventRecord(e0, b->st));
-            SGPU_CUDA(cudaGraphLaunch(exec, b->st));
-            SGPU_CUDA(cudaEventRecord(e1, b->st));
-            SGPU_CUDA(cudaEventSynchronize(e1));
-            float ms = 0.0f;
-            SGPU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            if (seconds) *seconds = ms * 1e-3;
-            sgpu::count_launch(); // the batch graph: one launch from the host
-        } catch (...) {
-            cleanup();
-            throw;
+            b->g->count(rounds, total); // cavities differ in kernels per iteration: an average
         }
-        cleanup();
+        float ms = 0.0f;
+        SGPU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (seconds) *seconds = ms * 1e-3;
     });
 }
 
@@ -1705,22 +1842,29 @@ int sgpu_batch_results(sgpu_batch* b, int* iterations, int* converged, double* r
     if (!b->ran) return sgpu::fail(SGPU_E_INVALID, "sgpu_batch_results: the batch has not run");
     return guarded([&] {
         const int n = static_cast<int>(b->s.size());
+        const sgpu::BatchDev& bd = b->g->bd;
         if (iterations)
-            SGPU_CUDA(cudaMemcpyAsync(iterations, b->d_iters, sizeof(int) * n, cudaMemcpyDeviceToHost, b->st));
+            SGPU_CUDA(cudaMemcpyAsync(iterations, bd.iters, sizeof(int) * n, cudaMemcpyDeviceToHost, b->st));
         if (converged)
-            SGPU_CUDA(cudaMemcpyAsync(converged, b->d_conv, sizeof(int) * n, cudaMemcpyDeviceToHost, b->st));
+            SGPU_CUDA(cudaMemcpyAsync(converged, bd.converged, sizeof(int) * n, cudaMemcpyDeviceToHost, b->st));
         if (residuals)
-            SGPU_CUDA(cudaMemcpyAsync(residuals, b->d_last, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, b->st));
+            SGPU_CUDA(cudaMemcpyAsync(residuals, bd.last, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, b->st));
         SGPU_CUDA(cudaStreamSynchronize(b->st));
     });
 }
 
 int sgpu_batch_log(sgpu_batch* b, double* host) {
     SGPU_NEED_BATCH(b);
-    if (!host || !b->d_log) return sgpu::fail(SGPU_E_INVALID, "sgpu_batch_log: no log (run with log_cap > 0)");
+    if (!host || !b->g || !b->g->bd.log)
+        return sgpu::fail(SGPU_E_INVALID, "sgpu_batch_log: no log (run with log_cap > 0)");
     return guarded([&] {
-        const std::size_t n = b->s.size() * static_cast<std::size_t>(b->log_cap) * 4;
-        SGPU_CUDA(cudaMemcpyAsync(host, b->d_log, sizeof(double) * n, cudaMemcpyDeviceToHost, b->st));
+        // rows of the requested log_cap of the last run (the buffer may be longer)
+        const int cap = b->g->log_cap;
+        for (std::size_t c = 0; c < b->s.size(); ++c)
+            SGPU_CUDA(cudaMemcpyAsync(host + c * static_cast<std::size_t>(b->last_log_cap) * 4,
+                                      b->g->bd.log + c * static_cast<std::size_t>(cap) * 4,
+                                      sizeof(double) * 4 * static_cast<std::size_t>(b->last_log_cap),
+                                      cudaMemcpyDeviceToHost, b->st));
         SGPU_CUDA(cudaStreamSynchronize(b->st));
     });
 }

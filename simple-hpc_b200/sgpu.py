@@ -421,8 +421,12 @@ class Solver:
         _check(lib().sgpu_run(self._h, maxit, _dptr(log), print_every, C.byref(res)))
         return res, log[: res.iterations].copy()
 
-    def download(self, field_id: int) -> np.ndarray:
-        out = np.empty(self.shape)
+    def download(self, field_id: int, out: np.ndarray | None = None) -> np.ndarray:
+        """The field as an (nrows, ncols) array; into `out` (e.g. pinned host memory) if given."""
+        if out is None:
+            out = np.empty(self.shape)
+        elif out.shape != self.shape or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous float64 array of shape {self.shape}")
         _check(lib().sgpu_download(self._h, field_id, _dptr(out)))
         return out
 

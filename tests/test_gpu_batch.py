@@ -120,3 +120,27 @@ def test_batch_rejects_unsupported(sgpu_mod):
         p = sgpu_mod.params_from_config(config_text(cavity(16, 100, **bad)))
         with pytest.raises(sgpu_mod.SgpuError, match="batch"):
             sgpu_mod.Batch([p])
+
+
+@pytest.mark.parametrize("extra", [{}, {"precision": "mixed"}, {"pressure_solver": "gs_redblack"}])
+def test_run_graph_equals_host_loop(sgpu_mod, extra, capfd):
+    """sgpu_run replays one captured outer iteration inside a WHILE graph with the stopping test on
+    the device; with the per-phase timers on it issues every launch from the host. Both must give
+    the same iterations, residual log and fields, bit for bit, also across print_every chunks."""
+    cfg = cavity(32, 100, **extra)
+    out = []
+    for profiling in (True, False):
+        p = sgpu_mod.params_from_config(config_text(cfg))
+        with sgpu_mod.Solver(p) as s:
+            s.set_profiling(profiling)
+            res, log = s.run(4000, print_every=100)
+            out.append((res.iterations, res.converged, log, [s.download(f) for f in (0, 1, 2)]))
+    printed = capfd.readouterr().out.splitlines()
+    (i0, c0, l0, f0), (i1, c1, l1, f1) = out
+    assert i0 == i1 and c0 == c1 and c0
+    assert np.array_equal(l0, l1)
+    for a, b in zip(f0, f1):
+        assert bit_equal(a, b)
+    # the same progress lines from both paths
+    half = len(printed) // 2
+    assert printed[:half] == printed[half:] and printed[0].startswith("iter 1 ")

@@ -43,6 +43,9 @@ SOURCES = {
     "io.cpp": EXACT,
     "noalloc.cu": EXACT,
     "cnn.cu": FAST,
+    "mg32.cu": FAST,
+    "mg_fast32.cu": FAST,
+    "mixed32.cu": FAST,
 }
 DRIVER = ["driver.cpp"]
 

@@ -283,15 +283,12 @@ template <class T> void launch_mg_b_sq(const LevelViewT<T>& L, double* cells, cu
     k_mg_b_sq<T><<<grid2(L.nx, L.ny), dim3(BX, BY), 0, st>>>(L, cells);
     SGPU_LAUNCH();
 }
-template void launch_mg_residual_sq<double>(const LevelViewT<double>&, double*, cudaStream_t);
-template void launch_mg_residual_sq<float>(const LevelViewT<float>&, double*, cudaStream_t);
-template void launch_mg_b_sq<double>(const LevelViewT<double>&, double*, cudaStream_t);
-template void launch_mg_b_sq<float>(const LevelViewT<float>&, double*, cudaStream_t);
-
+#ifndef SGPU_FLOAT_UNIT
 void launch_mg_sub_mean(const LevelView& L, double* x, const double* sum, cudaStream_t st) {
     k_mg_sub_mean<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, st>>>(L, x, sum);
     SGPU_LAUNCH();
 }
+#endif
 
 #define SGPU_MG_INST(T)                                                                            \
     template void launch_mg_tail<T>(const MgLevelsT<T>&, int, int, int, double, double, double*,   \
@@ -302,9 +299,16 @@ void launch_mg_sub_mean(const LevelView& L, double* x, const double* sum, cudaSt
     template void launch_mg_restrict<T>(const LevelViewT<T>&, const LevelViewT<T>&, cudaStream_t); \
     template void launch_mg_prolong<T>(const LevelViewT<T>&, const LevelViewT<T>&, double,         \
                                        cudaStream_t);                                              \
-    template void launch_mg_coarse<T>(const LevelViewT<T>&, double*, double, int*, cudaStream_t);
+    template void launch_mg_coarse<T>(const LevelViewT<T>&, double*, double, int*, cudaStream_t);  \
+    template void launch_mg_residual_sq<T>(const LevelViewT<T>&, double*, cudaStream_t);           \
+    template void launch_mg_b_sq<T>(const LevelViewT<T>&, double*, cudaStream_t);
+// This file alone instantiates the double kernels (built without contraction: the reference's
+// bits); mg32.cu includes it with SGPU_FLOAT_UNIT for the float ones (contraction allowed).
+#ifndef SGPU_FLOAT_UNIT
 SGPU_MG_INST(double)
+#else
 SGPU_MG_INST(float)
+#endif
 #undef SGPU_MG_INST
 
 } // namespace sgpu

@@ -320,7 +320,9 @@ void up_t(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, T* xout,
 
 } // namespace
 
+#ifndef SGPU_FLOAT_UNIT
 bool mg_fast_supported(int pre, int post) { return pre >= 1 && pre <= 4 && post >= 0 && post <= 4; }
+#endif
 
 template <class T>
 void launch_mg_down(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, int pre, bool x_zero,
@@ -347,13 +349,18 @@ void launch_mg_up(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, 
     }
 }
 
+// This file alone instantiates the double kernels (built without contraction: the reference's
+// bits); mg_fast32.cu includes it with SGPU_FLOAT_UNIT for the float ones (contraction allowed).
+#ifndef SGPU_FLOAT_UNIT
 template void launch_mg_down<double>(const LevelViewT<double>&, const LevelViewT<double>&, double*,
                                      int, bool, int, cudaStream_t);
-template void launch_mg_down<float>(const LevelViewT<float>&, const LevelViewT<float>&, float*, int,
-                                    bool, int, cudaStream_t);
 template void launch_mg_up<double>(const LevelViewT<double>&, const LevelViewT<double>&,
                                    const double*, double*, double, int, int, cudaStream_t);
+#else
+template void launch_mg_down<float>(const LevelViewT<float>&, const LevelViewT<float>&, float*, int,
+                                    bool, int, cudaStream_t);
 template void launch_mg_up<float>(const LevelViewT<float>&, const LevelViewT<float>&, const float*,
                                   float*, double, int, int, cudaStream_t);
+#endif
 
 } // namespace sgpu

@@ -308,6 +308,9 @@ Range update_range(const DevParams& p, bool v) {
 
 } // namespace
 
+// This file alone defines the FP64 launchers (built without contraction); mixed32.cu includes it
+// with SGPU_FLOAT_UNIT for the FP32 correction sweep (contraction allowed).
+#ifndef SGPU_FLOAT_UNIT
 void launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x, const double* oth,
                            const double* pf, double* AP, double* cells, float4* rec,
                            cudaStream_t st) {
@@ -317,17 +320,6 @@ void launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x
     if (v_component) k_mom_prep_mixed<true><<<grid, dim3(32, 8), 0, st>>>(p, x, oth, pf, AP, cells, rec, ur);
     else k_mom_prep_mixed<false><<<grid, dim3(32, 8), 0, st>>>(p, x, oth, pf, AP, cells, rec, ur);
     SGPU_LAUNCH();
-}
-
-void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, float* eout,
-                       const float4* rec, bool e_zero, int seg_rows, cudaStream_t st) {
-    if (p.ncol == 5) {
-        if (v_component) launch_corr<5, true, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
-        else launch_corr<5, false, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
-    } else {
-        if (v_component) launch_corr<2, true, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
-        else launch_corr<2, false, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
-    }
 }
 
 void launch_add_correction(const DevParams& p, bool v_component, double* x, const float* e,
@@ -362,6 +354,18 @@ void launch_correct_mixed(const DevParams& p, const LevelView32& L0, const doubl
     SGPU_LAUNCH();
 }
 
+#else
+void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, float* eout,
+                       const float4* rec, bool e_zero, int seg_rows, cudaStream_t st) {
+    if (p.ncol == 5) {
+        if (v_component) launch_corr<5, true, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
+        else launch_corr<5, false, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
+    } else {
+        if (v_component) launch_corr<2, true, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
+        else launch_corr<2, false, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
+    }
+}
+
 void init_mixed_kernels() {
     const int smem = kRing * 256 * static_cast<int>(sizeof(float));
     SGPU_CUDA(cudaFuncSetAttribute(k_corr_stream<5, false, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -379,5 +383,7 @@ int corr_blocks_per_sm(int ncol) {
         SGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_corr_stream<2, false, 256>, 256, smem));
     return n > 0 ? n : 1;
 }
+
+#endif
 
 } // namespace sgpu

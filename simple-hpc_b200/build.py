@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import concurrent.futures as cf
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -69,6 +70,8 @@ def git_hash() -> str:
 def _compile(src: Path, flags: list[str], verbose: bool) -> Path:
     obj = OBJ / (src.name + ".o")
     deps = [src] + sorted(CSRC.glob("*.hpp")) + sorted(CSRC.glob("*.cuh")) + [INCLUDE / "sgpu.h"]
+    # sources that #include another .cu (the FP32 units) depend on it too
+    deps += [CSRC / m for m in re.findall(r'#include "([\w.]+\.cu)"', src.read_text())]
     if obj.exists() and all(obj.stat().st_mtime >= d.stat().st_mtime for d in deps if d.exists()):
         return obj
     lang = ["-x", "cu"] if src.suffix == ".cu" else ["-x", "c++"]

@@ -15,6 +15,8 @@
 // below a size threshold and the coarsest solve run in one CTA (k_mg_tail in mg.cu).
 #include "kernels.hpp"
 
+#include <cstdlib>
+
 namespace sgpu {
 
 namespace {
@@ -99,8 +101,8 @@ template <int NC, class T> struct StepRegs {
 };
 
 // PRE red-black sweeps, residual and restriction in one streaming pass (see the file comment).
-template <int NT, int PRE, int PD, class T>
-__global__ void __launch_bounds__(NT, 2)
+template <int NT, int PRE, int PD, int MINB, class T>
+__global__ void __launch_bounds__(NT, MINB)
     k_mg_down(LevelViewT<T> L, LevelViewT<T> C, T* __restrict__ xout, int x_zero, int seg_rows,
               int HC) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -191,8 +193,8 @@ __global__ void __launch_bounds__(NT, 2)
 }
 
 // Prolongation and POST red-black sweeps in one streaming pass (see the file comment).
-template <int NT, int POST, int PD, class T>
-__global__ void __launch_bounds__(NT, 2)
+template <int NT, int POST, int PD, int MINB, class T>
+__global__ void __launch_bounds__(NT, MINB)
     k_mg_up(LevelViewT<T> C, LevelViewT<T> L, const T* __restrict__ xin, T* __restrict__ xout,
             double omega, int seg_rows, int HC) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -267,13 +269,12 @@ __global__ void __launch_bounds__(NT, 2)
 }
 
 constexpr int kNT = 256;
-// Register sets in the coefficient pipeline (steps of prefetch): FP32 cells are half the registers.
-template <class T> constexpr int kStepPrefetch = sizeof(T) == 4 ? 3 : 2;
 
-int seg_for(int nx, int ny, int HC, int sms) {
+// Rows per CTA segment: one wave of the kernel's resident CTAs (blocks_per_sm per SM).
+int seg_for(int nx, int ny, int HC, int sms, int blocks_per_sm) {
     const int W = kNT - 2 * HC;
     const int strips = (ny + W - 1) / W;
-    const int want = (2 * sms) / strips > 0 ? (2 * sms) / strips : 1; // one wave, 2 CTAs per SM
+    const int want = (blocks_per_sm * sms) / strips > 0 ? (blocks_per_sm * sms) / strips : 1;
     int seg = (nx + want - 1) / want;
     seg = (seg + 1) & ~1; // even: restriction pairs stay inside one CTA
     const int min_seg = 2 * HC + 8;
@@ -281,41 +282,102 @@ int seg_for(int nx, int ny, int HC, int sms) {
     return seg;
 }
 
-template <class K> void allow_smem(K kernel, int bytes, bool& done) {
+template <class K> int prepare_kernel(K kernel, int smem, bool& done, int& blocks) {
     if (!done) {
-        SGPU_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        SGPU_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        SGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kNT, smem));
+        if (blocks < 1) blocks = 1;
         done = true;
     }
+    return blocks;
+}
+
+// Register budget of the level kernels: PD register sets in the coefficient pipeline against
+// MINB resident CTAs per SM. The kernels are latency-bound, so resident warps count for more than
+// prefetch depth. Measured at 4096^2: float (1, 4) beats (2, 3) and (3, 2). SGPU_MG_VARIANT and
+// SGPU_MG_VARIANT64 select other budgets for the float and double kernels (tuning switches: the
+// arithmetic is the same).
+int env_variant(const char* name, int dflt) {
+    const char* e = std::getenv(name);
+    return e ? std::atoi(e) : dflt;
+}
+int mg_variant() {
+    static const int v = env_variant("SGPU_MG_VARIANT", 2);
+    return v;
+}
+int mg_variant64() {
+    static const int v = env_variant("SGPU_MG_VARIANT64", 0);
+    return v;
+}
+
+template <int PRE, int PD, int MINB, class T>
+void down_v(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, bool x_zero, int sms,
+            cudaStream_t st) {
+    const int HC = 2 * PRE + 2;
+    constexpr int smem = kRing * kNT * static_cast<int>(sizeof(T));
+    static bool done = false;
+    static int blocks = 0;
+    auto kernel = k_mg_down<kNT, PRE, PD, MINB, T>;
+    const int seg = seg_for(F.nx, F.ny, HC, sms, prepare_kernel(kernel, smem, done, blocks));
+    const int W = kNT - 2 * HC;
+    const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
+    kernel<<<grid, kNT, smem, st>>>(F, C, xout, x_zero ? 1 : 0, seg, HC);
+    SGPU_LAUNCH();
+}
+
+template <int POST, int PD, int MINB, class T>
+void up_v(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, T* xout, double omega,
+          int sms, cudaStream_t st) {
+    const int HC = 2 * POST + 2;
+    constexpr int smem = kRing * kNT * static_cast<int>(sizeof(T));
+    static bool done = false;
+    static int blocks = 0;
+    auto kernel = k_mg_up<kNT, POST, PD, MINB, T>;
+    const int seg = seg_for(F.nx, F.ny, HC, sms, prepare_kernel(kernel, smem, done, blocks));
+    const int W = kNT - 2 * HC;
+    const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
+    kernel<<<grid, kNT, smem, st>>>(C, F, xin, xout, omega, seg, HC);
+    SGPU_LAUNCH();
 }
 
 template <int PRE, class T>
 void down_t(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, bool x_zero, int sms,
             cudaStream_t st) {
-    const int HC = 2 * PRE + 2;
-    const int seg = seg_for(F.nx, F.ny, HC, sms);
-    const int W = kNT - 2 * HC;
-    const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
-    constexpr int smem = kRing * kNT * static_cast<int>(sizeof(T));
-    static bool attr = false;
-    constexpr int PD = kStepPrefetch<T>;
-    allow_smem(k_mg_down<kNT, PRE, PD, T>, smem, attr);
-    k_mg_down<kNT, PRE, PD, T><<<grid, kNT, smem, st>>>(F, C, xout, x_zero ? 1 : 0, seg, HC);
-    SGPU_LAUNCH();
+    if constexpr (sizeof(T) == 8) {
+        switch (mg_variant64()) {
+        case 1: down_v<PRE, 1, 3>(F, C, xout, x_zero, sms, st); break;
+        case 2: down_v<PRE, 1, 4>(F, C, xout, x_zero, sms, st); break;
+        default: down_v<PRE, 2, 2>(F, C, xout, x_zero, sms, st); break;
+        }
+    } else {
+        switch (mg_variant()) {
+        case 0: down_v<PRE, 3, 2>(F, C, xout, x_zero, sms, st); break;
+        case 1: down_v<PRE, 2, 3>(F, C, xout, x_zero, sms, st); break;
+        case 3: down_v<PRE, 1, 5>(F, C, xout, x_zero, sms, st); break;
+        case 4: down_v<PRE, 1, 6>(F, C, xout, x_zero, sms, st); break;
+        default: down_v<PRE, 1, 4>(F, C, xout, x_zero, sms, st); break;
+        }
+    }
 }
 
 template <int POST, class T>
 void up_t(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, T* xout, double omega,
           int sms, cudaStream_t st) {
-    const int HC = 2 * POST + 2;
-    const int seg = seg_for(F.nx, F.ny, HC, sms);
-    const int W = kNT - 2 * HC;
-    const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
-    constexpr int smem = kRing * kNT * static_cast<int>(sizeof(T));
-    static bool attr = false;
-    constexpr int PD = kStepPrefetch<T>;
-    allow_smem(k_mg_up<kNT, POST, PD, T>, smem, attr);
-    k_mg_up<kNT, POST, PD, T><<<grid, kNT, smem, st>>>(C, F, xin, xout, omega, seg, HC);
-    SGPU_LAUNCH();
+    if constexpr (sizeof(T) == 8) {
+        switch (mg_variant64()) {
+        case 1: up_v<POST, 1, 3>(C, F, xin, xout, omega, sms, st); break;
+        case 2: up_v<POST, 1, 4>(C, F, xin, xout, omega, sms, st); break;
+        default: up_v<POST, 2, 2>(C, F, xin, xout, omega, sms, st); break;
+        }
+    } else {
+        switch (mg_variant()) {
+        case 0: up_v<POST, 3, 2>(C, F, xin, xout, omega, sms, st); break;
+        case 1: up_v<POST, 2, 3>(C, F, xin, xout, omega, sms, st); break;
+        case 3: up_v<POST, 1, 5>(C, F, xin, xout, omega, sms, st); break;
+        case 4: up_v<POST, 1, 6>(C, F, xin, xout, omega, sms, st); break;
+        default: up_v<POST, 1, 4>(C, F, xin, xout, omega, sms, st); break;
+        }
+    }
 }
 
 } // namespace

@@ -19,6 +19,8 @@
 #include "kernels.hpp"
 #include "stencil.cuh"
 
+#include <cstdlib>
+
 namespace sgpu {
 
 namespace {
@@ -89,8 +91,8 @@ struct Rec {
 // streaming of k_mom_stream (fused.cu): cell (r, j) of colour c at step r + 2c, two steps per
 // barrier for five colours, strip halo 2 per colour. The next super-step's records are loaded one
 // super-step ahead into the other of two register sets. e_zero: e_in is zero and is not read.
-template <int NCOL, bool V, int NT>
-__global__ void __launch_bounds__(NT, 3)
+template <int NCOL, bool V, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
     k_corr_stream(DevParams p, const float* __restrict__ ein, float* __restrict__ eout,
                   const float4* __restrict__ rec, int e_zero, int seg_rows) {
     constexpr int SPB = NCOL == 5 ? 2 : 1;
@@ -291,19 +293,36 @@ __global__ void k_correct_mixed(DevParams p, const float* __restrict__ pc32, int
     pc64[q] = pc;
 }
 
-template <int NCOL, bool V, int NT>
+Range update_range(const DevParams& p, bool v) {
+    const int H = p.H;
+    return v ? Range{H + 1, p.NX + H - 1, H + 1, p.NY + H} : Range{H, p.NX + H - 1, H + 1, p.NY + H - 1};
+}
+
+// Resident CTAs per SM the correction sweep's registers are bounded for: 3, or 4 when
+// SGPU_CORR_MINB=4 (a tuning switch: the arithmetic is the same).
+int corr_minb() {
+    static const int v = [] {
+        const char* e = std::getenv("SGPU_CORR_MINB");
+        return e && std::atoi(e) == 4 ? 4 : 3;
+    }();
+    return v;
+}
+
+template <int NCOL, bool V, int NT, int MINB>
 void launch_corr(const DevParams& p, const float* ein, float* eout, const float4* rec, bool e_zero,
                  int seg_rows, cudaStream_t st) {
     constexpr int W = NT - 4 * NCOL;
     const dim3 grid((p.ncols + W - 1) / W, (p.nrows + seg_rows - 1) / seg_rows);
     constexpr int smem = kRing * NT * static_cast<int>(sizeof(float));
-    k_corr_stream<NCOL, V, NT><<<grid, NT, smem, st>>>(p, ein, eout, rec, e_zero ? 1 : 0, seg_rows);
+    k_corr_stream<NCOL, V, NT, MINB><<<grid, NT, smem, st>>>(p, ein, eout, rec, e_zero ? 1 : 0, seg_rows);
     SGPU_LAUNCH();
 }
 
-Range update_range(const DevParams& p, bool v) {
-    const int H = p.H;
-    return v ? Range{H + 1, p.NX + H - 1, H + 1, p.NY + H} : Range{H, p.NX + H - 1, H + 1, p.NY + H - 1};
+template <int NCOL, bool V>
+void launch_corr_m(const DevParams& p, const float* ein, float* eout, const float4* rec, bool e_zero,
+                   int seg_rows, cudaStream_t st) {
+    if (corr_minb() == 4) launch_corr<NCOL, V, 256, 4>(p, ein, eout, rec, e_zero, seg_rows, st);
+    else launch_corr<NCOL, V, 256, 3>(p, ein, eout, rec, e_zero, seg_rows, st);
 }
 
 } // namespace
@@ -358,29 +377,33 @@ void launch_correct_mixed(const DevParams& p, const LevelView32& L0, const doubl
 void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, float* eout,
                        const float4* rec, bool e_zero, int seg_rows, cudaStream_t st) {
     if (p.ncol == 5) {
-        if (v_component) launch_corr<5, true, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
-        else launch_corr<5, false, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
+        if (v_component) launch_corr_m<5, true>(p, ein, eout, rec, e_zero, seg_rows, st);
+        else launch_corr_m<5, false>(p, ein, eout, rec, e_zero, seg_rows, st);
     } else {
-        if (v_component) launch_corr<2, true, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
-        else launch_corr<2, false, 256>(p, ein, eout, rec, e_zero, seg_rows, st);
+        if (v_component) launch_corr_m<2, true>(p, ein, eout, rec, e_zero, seg_rows, st);
+        else launch_corr_m<2, false>(p, ein, eout, rec, e_zero, seg_rows, st);
     }
 }
 
 void init_mixed_kernels() {
     const int smem = kRing * 256 * static_cast<int>(sizeof(float));
-    SGPU_CUDA(cudaFuncSetAttribute(k_corr_stream<5, false, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    SGPU_CUDA(cudaFuncSetAttribute(k_corr_stream<5, true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    SGPU_CUDA(cudaFuncSetAttribute(k_corr_stream<2, false, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    SGPU_CUDA(cudaFuncSetAttribute(k_corr_stream<2, true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+#define SGPU_SMEM(NC, V, M) \
+    SGPU_CUDA(cudaFuncSetAttribute(k_corr_stream<NC, V, 256, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))
+    SGPU_SMEM(5, false, 3); SGPU_SMEM(5, true, 3); SGPU_SMEM(2, false, 3); SGPU_SMEM(2, true, 3);
+    SGPU_SMEM(5, false, 4); SGPU_SMEM(5, true, 4); SGPU_SMEM(2, false, 4); SGPU_SMEM(2, true, 4);
+#undef SGPU_SMEM
 }
 
 int corr_blocks_per_sm(int ncol) {
     const int smem = kRing * 256 * static_cast<int>(sizeof(float));
     int n = 0;
+    const bool four = corr_minb() == 4;
     if (ncol == 5)
-        SGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_corr_stream<5, false, 256>, 256, smem));
+        SGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, four ? k_corr_stream<5, false, 256, 4> : k_corr_stream<5, false, 256, 3>, 256, smem));
     else
-        SGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_corr_stream<2, false, 256>, 256, smem));
+        SGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, four ? k_corr_stream<2, false, 256, 4> : k_corr_stream<2, false, 256, 3>, 256, smem));
     return n > 0 ? n : 1;
 }
 

@@ -21,6 +21,10 @@ struct SumScratch {
 };
 void launch_ordered_sum(const double* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
                         double* out, const SumScratch& s, const int* skip, cudaStream_t st);
+// One plane in the same order with a small shared-memory footprint (a 3-tile ring, 25 KB): slower
+// alone, but it can run on a second stream beside a kernel whose grid fills the SMs.
+void launch_ordered_sum_lean(const double* vals, int ld, int nr, int nc, double* out, const SumScratch& s,
+                             cudaStream_t st);
 // The same order over FP32 values, each widened to double before it is added.
 void launch_ordered_sum(const float* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
                         double* out, const SumScratch& s, const int* skip, cudaStream_t st);

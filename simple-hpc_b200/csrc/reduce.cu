@@ -20,7 +20,8 @@ namespace sgpu {
 namespace {
 
 constexpr int kTile = 32;   // columns per tile (and rows per warp)
-constexpr int kStages = 12; // tiles in flight per warp
+constexpr int kStages = 12; // tiles in flight per warp (the standalone sum)
+constexpr int kLeanStages = 3; // the lean variant: little shared memory, to run beside other kernels
 constexpr int kPitch = kTile + 1; // padded tile row: lanes reading one column hit distinct banks
 
 template <class T> __device__ __forceinline__ void cp_async(T* smem, const T* gmem) {
@@ -36,7 +37,7 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 }
 
 // One warp per CTA (32 rows); the grid covers ceil(nr / 32) x K planes.
-template <class TIn>
+template <class TIn, int STAGES>
 __global__ void __launch_bounds__(32)
     k_ordered_sum(const TIn* __restrict__ vals, std::size_t plane_stride, int ld, int nr, int nc,
                   double* __restrict__ rows, unsigned int* counter, double* __restrict__ out,
@@ -58,19 +59,19 @@ __global__ void __launch_bounds__(32)
             const int c = k * kTile + lane;
             if (c < nc)
                 for (int rr = 0; rr < nrow; ++rr)
-                    cp_async(&tile[k % kStages][rr][lane], src + static_cast<std::size_t>(rr) * ld + c);
+                    cp_async(&tile[k % STAGES][rr][lane], src + static_cast<std::size_t>(rr) * ld + c);
         }
         cp_async_commit();
     };
-    for (int k = 0; k < kStages - 1; ++k) issue(k);
+    for (int k = 0; k < STAGES - 1; ++k) issue(k);
 
     double s = 0.0; // this lane's row: r0 + lane
     for (int k = 0; k < ntiles; ++k) {
-        issue(k + kStages - 1);
-        cp_async_wait<kStages - 1>(); // tile k has landed (this lane's copies)
+        issue(k + STAGES - 1);
+        cp_async_wait<STAGES - 1>(); // tile k has landed (this lane's copies)
         __syncwarp();                 // ... and everyone's
         const int cnt = min(kTile, nc - k * kTile);
-        const TIn* t = tile[k % kStages][lane];
+        const TIn* t = tile[k % STAGES][lane];
         if (cnt == kTile) {
             double v[kTile];
 #pragma unroll
@@ -128,7 +129,7 @@ __global__ void __launch_bounds__(32)
     if (lane == 0) *counter = 0u; // ready for the next launch on this stream
 }
 
-template <class TIn>
+template <class TIn, int STAGES>
 void launch_sum(const TIn* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
                 double* out, const SumScratch& s, const int* skip, cudaStream_t st) {
     if (K < 1 || K > 32 || K > s.max_k || nr > s.max_rows)
@@ -138,16 +139,16 @@ void launch_sum(const TIn* vals, std::size_t plane_stride, int ld, int nr, int n
         return;
     }
     const dim3 grid((nr + kTile - 1) / kTile, K);
-    constexpr int smem = kStages * kTile * kPitch * static_cast<int>(sizeof(TIn));
+    constexpr int smem = STAGES * kTile * kPitch * static_cast<int>(sizeof(TIn));
     static bool attr = false; // per process
     if (!attr) {
-        SGPU_CUDA(cudaFuncSetAttribute(k_ordered_sum<TIn>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        SGPU_CUDA(cudaFuncSetAttribute(k_ordered_sum<TIn, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         attr = true;
     }
     // Rows per staged chunk of the final pass: K planes of (chunk + 1) doubles fit the tile ring.
     const int chunk = std::min(2048, (smem / (static_cast<int>(sizeof(double)) * K) - 1) / kTile * kTile);
-    k_ordered_sum<TIn><<<grid, 32, smem, st>>>(vals, plane_stride, ld, nr, nc, s.rows, s.counter, out,
-                                                skip, chunk);
+    k_ordered_sum<TIn, STAGES><<<grid, 32, smem, st>>>(vals, plane_stride, ld, nr, nc, s.rows, s.counter, out,
+                                                        skip, chunk);
     SGPU_LAUNCH();
 }
 
@@ -155,12 +156,17 @@ void launch_sum(const TIn* vals, std::size_t plane_stride, int ld, int nr, int n
 
 void launch_ordered_sum(const double* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
                         double* out, const SumScratch& s, const int* skip, cudaStream_t st) {
-    launch_sum(vals, plane_stride, ld, nr, nc, K, out, s, skip, st);
+    launch_sum<double, kStages>(vals, plane_stride, ld, nr, nc, K, out, s, skip, st);
 }
 
 void launch_ordered_sum(const float* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
                         double* out, const SumScratch& s, const int* skip, cudaStream_t st) {
-    launch_sum(vals, plane_stride, ld, nr, nc, K, out, s, skip, st);
+    launch_sum<float, kStages>(vals, plane_stride, ld, nr, nc, K, out, s, skip, st);
+}
+
+void launch_ordered_sum_lean(const double* vals, int ld, int nr, int nc, double* out, const SumScratch& s,
+                             cudaStream_t st) {
+    launch_sum<double, kLeanStages>(vals, 0, ld, nr, nc, 1, out, s, nullptr, st);
 }
 
 } // namespace sgpu

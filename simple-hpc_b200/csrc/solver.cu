@@ -217,9 +217,10 @@ struct Solver {
         if (vcomp) launch_bc_v(dp, v, st);
         else launch_bc_u(dp, u, st);
         mark(vcomp ? SGPU_PH_ASSEMBLE_V : SGPU_PH_ASSEMBLE_U);
-        launch_mom_prep(dp, vcomp, x, oth, pf, xF, AP, cells, st);
+        double* cplane = cells + (vcomp ? plane : 0);
+        launch_mom_prep(dp, vcomp, x, oth, pf, xF, AP, cplane, st);
         mark(vcomp ? SGPU_PH_RESIDUAL_V : SGPU_PH_RESIDUAL_U);
-        momentum_sum(vcomp, res);
+        momentum_sum(vcomp, res, cplane);
         mark(vcomp ? SGPU_PH_SWEEP_V : SGPU_PH_SWEEP_U);
         const int n = vcomp ? prm.maxit_inner_v : prm.maxit_inner_u;
         double* in = x;
@@ -233,16 +234,36 @@ struct Solver {
         if (in != x) launch_copy(in, x, g.elems(), st);
     }
 
-    // res_u / res_v: the ordered sum of |R| over the residual range (on the solver's stream: a
-    // concurrent sum would hold shared memory the sweep's single wave of CTAs needs).
-    void momentum_sum(bool vcomp, double* res) {
-        if (vcomp) launch_ordered_sum(cells, 0, prm.NY, prm.NX - 1, prm.NY, 1, res, ss, nullptr, st);
-        else launch_ordered_sum(cells, 0, prm.NY - 1, prm.NX, prm.NY - 1, 1, res, ss, nullptr, st);
+    // res_u / res_v: the ordered sum of |R| over the residual range, on the solver's stream. The sums
+    // feed only the stopping test, and SGPU_SIDE_SUMS=1 runs them on a side stream beside the sweeps
+    // (lean sum kernel; u and v |R| in separate planes; joined before assemble_p). Measured at
+    // 4096^2 that is slower: a co-resident sum CTA stops the sweep's one-wave grid of 3 CTAs/SM
+    // from fitting (sweeps 1.9 -> 2.7 ms against 0.2 ms of sums), so the default is off.
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork[2] = {}, ev_done[2] = {};
+    bool side_sums = false;
+    void momentum_sum(bool vcomp, double* res, const double* vals) {
+        const int nr = vcomp ? prm.NX - 1 : prm.NX, nc = vcomp ? prm.NY : prm.NY - 1;
+        if (!side_sums || !side) {
+            launch_ordered_sum(vals, 0, nc, nr, nc, 1, res, ss, nullptr, st);
+            return;
+        }
+        const int k = vcomp ? 1 : 0;
+        SGPU_CUDA(cudaEventRecord(ev_fork[k], st));
+        SGPU_CUDA(cudaStreamWaitEvent(side, ev_fork[k], 0));
+        launch_ordered_sum_lean(vals, nc, nr, nc, res, ss, side);
+        SGPU_CUDA(cudaEventRecord(ev_done[k], side));
+    }
+    void join_sums() {
+        if (!side_sums || !side) return;
+        SGPU_CUDA(cudaStreamWaitEvent(st, ev_done[0], 0));
+        SGPU_CUDA(cudaStreamWaitEvent(st, ev_done[1], 0));
     }
 
     void fast_iteration_enqueue(double* res3) {
         fast_momentum(false, res3 + 0);
         fast_momentum(true, res3 + 1);
+        join_sums();
         mark(SGPU_PH_ASSEMBLE_P);
         launch_assemble_p_fused(dp, cu.a[8], cv.a[8], u, v, w, cells, nullptr, st);
         launch_ordered_sum(cells, 0, prm.NY, prm.NX, prm.NY, 1, res3 + 2, ss, nullptr, st);
@@ -331,9 +352,10 @@ struct Solver {
         if (vcomp) launch_bc_v(dp, v, st);
         else launch_bc_u(dp, u, st);
         mark(vcomp ? SGPU_PH_ASSEMBLE_V : SGPU_PH_ASSEMBLE_U);
-        launch_mom_prep_mixed(dp, vcomp, x, oth, pf, AP, cells, rec32, st);
+        double* cplane = cells + (vcomp ? plane : 0);
+        launch_mom_prep_mixed(dp, vcomp, x, oth, pf, AP, cplane, rec32, st);
         mark(vcomp ? SGPU_PH_RESIDUAL_V : SGPU_PH_RESIDUAL_U);
-        momentum_sum(vcomp, res);
+        momentum_sum(vcomp, res, cplane);
         mark(vcomp ? SGPU_PH_SWEEP_V : SGPU_PH_SWEEP_U);
         const int n = vcomp ? prm.maxit_inner_v : prm.maxit_inner_u;
         int cur = 0; // e32[cur] holds the current correction (zero before the first sweep)
@@ -350,6 +372,7 @@ struct Solver {
         p_links_stale = true;
         mixed_momentum(false, res3 + 0);
         mixed_momentum(true, res3 + 1);
+        join_sums();
         mark(SGPU_PH_ASSEMBLE_P);
         launch_assemble_p_mixed(dp, cu.a[8], cv.a[8], u, v, w.b, lv32[0], cells, cells + plane, st);
         launch_ordered_sum(cells, plane, prm.NY, prm.NX, prm.NY, 2, sums + 24, ss, nullptr, st);
@@ -545,6 +568,12 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
         SGPU_CUDA(cudaGetDevice(&dev));
         SGPU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         seg_rows = stream_seg_rows(dp, sms);
+        if (const char* e = std::getenv("SGPU_SIDE_SUMS")) side_sums = std::atoi(e) != 0;
+        SGPU_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; ++k) {
+            SGPU_CUDA(cudaEventCreateWithFlags(&ev_fork[k], cudaEventDisableTiming));
+            SGPU_CUDA(cudaEventCreateWithFlags(&ev_done[k], cudaEventDisableTiming));
+        }
     }
     plane = static_cast<std::size_t>(p.NX) * p.NY;
     const int kplanes = p.pressure_solver == SGPU_P_CG ? 4 : 2;
@@ -689,6 +718,12 @@ Solver::~Solver() {
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : sw_ev)
         if (e) cudaEventDestroy(e);
+    if (side) cudaStreamSynchronize(side);
+    for (int k = 0; k < 2; ++k) {
+        if (ev_fork[k]) cudaEventDestroy(ev_fork[k]);
+        if (ev_done[k]) cudaEventDestroy(ev_done[k]);
+    }
+    if (side) cudaStreamDestroy(side);
 
     for (void* q : allocs) cudaFree(q);
     if (host_res) cudaFreeHost(host_res);

@@ -85,6 +85,7 @@ typedef struct sgpu_params {
     double dx, dy, nu;
     char output_dir[512];
     char cnn_weights[512];      /* key cnn_weights: path of a trained warm-start network */
+    char restart_from[512];     /* key restart_from: directory of u.csv, v.csv, p.csv to start from */
 } sgpu_params_t;
 
 /*
@@ -238,6 +239,15 @@ long long sgpu_launch_count(void);
 int sgpu_write_outputs(const sgpu_params_t* p, const double* u, const double* v, const double* pf,
                        const double* log, int iterations, const sgpu_result_t* result,
                        const char* cfg_path, const char* git_hash, const char* compiler);
+
+/*
+ * Restart (key restart_from; the reference always starts from u = v = p = 0): read u.csv, v.csv and
+ * p.csv from dir into host arrays of nrows x ncols, the files sgpu_write_outputs writes (full arrays,
+ * halos included, %.18e: the values round-trip exactly). A run restarted from the files of a run of
+ * k iterations continues with the fields of iteration k. Runs on the host only; a file with the
+ * wrong shape or an unparsable value is an SGPU_E_INVALID error naming it.
+ */
+int sgpu_read_fields(const sgpu_params_t* p, const char* dir, double* u, double* v, double* pf);
 
 /* ---- learned warm start for p' (keys warm_start, cnn_weights) ----
  *

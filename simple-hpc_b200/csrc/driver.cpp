@@ -80,6 +80,7 @@ struct Handle {
 
 } // namespace
 
+extern "C" int sgpu_read_fields(const sgpu_params_t* p, const char* dir, double* u, double* v, double* pf);
 extern "C" int sgpu_write_outputs(const sgpu_params_t* p, const double* u, const double* v,
                                   const double* pf, const double* log, int iterations,
                                   const sgpu_result_t* result, const char* cfg_path,
@@ -108,13 +109,16 @@ int main(int argc, char** argv) {
         std::fflush(stdout);
 
         Handle h;
-        check(sgpu_create(&p, nullptr, nullptr, nullptr, &h.h));
+        const std::size_t n = static_cast<std::size_t>(p.nrows) * p.ncols;
+        std::vector<double> u(n), v(n), pf(n);
+        const bool restart = p.restart_from[0] != '\0';
+        if (restart) check(sgpu_read_fields(&p, p.restart_from, u.data(), v.data(), pf.data()));
+        check(sgpu_create(&p, restart ? u.data() : nullptr, restart ? v.data() : nullptr,
+                          restart ? pf.data() : nullptr, &h.h));
         check(sgpu_set_profiling(h.h, 1));
         std::vector<double> log(4 * static_cast<std::size_t>(p.maxit > 0 ? p.maxit : 1));
         sgpu_result_t r{};
         check(sgpu_run(h.h, p.maxit, log.data(), 100, &r));
-        const std::size_t n = static_cast<std::size_t>(p.nrows) * p.ncols;
-        std::vector<double> u(n), v(n), pf(n);
         check(sgpu_download(h.h, SGPU_F_U, u.data()));
         check(sgpu_download(h.h, SGPU_F_V, v.data()));
         check(sgpu_download(h.h, SGPU_F_P, pf.data()));

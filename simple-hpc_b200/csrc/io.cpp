@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <filesystem>
 #include <string>
@@ -190,7 +191,77 @@ void write_outputs(const sgpu_params_t& p, const double* u, const double* v, con
     std::fclose(fp);
 }
 
+// Reads a rows x cols CSV of doubles (the format write_csv writes: comma-separated, one line per
+// row). Rows are parsed in parallel blocks once their line starts are known.
+void read_csv(const std::string& path, double* out, int rows, int cols) {
+    std::FILE* fp = std::fopen(path.c_str(), "rb");
+    if (!fp) throw Error(SGPU_E_INVALID, "restart: cannot read " + path);
+    std::string text;
+    {
+        std::fseek(fp, 0, SEEK_END);
+        const long n = std::ftell(fp);
+        std::fseek(fp, 0, SEEK_SET);
+        text.resize(n > 0 ? static_cast<std::size_t>(n) : 0);
+        const std::size_t got = n > 0 ? std::fread(&text[0], 1, text.size(), fp) : 0;
+        std::fclose(fp);
+        if (got != text.size()) throw Error(SGPU_E_INVALID, "restart: short read of " + path);
+    }
+    std::vector<std::size_t> starts;
+    starts.reserve(static_cast<std::size_t>(rows) + 1);
+    std::size_t pos = 0;
+    while (pos < text.size()) {
+        starts.push_back(pos);
+        const std::size_t nl = text.find('\n', pos);
+        pos = nl == std::string::npos ? text.size() : nl + 1;
+    }
+    if (static_cast<int>(starts.size()) != rows)
+        throw Error(SGPU_E_INVALID, "restart: " + path + " has " + std::to_string(starts.size()) +
+                                        " rows, the configuration needs " + std::to_string(rows));
+    starts.push_back(text.size());
+    const int nt = std::max(1, std::min<int>(static_cast<int>(std::thread::hardware_concurrency()), 32));
+    std::vector<std::string> errors(static_cast<std::size_t>(nt));
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t)
+        th.emplace_back([&, t] {
+            for (int i = t; i < rows && errors[t].empty(); i += nt) {
+                const char* c = text.c_str() + starts[i];
+                const char* end = text.c_str() + starts[i + 1];
+                for (int j = 0; j < cols; ++j) {
+                    char* stop = nullptr;
+                    const double val = std::strtod(c, &stop);
+                    const bool sep_ok = j + 1 < cols ? (stop < end && *stop == ',')
+                                                     : (stop == end || *stop == '\n' || *stop == '\r');
+                    if (stop == c || !sep_ok) {
+                        errors[t] = "restart: " + path + " row " + std::to_string(i + 1) +
+                                    ": expected " + std::to_string(cols) + " comma-separated numbers";
+                        break;
+                    }
+                    out[static_cast<std::size_t>(i) * cols + j] = val;
+                    c = stop + 1;
+                }
+            }
+        });
+    for (auto& x : th) x.join();
+    for (const auto& e : errors)
+        if (!e.empty()) throw Error(SGPU_E_INVALID, e);
+}
+
 } // namespace sgpu
+
+extern "C" int sgpu_read_fields(const sgpu_params_t* p, const char* dir, double* u, double* v, double* pf) {
+    if (!p || !dir || !u || !v || !pf) return sgpu::fail(SGPU_E_INVALID, "sgpu_read_fields: null argument");
+    try {
+        const std::filesystem::path d(dir);
+        sgpu::read_csv((d / "u.csv").string(), u, p->nrows, p->ncols);
+        sgpu::read_csv((d / "v.csv").string(), v, p->nrows, p->ncols);
+        sgpu::read_csv((d / "p.csv").string(), pf, p->nrows, p->ncols);
+        return SGPU_OK;
+    } catch (const sgpu::Error& e) {
+        return sgpu::fail(e.code, e.what());
+    } catch (const std::exception& e) {
+        return sgpu::fail(SGPU_E_INVALID, e.what());
+    }
+}
 
 extern "C" int sgpu_write_outputs(const sgpu_params_t* p, const double* u, const double* v,
                                   const double* pf, const double* log, int iterations,

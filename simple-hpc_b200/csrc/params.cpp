@@ -5,7 +5,7 @@
 // an empty key or value, or a repeated key is an error naming the line. Building the parameters
 // follows make_params (src/params.cpp:50-180): a whitelist of keys, integer / number / True|False /
 // enum parsing with the reference's messages, validation, and the derived nrows, ncols, dx, dy, nu.
-// Keys added by this build (precision, mg_mode, warm_start, cnn_weights, graph_batch) are accepted
+// Keys added by this build (precision, mg_mode, warm_start, cnn_weights, graph_batch, restart_from) are accepted
 // here only; every reference key keeps its meaning and default.
 #include "common.hpp"
 
@@ -177,7 +177,7 @@ void params_from_config(const std::string& text, sgpu_params_t& p) {
         "pressure_tolerance", "pressure_maxit", "mg_cycles", "mg_pre", "mg_post", "mg_omega",
         "mpi_grid", "halo_overlap", "write_fields",
         // this build
-        "precision", "mg_mode", "warm_start", "cnn_weights", "graph_batch"};
+        "precision", "mg_mode", "warm_start", "cnn_weights", "graph_batch", "restart_from"};
     // The reference iterates a std::map, so the first unknown key in sorted order is reported.
     std::map<std::string, std::string> sorted(kv.begin(), kv.end());
     for (const auto& e : sorted)
@@ -245,6 +245,7 @@ void params_from_config(const std::string& text, sgpu_params_t& p) {
         else if (k == "warm_start")
             p.warm_start = parse_choice(k, v, {{"zero", 0}, {"cnn", 1}});
         else if (k == "cnn_weights") copy_str(p.cnn_weights, sizeof p.cnn_weights, v);
+        else if (k == "restart_from") copy_str(p.restart_from, sizeof p.restart_from, v);
         else if (k == "graph_batch") p.graph_batch = parse_int(k, v);
     }
     params_finalize(p);

@@ -60,6 +60,7 @@ class Params(C.Structure):
         ("precision", C.c_int), ("mg_mode", C.c_int), ("warm_start", C.c_int), ("graph_batch", C.c_int),
         ("nrows", C.c_int), ("ncols", C.c_int), ("dx", C.c_double), ("dy", C.c_double), ("nu", C.c_double),
         ("output_dir", C.c_char * 512), ("cnn_weights", C.c_char * 512),
+        ("restart_from", C.c_char * 512),
     ]
 
     @property
@@ -115,6 +116,7 @@ def lib() -> C.CDLL:
             "sgpu_stream": (I, [H, C.POINTER(C.c_void_p)]), "sgpu_launch_count": (C.c_longlong, []),
             "sgpu_write_outputs": (I, [P, D, D, D, D, I, C.POINTER(Result), C.c_char_p, C.c_char_p,
                                        C.c_char_p]),
+            "sgpu_read_fields": (I, [P, C.c_char_p, D, D, D]),
             # learned warm start
             "sgpu_cnn_load": (I, [H, C.c_char_p]),
             "sgpu_cnn_create": (I, [I, I, C.c_uint, C.POINTER(H)]),
@@ -336,6 +338,13 @@ def write_outputs(p: Params, u: np.ndarray, v: np.ndarray, pf: np.ndarray, log: 
     _check(lib().sgpu_write_outputs(C.byref(p), *(_dptr(a) for a in arrs), _dptr(lg), lg.shape[0],
                                     C.byref(result), cfg_path.encode(), git_hash.encode(),
                                     compiler.encode()))
+
+
+def read_fields(p: Params, directory) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """u, v, p from the u.csv, v.csv, p.csv a run wrote into `directory` (restart_from)."""
+    out = [np.empty((p.nrows, p.ncols)) for _ in range(3)]
+    _check(lib().sgpu_read_fields(C.byref(p), str(directory).encode(), *(_dptr(a) for a in out)))
+    return out[0], out[1], out[2]
 
 
 def launch_count() -> int:

@@ -14,7 +14,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from conftest import REPO, config_text, cuda_available, snapshot_config
+from conftest import REPO, bit_equal, config_text, cuda_available, snapshot_config
 
 FIELD_FILES = ["u.csv", "v.csv", "p.csv", "ux_centre.csv", "uy_centre.csv", "alog.csv"]
 
@@ -96,3 +96,53 @@ def test_cli_gpu_run_writes_reference_outputs(sgpu_mod, oracle_mod, tmp_path):
         assert (tmp_path / "out" / name).read_bytes() == (ref_dir / name).read_bytes(), name
     info = json.loads((tmp_path / "out" / "run_info.json").read_text())
     assert info["backend"] == "gpu" and info["iterations"] == log.shape[0] and info["converged"]
+
+
+def test_restart_files_round_trip(sgpu_mod, tmp_path):
+    """restart_from reads back exactly the u.csv, v.csv, p.csv the writer writes (%.18e)."""
+    cfg = snapshot_config("short_16")
+    cfg["output_dir"] = str(tmp_path / "run")
+    p = sgpu_mod.params_from_config(config_text(cfg))
+    rng = np.random.default_rng(4)
+    u, v, pf = (rng.normal(size=(p.nrows, p.ncols)) * 10.0 ** rng.integers(-300, 300, (p.nrows, p.ncols))
+                for _ in range(3))
+    u[0, 0], v[1, 1], pf[2, 2] = -0.0, 5e-324, -1.7976931348623157e308
+    sgpu_mod.write_outputs(p, u, v, pf, np.zeros((1, 4)))
+    ru, rv, rp = sgpu_mod.read_fields(p, tmp_path / "run")
+    for a, b in ((ru, u), (rv, v), (rp, pf)):
+        assert a.view(np.uint64).tolist() == b.view(np.uint64).tolist()
+    # a grid of another size, a missing file and a damaged value are errors naming the file
+    cfg2 = dict(cfg, N_cells_x="20")
+    p2 = sgpu_mod.params_from_config(config_text(cfg2))
+    with pytest.raises(sgpu_mod.SgpuError, match="u.csv has"):
+        sgpu_mod.read_fields(p2, tmp_path / "run")
+    with pytest.raises(sgpu_mod.SgpuError, match="cannot read"):
+        sgpu_mod.read_fields(p, tmp_path / "nowhere")
+    f = tmp_path / "run" / "v.csv"
+    f.write_text(f.read_text().replace(",", ",x", 1))
+    with pytest.raises(sgpu_mod.SgpuError, match="v.csv row 1"):
+        sgpu_mod.read_fields(p, tmp_path / "run")
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")
+def test_restart_continues_the_run(sgpu_mod, tmp_path):
+    """10 iterations, written out, then 10 more from restart_from: the fields of 20 straight."""
+    base = snapshot_config("converged_32x40")
+    base.update(momentum_solver="gs_multicolour", pressure_solver="mg", error_tolerance="0")
+    p = sgpu_mod.params_from_config(config_text(dict(base, output_dir=str(tmp_path / "a"))))
+    with sgpu_mod.Solver(p) as s:
+        res, log = s.run(10)
+        f10 = [s.download(k) for k in (0, 1, 2)]
+    sgpu_mod.write_outputs(p, *f10, log, res)
+    p2 = sgpu_mod.params_from_config(config_text(dict(base, restart_from=str(tmp_path / "a"))))
+    assert p2.restart_from.decode() == str(tmp_path / "a")
+    u, v, pf = sgpu_mod.read_fields(p2, p2.restart_from.decode())
+    with sgpu_mod.Solver(p2, u, v, pf) as s:
+        s.run(10)
+        restarted = [s.download(k) for k in (0, 1, 2)]
+    with sgpu_mod.Solver(p) as s:
+        s.run(20)
+        straight = [s.download(k) for k in (0, 1, 2)]
+    for a, b in zip(restarted, straight):
+        assert bit_equal(a, b)

@@ -466,7 +466,7 @@ def main() -> None:
     cells = (p.NX - 1) * p.NY  # cells one sweep updates: u NX x (NY-1), v (NX-1) x NY (square grid)
     if args.precision == "mixed":
         kernel = "k_corr_stream (one FP32 multicolour correction sweep)"
-        bytes_per_cell = 48 + 4 + 4  # record read, e_in read, e_out written
+        bytes_per_cell = 40 + 4 + 4  # record (near links, far links, 1/AP and R) read, e_in read, e_out written
     else:
         kernel = "k_mom_stream (one FP64 multicolour sweep)"
         bytes_per_cell = 5 * 8  # x_in, frozen x, other velocity, p read; x_out written

@@ -140,14 +140,21 @@ void launch_cg_dir(const DevParams& p, CgPtr cg, const CgScalars* sc, cudaStream
 void init_mixed_kernels();
 // Resident CTAs per SM of the FP32 correction sweep (its register and shared-memory footprint).
 int corr_blocks_per_sm(int ncol);
-// FP64 prep: |R| into cells, AP (FP64), and per cell a 48-byte FP32 record (3 float4:
-// AE AW AN AS | AEE AWW ANN ASS | 1/AP R 0 0) at rec + 3 * (i * pitch + j), over the update range.
+// Per-cell FP32 momentum records of the mixed path, three arrays indexed like the fields
+// (i * pitch + j): the near links {AE AW AN AS}, the far links {AEE AWW ANN ASS}, and {1/AP, R}.
+// 40 bytes per cell; a warp's load of each array is contiguous.
+struct MomRec32 {
+    float4* near_links;
+    float4* far_links;
+    float2* diag;
+};
+// FP64 prep: |R| into cells, AP (FP64), and the cell's FP32 record, over the update range.
 void launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x, const double* oth,
-                           const double* pf, double* AP, double* cells, float4* rec,
+                           const double* pf, double* AP, double* cells, MomRec32 rec,
                            cudaStream_t st);
 // One FP32 multicolour correction sweep e_in -> e_out (e_zero: e_in is zero and not read).
 void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, float* eout,
-                       const float4* rec, bool e_zero, int seg_rows, cudaStream_t st);
+                       MomRec32 rec, bool e_zero, int seg_rows, cudaStream_t st);
 // x += e over the component's update range.
 void launch_add_correction(const DevParams& p, bool v_component, double* x, const float* e,
                            cudaStream_t st);

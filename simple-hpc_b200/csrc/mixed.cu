@@ -4,9 +4,9 @@
 // depend on stays FP64:
 //  * Momentum. The FP64 prep pass computes each cell's coefficients and the residual
 //    R = nb(u) + pressure term - AP u exactly as the FP64 path does (momentum_u.cpp:43-59), so
-//    res_u / res_v and their ordered sums are FP64. It also stores, per cell, one 48-byte FP32
-//    record: the 8 neighbour coefficients, 1/AP and R. The maxit_inner multicolour sweeps then run
-//    on the correction e = u_new - u in FP32: the reference's update
+//    res_u / res_v and their ordered sums are FP64. It also stores, per cell, a 40-byte FP32
+//    record in three arrays: the 8 neighbour coefficients, 1/AP and R. The maxit_inner
+//    multicolour sweeps then run on the correction e = u_new - u in FP32: the reference's update
 //    u <- a (nb(u) + pt) / AP + (1 - a) u (momentum_u.cpp:136-137) is, for u = u0 + e, exactly
 //    e <- e + a ((R(u0) + nb(e)) / AP - e), applied in the same colour order by the same
 //    time-skewed streaming scheme as the FP64 sweep. The field update u += e is FP64.
@@ -47,7 +47,7 @@ template <bool V>
 __global__ void k_mom_prep_mixed(DevParams p, const double* __restrict__ x,
                                  const double* __restrict__ oth, const double* __restrict__ pf,
                                  double* __restrict__ AP, double* __restrict__ cells,
-                                 float4* __restrict__ rec, Range ur) {
+                                 MomRec32 rec, Range ur) {
     const int j = ur.j0 + static_cast<int>(blockIdx.x * 32 + threadIdx.x);
     const int i = ur.i0 + static_cast<int>(blockIdx.y * 8 + threadIdx.y);
     if (i > ur.i1 || j > ur.j1) return;
@@ -72,19 +72,19 @@ __global__ void k_mom_prep_mixed(DevParams p, const double* __restrict__ x,
     const double R = nb + pt - c.AP * x[q];
     cells[static_cast<std::size_t>(i - ur.i0) * ur.cols() + (j - ur.j0)] = fabs(R);
     AP[q] = c.AP;
-    float4* r = rec + 3 * q;
-    r[0] = make_float4(static_cast<float>(c.AE), static_cast<float>(c.AW), static_cast<float>(c.AN),
-                       static_cast<float>(c.AS));
-    r[1] = make_float4(static_cast<float>(c.AEE), static_cast<float>(c.AWW),
-                       static_cast<float>(c.ANN), static_cast<float>(c.ASS));
-    r[2] = make_float4(static_cast<float>(1.0 / c.AP), static_cast<float>(R), 0.0f, 0.0f);
+    rec.near_links[q] = make_float4(static_cast<float>(c.AE), static_cast<float>(c.AW),
+                                    static_cast<float>(c.AN), static_cast<float>(c.AS));
+    rec.far_links[q] = make_float4(static_cast<float>(c.AEE), static_cast<float>(c.AWW),
+                                   static_cast<float>(c.ANN), static_cast<float>(c.ASS));
+    rec.diag[q] = make_float2(static_cast<float>(1.0 / c.AP), static_cast<float>(R));
 }
 
 constexpr int kRing = 32;
 constexpr int kPrefetch = 8;
 
 struct Rec {
-    float4 a, b, c;
+    float4 a, b;
+    float2 c; // 1/AP, R
 };
 
 // One FP32 multicolour correction sweep e_in -> e_out from the stored records; the time-skewed
@@ -94,7 +94,7 @@ struct Rec {
 template <int NCOL, bool V, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     k_corr_stream(DevParams p, const float* __restrict__ ein, float* __restrict__ eout,
-                  const float4* __restrict__ rec, int e_zero, int seg_rows) {
+                  MomRec32 rec, int e_zero, int seg_rows) {
     constexpr int SPB = NCOL == 5 ? 2 : 1;
     constexpr int HC = 2 * NCOL;
     constexpr int W = NT - 2 * HC;
@@ -134,7 +134,9 @@ __global__ void __launch_bounds__(NT, MINB)
     }
     const float relax = static_cast<float>(V ? p.av : p.au);
     float* ringc = ring_mem + tid;
-    const float4* recc = rec + 3 * col;
+    const float4* __restrict__ rnear = rec.near_links + col;
+    const float4* __restrict__ rfar = rec.far_links + col;
+    const float2* __restrict__ rdiag = rec.diag + col;
     int next = L0;
     auto issue = [&]() {
         if (next < L1 && col_in) {
@@ -150,10 +152,10 @@ __global__ void __launch_bounds__(NT, MINB)
         return ((colmask >> c) & 1u) && r >= s_rmin[c] && r <= s_rmax[c];
     };
     auto load_rec = [&](int r, Rec& x) {
-        const float4* q = recc + 3 * r * ld;
-        x.a = __ldg(q);
-        x.b = __ldg(q + 1);
-        x.c = __ldg(q + 2);
+        const int o = r * ld;
+        x.a = __ldg(rnear + o);
+        if (NCOL == 5) x.b = __ldg(rfar + o);
+        x.c = __ldg(rdiag + o);
     };
     auto update = [&](int r, const Rec& x) {
         float* rc = ringc + (r & (kRing - 1)) * NT;
@@ -309,7 +311,7 @@ int corr_minb() {
 }
 
 template <int NCOL, bool V, int NT, int MINB>
-void launch_corr(const DevParams& p, const float* ein, float* eout, const float4* rec, bool e_zero,
+void launch_corr(const DevParams& p, const float* ein, float* eout, MomRec32 rec, bool e_zero,
                  int seg_rows, cudaStream_t st) {
     constexpr int W = NT - 4 * NCOL;
     const dim3 grid((p.ncols + W - 1) / W, (p.nrows + seg_rows - 1) / seg_rows);
@@ -319,7 +321,7 @@ void launch_corr(const DevParams& p, const float* ein, float* eout, const float4
 }
 
 template <int NCOL, bool V>
-void launch_corr_m(const DevParams& p, const float* ein, float* eout, const float4* rec, bool e_zero,
+void launch_corr_m(const DevParams& p, const float* ein, float* eout, MomRec32 rec, bool e_zero,
                    int seg_rows, cudaStream_t st) {
     if (corr_minb() == 4) launch_corr<NCOL, V, 256, 4>(p, ein, eout, rec, e_zero, seg_rows, st);
     else launch_corr<NCOL, V, 256, 3>(p, ein, eout, rec, e_zero, seg_rows, st);
@@ -331,7 +333,7 @@ void launch_corr_m(const DevParams& p, const float* ein, float* eout, const floa
 // with SGPU_FLOAT_UNIT for the FP32 correction sweep (contraction allowed).
 #ifndef SGPU_FLOAT_UNIT
 void launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x, const double* oth,
-                           const double* pf, double* AP, double* cells, float4* rec,
+                           const double* pf, double* AP, double* cells, MomRec32 rec,
                            cudaStream_t st) {
     const Range ur = update_range(p, v_component);
     if (ur.rows() <= 0 || ur.cols() <= 0) return;
@@ -375,7 +377,7 @@ void launch_correct_mixed(const DevParams& p, const LevelView32& L0, const doubl
 
 #else
 void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, float* eout,
-                       const float4* rec, bool e_zero, int seg_rows, cudaStream_t st) {
+                       MomRec32 rec, bool e_zero, int seg_rows, cudaStream_t st) {
     if (p.ncol == 5) {
         if (v_component) launch_corr_m<5, true>(p, ein, eout, rec, e_zero, seg_rows, st);
         else launch_corr_m<5, false>(p, ein, eout, rec, e_zero, seg_rows, st);

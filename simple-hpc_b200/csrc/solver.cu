@@ -338,7 +338,7 @@ struct Solver {
         launch_p_links_app(dp, cu.a[8], cv.a[8], w, st);
         p_links_stale = false;
     }
-    float4* rec32 = nullptr;          // per-cell FP32 records: coefficients, 1/AP, R
+    MomRec32 rec32{};                 // per-cell FP32 records: coefficients, 1/AP, R
     float* e32[2] = {nullptr, nullptr}; // correction ping-pong
     std::vector<LevelView32> lv32;    // FP32 multigrid hierarchy (level 0: the p' operator)
     std::vector<float*> mg32_x2;
@@ -670,7 +670,9 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
         mixed = true;
         init_mixed_kernels();
         seg_rows = stream_seg_rows(dp, sms, corr_blocks_per_sm(dp.ncol));
-        rec32 = dalloc<float4>(3 * g.elems());
+        rec32.near_links = dalloc<float4>(g.elems());
+        rec32.far_links = dalloc<float4>(g.elems());
+        rec32.diag = dalloc<float2>(g.elems());
         e32[0] = dalloc<float>(g.elems());
         e32[1] = dalloc<float>(g.elems());
         const int nl = static_cast<int>(lv.size());

@@ -18,6 +18,7 @@
 #include "stencil.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <climits>
 
 namespace sgpu {
@@ -478,13 +479,13 @@ void launch_stream_v(const DevParams& p, const double* xin, double* xout, const 
 
 // Rows per CTA segment of the streaming sweep: enough segments to fill the GPU with one wave of
 // 2 CTAs per SM, but never so short that the 2 * NCOL-row halo dominates.
-int stream_seg_rows(const DevParams& p, int sms, int blocks_per_sm) {
+int stream_seg_rows(const DevParams& p, int sms, int blocks_per_sm, int min_seg) {
     const int W = 256 - 4 * p.ncol;
     const int strips = (p.ncols + W - 1) / W;
     const int want = std::max(1, (blocks_per_sm * sms) / strips); // one wave of resident CTAs
     int seg = (p.nrows + want - 1) / want;
-    const int min_seg = 8 * p.ncol;
-    if (seg < min_seg) seg = min_seg;
+    const int lo = min_seg > 0 ? min_seg : 8 * p.ncol;
+    if (seg < lo) seg = lo;
     return seg;
 }
 

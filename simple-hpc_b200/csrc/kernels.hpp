@@ -111,11 +111,11 @@ bool mg_fast_supported(int pre, int post);
 // smoothed iterate is written to xout (F.x is left unchanged when pre > 0).
 template <class T>
 void launch_mg_down(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, int pre, bool x_zero,
-                    int sms, cudaStream_t st);
+                    int sms, int min_seg, cudaStream_t st);
 // xout = xin + omega * P C.x, then post red-black sweeps (F's coefficients and b).
 template <class T>
 void launch_mg_up(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, T* xout,
-                  double omega, int post, int sms, cudaStream_t st);
+                  double omega, int post, int sms, int min_seg, cudaStream_t st);
 
 // ---- conjugate gradient (cg.cu) ----
 struct CgScalars {
@@ -168,8 +168,9 @@ void launch_correct_mixed(const DevParams& p, const LevelView32& L0, const doubl
                           double* pc64, cudaStream_t st);
 
 // ---- fused fast path (fused.cu) ----
-// Rows per CTA segment of the streaming sweeps: one wave of blocks_per_sm resident CTAs per SM.
-int stream_seg_rows(const DevParams& p, int sms, int blocks_per_sm = 2);
+// Rows per CTA segment of the streaming sweeps: one wave of blocks_per_sm resident CTAs per SM, at
+// least min_seg rows (min_seg <= 0: 8 x the colour count).
+int stream_seg_rows(const DevParams& p, int sms, int blocks_per_sm = 2, int min_seg = 0);
 // Momentum prep: |R| into cells, AP over the update range, frozen copy xF of x.
 void launch_mom_prep(const DevParams& p, bool v_component, const double* x, const double* oth,
                      const double* pf, double* xF, double* AP, double* cells, cudaStream_t st);

@@ -15,6 +15,7 @@
 // below a size threshold and the coarsest solve run in one CTA (k_mg_tail in mg.cu).
 #include "kernels.hpp"
 
+#include <algorithm>
 #include <cstdlib>
 
 namespace sgpu {
@@ -270,15 +271,19 @@ __global__ void __launch_bounds__(NT, MINB)
 
 constexpr int kNT = 256;
 
-// Rows per CTA segment: one wave of the kernel's resident CTAs (blocks_per_sm per SM).
-int seg_for(int nx, int ny, int HC, int sms, int blocks_per_sm) {
+// Rows per CTA segment: one wave of the kernel's resident CTAs (blocks_per_sm per SM), at least
+// min_seg rows (min_seg <= 0: 2 HC + 8, which bounds the halo and skew rows a CTA walks besides its
+// own to about half of them). A lone small level is bound by the per-step latency of each CTA's
+// walk, so a single solve takes short segments and more CTAs; a batch of cavities fills the GPU
+// and keeps the bound.
+int seg_for(int nx, int ny, int HC, int sms, int blocks_per_sm, int min_seg) {
     const int W = kNT - 2 * HC;
     const int strips = (ny + W - 1) / W;
     const int want = (blocks_per_sm * sms) / strips > 0 ? (blocks_per_sm * sms) / strips : 1;
     int seg = (nx + want - 1) / want;
     seg = (seg + 1) & ~1; // even: restriction pairs stay inside one CTA
-    const int min_seg = 2 * HC + 8;
-    if (seg < min_seg) seg = min_seg;
+    const int lo = min_seg > 0 ? std::max(2, min_seg & ~1) : 2 * HC + 8;
+    if (seg < lo) seg = lo;
     return seg;
 }
 
@@ -311,14 +316,14 @@ int mg_variant64() {
 }
 
 template <int PRE, int PD, int MINB, class T>
-void down_v(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, bool x_zero, int sms,
+void down_v(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, bool x_zero, int sms, int min_seg,
             cudaStream_t st) {
     const int HC = 2 * PRE + 2;
     constexpr int smem = kRing * kNT * static_cast<int>(sizeof(T));
     static bool done = false;
     static int blocks = 0;
     auto kernel = k_mg_down<kNT, PRE, PD, MINB, T>;
-    const int seg = seg_for(F.nx, F.ny, HC, sms, prepare_kernel(kernel, smem, done, blocks));
+    const int seg = seg_for(F.nx, F.ny, HC, sms, prepare_kernel(kernel, smem, done, blocks), min_seg);
     const int W = kNT - 2 * HC;
     const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
     kernel<<<grid, kNT, smem, st>>>(F, C, xout, x_zero ? 1 : 0, seg, HC);
@@ -327,13 +332,13 @@ void down_v(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, bool x_zero
 
 template <int POST, int PD, int MINB, class T>
 void up_v(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, T* xout, double omega,
-          int sms, cudaStream_t st) {
+          int sms, int min_seg, cudaStream_t st) {
     const int HC = 2 * POST + 2;
     constexpr int smem = kRing * kNT * static_cast<int>(sizeof(T));
     static bool done = false;
     static int blocks = 0;
     auto kernel = k_mg_up<kNT, POST, PD, MINB, T>;
-    const int seg = seg_for(F.nx, F.ny, HC, sms, prepare_kernel(kernel, smem, done, blocks));
+    const int seg = seg_for(F.nx, F.ny, HC, sms, prepare_kernel(kernel, smem, done, blocks), min_seg);
     const int W = kNT - 2 * HC;
     const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
     kernel<<<grid, kNT, smem, st>>>(C, F, xin, xout, omega, seg, HC);
@@ -341,41 +346,41 @@ void up_v(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, T* xout,
 }
 
 template <int PRE, class T>
-void down_t(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, bool x_zero, int sms,
+void down_t(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, bool x_zero, int sms, int min_seg,
             cudaStream_t st) {
     if constexpr (sizeof(T) == 8) {
         switch (mg_variant64()) {
-        case 1: down_v<PRE, 1, 3>(F, C, xout, x_zero, sms, st); break;
-        case 2: down_v<PRE, 1, 4>(F, C, xout, x_zero, sms, st); break;
-        default: down_v<PRE, 2, 2>(F, C, xout, x_zero, sms, st); break;
+        case 1: down_v<PRE, 1, 3>(F, C, xout, x_zero, sms, min_seg, st); break;
+        case 2: down_v<PRE, 1, 4>(F, C, xout, x_zero, sms, min_seg, st); break;
+        default: down_v<PRE, 2, 2>(F, C, xout, x_zero, sms, min_seg, st); break;
         }
     } else {
         switch (mg_variant()) {
-        case 0: down_v<PRE, 3, 2>(F, C, xout, x_zero, sms, st); break;
-        case 1: down_v<PRE, 2, 3>(F, C, xout, x_zero, sms, st); break;
-        case 3: down_v<PRE, 1, 5>(F, C, xout, x_zero, sms, st); break;
-        case 4: down_v<PRE, 1, 6>(F, C, xout, x_zero, sms, st); break;
-        default: down_v<PRE, 1, 4>(F, C, xout, x_zero, sms, st); break;
+        case 0: down_v<PRE, 3, 2>(F, C, xout, x_zero, sms, min_seg, st); break;
+        case 1: down_v<PRE, 2, 3>(F, C, xout, x_zero, sms, min_seg, st); break;
+        case 3: down_v<PRE, 1, 5>(F, C, xout, x_zero, sms, min_seg, st); break;
+        case 4: down_v<PRE, 1, 6>(F, C, xout, x_zero, sms, min_seg, st); break;
+        default: down_v<PRE, 1, 4>(F, C, xout, x_zero, sms, min_seg, st); break;
         }
     }
 }
 
 template <int POST, class T>
 void up_t(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, T* xout, double omega,
-          int sms, cudaStream_t st) {
+          int sms, int min_seg, cudaStream_t st) {
     if constexpr (sizeof(T) == 8) {
         switch (mg_variant64()) {
-        case 1: up_v<POST, 1, 3>(C, F, xin, xout, omega, sms, st); break;
-        case 2: up_v<POST, 1, 4>(C, F, xin, xout, omega, sms, st); break;
-        default: up_v<POST, 2, 2>(C, F, xin, xout, omega, sms, st); break;
+        case 1: up_v<POST, 1, 3>(C, F, xin, xout, omega, sms, min_seg, st); break;
+        case 2: up_v<POST, 1, 4>(C, F, xin, xout, omega, sms, min_seg, st); break;
+        default: up_v<POST, 2, 2>(C, F, xin, xout, omega, sms, min_seg, st); break;
         }
     } else {
         switch (mg_variant()) {
-        case 0: up_v<POST, 3, 2>(C, F, xin, xout, omega, sms, st); break;
-        case 1: up_v<POST, 2, 3>(C, F, xin, xout, omega, sms, st); break;
-        case 3: up_v<POST, 1, 5>(C, F, xin, xout, omega, sms, st); break;
-        case 4: up_v<POST, 1, 6>(C, F, xin, xout, omega, sms, st); break;
-        default: up_v<POST, 1, 4>(C, F, xin, xout, omega, sms, st); break;
+        case 0: up_v<POST, 3, 2>(C, F, xin, xout, omega, sms, min_seg, st); break;
+        case 1: up_v<POST, 2, 3>(C, F, xin, xout, omega, sms, min_seg, st); break;
+        case 3: up_v<POST, 1, 5>(C, F, xin, xout, omega, sms, min_seg, st); break;
+        case 4: up_v<POST, 1, 6>(C, F, xin, xout, omega, sms, min_seg, st); break;
+        default: up_v<POST, 1, 4>(C, F, xin, xout, omega, sms, min_seg, st); break;
         }
     }
 }
@@ -388,25 +393,25 @@ bool mg_fast_supported(int pre, int post) { return pre >= 1 && pre <= 4 && post 
 
 template <class T>
 void launch_mg_down(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, int pre, bool x_zero,
-                    int sms, cudaStream_t st) {
+                    int sms, int min_seg, cudaStream_t st) {
     switch (pre) {
-    case 1: down_t<1>(F, C, xout, x_zero, sms, st); break;
-    case 2: down_t<2>(F, C, xout, x_zero, sms, st); break;
-    case 3: down_t<3>(F, C, xout, x_zero, sms, st); break;
-    case 4: down_t<4>(F, C, xout, x_zero, sms, st); break;
+    case 1: down_t<1>(F, C, xout, x_zero, sms, min_seg, st); break;
+    case 2: down_t<2>(F, C, xout, x_zero, sms, min_seg, st); break;
+    case 3: down_t<3>(F, C, xout, x_zero, sms, min_seg, st); break;
+    case 4: down_t<4>(F, C, xout, x_zero, sms, min_seg, st); break;
     default: throw Error(SGPU_E_INVALID, "streaming multigrid supports mg_pre 1..4");
     }
 }
 
 template <class T>
 void launch_mg_up(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, T* xout,
-                  double omega, int post, int sms, cudaStream_t st) {
+                  double omega, int post, int sms, int min_seg, cudaStream_t st) {
     switch (post) {
-    case 0: up_t<0>(C, F, xin, xout, omega, sms, st); break;
-    case 1: up_t<1>(C, F, xin, xout, omega, sms, st); break;
-    case 2: up_t<2>(C, F, xin, xout, omega, sms, st); break;
-    case 3: up_t<3>(C, F, xin, xout, omega, sms, st); break;
-    case 4: up_t<4>(C, F, xin, xout, omega, sms, st); break;
+    case 0: up_t<0>(C, F, xin, xout, omega, sms, min_seg, st); break;
+    case 1: up_t<1>(C, F, xin, xout, omega, sms, min_seg, st); break;
+    case 2: up_t<2>(C, F, xin, xout, omega, sms, min_seg, st); break;
+    case 3: up_t<3>(C, F, xin, xout, omega, sms, min_seg, st); break;
+    case 4: up_t<4>(C, F, xin, xout, omega, sms, min_seg, st); break;
     default: throw Error(SGPU_E_INVALID, "streaming multigrid supports mg_post 0..4");
     }
 }
@@ -415,14 +420,14 @@ void launch_mg_up(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, 
 // bits); mg_fast32.cu includes it with SGPU_FLOAT_UNIT for the float ones (contraction allowed).
 #ifndef SGPU_FLOAT_UNIT
 template void launch_mg_down<double>(const LevelViewT<double>&, const LevelViewT<double>&, double*,
-                                     int, bool, int, cudaStream_t);
+                                     int, bool, int, int, cudaStream_t);
 template void launch_mg_up<double>(const LevelViewT<double>&, const LevelViewT<double>&,
-                                   const double*, double*, double, int, int, cudaStream_t);
+                                   const double*, double*, double, int, int, int, cudaStream_t);
 #else
 template void launch_mg_down<float>(const LevelViewT<float>&, const LevelViewT<float>&, float*, int,
-                                    bool, int, cudaStream_t);
+                                    bool, int, int, cudaStream_t);
 template void launch_mg_up<float>(const LevelViewT<float>&, const LevelViewT<float>&, const float*,
-                                  float*, double, int, int, cudaStream_t);
+                                  float*, double, int, int, int, cudaStream_t);
 #endif
 
 } // namespace sgpu

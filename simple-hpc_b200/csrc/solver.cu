@@ -111,6 +111,15 @@ struct Solver {
     double* tmp = nullptr;
     int sms = 148;
     int seg_rows = 64;
+    // Minimum rows per CTA segment of the streaming kernels. A single solve owns the GPU and is
+    // bound by each CTA's per-step latency on small grids, so it takes short segments (8 rows); a
+    // batch fills the GPU with many cavities and keeps the kernels' defaults (0), which bound the
+    // halo and skew work per row (use_batch_shape).
+    int min_seg = 8;
+    void use_batch_shape() {
+        min_seg = 0;
+        if (fast) seg_rows = stream_seg_rows(dp, sms, mixed ? corr_blocks_per_sm(dp.ncol) : 2, 0);
+    }
 
     int ncol = 5;
     IterGraph* run_graph = nullptr; // sgpu_run's graph (built on first use)
@@ -386,12 +395,13 @@ struct Solver {
         const bool guess = apply_warm_start(L0);
         auto vcycle32 = [&](bool x_zero) {
             for (int l = 0; l < mg_tail; ++l)
-                launch_mg_down<float>(lv32[l], lv32[l + 1], mg32_x2[l], prm.mg_pre, x_zero || l > 0, sms, st);
+                launch_mg_down<float>(lv32[l], lv32[l + 1], mg32_x2[l], prm.mg_pre, x_zero || l > 0, sms,
+                                      min_seg, st);
             launch_mg_tail<float>(mgl32, mg_tail, prm.mg_pre, prm.mg_post, prm.mg_omega, kCoarseTol32,
                                   coarse_rowbuf, stats, st);
             for (int l = mg_tail - 1; l >= 0; --l)
                 launch_mg_up<float>(lv32[l + 1], lv32[l], mg32_x2[l], lv32[l].x, prm.mg_omega,
-                                    prm.mg_post, sms, st);
+                                    prm.mg_post, sms, min_seg, st);
         };
         last_vcycles = run_cycles(L0, !guess, vcycle32);
         launch_ordered_sum(L0.x, 0, L0.stride, L0.nx, L0.ny, 1, sums + 26, ss, nullptr, st);
@@ -567,7 +577,7 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
         int dev = 0;
         SGPU_CUDA(cudaGetDevice(&dev));
         SGPU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        seg_rows = stream_seg_rows(dp, sms);
+        seg_rows = stream_seg_rows(dp, sms, 2, min_seg);
         if (const char* e = std::getenv("SGPU_SIDE_SUMS")) side_sums = std::atoi(e) != 0;
         SGPU_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
         for (int k = 0; k < 2; ++k) {
@@ -669,7 +679,7 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
                         "mg and 1 <= mg_pre <= 4, 0 <= mg_post <= 4");
         mixed = true;
         init_mixed_kernels();
-        seg_rows = stream_seg_rows(dp, sms, corr_blocks_per_sm(dp.ncol));
+        seg_rows = stream_seg_rows(dp, sms, corr_blocks_per_sm(dp.ncol), min_seg);
         rec32.near_links = dalloc<float4>(g.elems());
         rec32.far_links = dalloc<float4>(g.elems());
         rec32.diag = dalloc<float2>(g.elems());
@@ -897,11 +907,11 @@ template <class T> void Solver::sample_pair(std::vector<LevelViewT<T>>& L, float
 void Solver::mg_vcycle_fast(bool x_is_zero) {
     const int nl = static_cast<int>(lv.size());
     for (int l = 0; l < mg_tail; ++l)
-        launch_mg_down(lv[l], lv[l + 1], mg_x2[l], prm.mg_pre, x_is_zero || l > 0, sms, st);
+        launch_mg_down(lv[l], lv[l + 1], mg_x2[l], prm.mg_pre, x_is_zero || l > 0, sms, min_seg, st);
     launch_mg_tail(mgl, mg_tail, prm.mg_pre, prm.mg_post, prm.mg_omega, kCoarseTol64, coarse_rowbuf,
                    stats, st);
     for (int l = mg_tail - 1; l >= 0; --l)
-        launch_mg_up(lv[l + 1], lv[l], mg_x2[l], lv[l].x, prm.mg_omega, prm.mg_post, sms, st);
+        launch_mg_up(lv[l + 1], lv[l], mg_x2[l], lv[l].x, prm.mg_omega, prm.mg_post, sms, min_seg, st);
     (void)nl;
 }
 
@@ -1757,6 +1767,7 @@ int sgpu_batch_create(const sgpu_params_t* params, int count, sgpu_batch** out) 
             if (p.warm_start)
                 throw sgpu::Error(SGPU_E_INVALID, who + "warm_start = cnn is not supported in a batch");
             b->s.push_back(std::make_unique<sgpu::Solver>(p, nullptr, nullptr, nullptr));
+            b->s.back()->use_batch_shape();
         }
         SGPU_CUDA(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
         b->seg_tuned.assign(count, 0);

@@ -434,7 +434,7 @@ __global__ void k_assemble_p(DevParams p, const double* __restrict__ APU,
     const double b = -dx * (-v[q + ld] + v[q]) - dy * (-u[q - 1] + u[q]);
     w.b[q] = b;
     const std::size_t c = static_cast<std::size_t>(i - H) * p.NY + (j - H - 1);
-    cabs[c] = fabs(b);
+    if (cabs) cabs[c] = fabs(b);
     if (cb) cb[c] = b;
 }
 

@@ -25,6 +25,10 @@ void launch_ordered_sum(const double* vals, std::size_t plane_stride, int ld, in
 // alone, but it can run on a second stream beside a kernel whose grid fills the SMs.
 void launch_ordered_sum_lean(const double* vals, int ld, int nr, int nc, double* out, const SumScratch& s,
                              cudaStream_t st);
+// Two sums of one plane in one pass: out[0] = sum of |v|, out[1] = sum of v, each in the order above
+// (res_p and the mean of b from the field b itself, without compact copies).
+void launch_ordered_sum_abs_pair(const double* vals, int ld, int nr, int nc, double* out, const SumScratch& s,
+                                 cudaStream_t st);
 // The same order over FP32 values, each widened to double before it is added.
 void launch_ordered_sum(const float* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
                         double* out, const SumScratch& s, const int* skip, cudaStream_t st);
@@ -163,6 +167,9 @@ void launch_assemble_p_mixed(const DevParams& p, const double* APU, const double
                              const LevelView32& L0, double* cabs, double* cb, cudaStream_t st);
 void launch_b_to_f32(const DevParams& p, const double* bfield, const double* sum_b,
                      const LevelView32& L0, cudaStream_t st);
+// pc64 = FP32 p' minus its FP64 mean over the p' cells (the field correct_mixed applied).
+void launch_pc_from32(const DevParams& p, const LevelView32& L0, const double* sum_pc, double* pc64,
+                      cudaStream_t st);
 void launch_correct_mixed(const DevParams& p, const LevelView32& L0, const double* sum_pc,
                           const double* APU, const double* APV, double* u, double* v, double* pf,
                           double* pc64, cudaStream_t st);

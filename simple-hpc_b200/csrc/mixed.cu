@@ -255,8 +255,8 @@ __global__ void k_assemble_p_mixed(DevParams p, const double* __restrict__ APU,
     const double b = -dx * (-v[q + ld] + v[q]) - dy * (-u[q - 1] + u[q]);
     bfield[q] = b;
     const std::size_t c = static_cast<std::size_t>(I) * p.NY + J;
-    cabs[c] = fabs(b);
-    cb[c] = b;
+    if (cabs) cabs[c] = fabs(b);
+    if (cb) cb[c] = b;
 }
 
 // b32 = b - mean(b), rounded to FP32 (remove_mean0, multigrid.cpp:327-345, in FP64 first).
@@ -292,7 +292,17 @@ __global__ void k_correct_mixed(DevParams p, const float* __restrict__ pc32, int
         v[q] += p.dx * (pc - pcn) / APV[q];
     }
     pf[q] += p.ap * pc;
-    pc64[q] = pc;
+    if (pc64) pc64[q] = pc;
+}
+
+// The FP64 p' field as k_correct_mixed uses it (FP32 p' minus its FP64 mean), for a download.
+__global__ void k_pc_from32(DevParams p, const float* __restrict__ pc32, int ld32,
+                            const double* __restrict__ sum_pc, double* __restrict__ pc64) {
+    const int J = static_cast<int>(blockIdx.x * 32 + threadIdx.x);
+    const int I = static_cast<int>(blockIdx.y * 8 + threadIdx.y);
+    if (I >= p.NX || J >= p.NY) return;
+    const double m = *sum_pc / (static_cast<double>(p.NX) * p.NY);
+    pc64[ix(p, p.H + I, p.H + 1 + J)] = static_cast<double>(pc32[I * ld32 + J]) - m;
 }
 
 Range update_range(const DevParams& p, bool v) {
@@ -364,6 +374,13 @@ void launch_b_to_f32(const DevParams& p, const double* bfield, const double* sum
                      const LevelView32& L0, cudaStream_t st) {
     const dim3 grid((p.NY + 31) / 32, (p.NX + 7) / 8);
     k_b_to_f32<<<grid, dim3(32, 8), 0, st>>>(p, bfield, sum_b, L0);
+    SGPU_LAUNCH();
+}
+
+void launch_pc_from32(const DevParams& p, const LevelView32& L0, const double* sum_pc, double* pc64,
+                      cudaStream_t st) {
+    const dim3 grid((p.NY + 31) / 32, (p.NX + 7) / 8);
+    k_pc_from32<<<grid, dim3(32, 8), 0, st>>>(p, L0.x, L0.stride, sum_pc, pc64);
     SGPU_LAUNCH();
 }
 

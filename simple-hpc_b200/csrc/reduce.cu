@@ -36,8 +36,9 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// One warp per CTA (32 rows); the grid covers ceil(nr / 32) x K planes.
-template <class TIn, int STAGES>
+// One warp per CTA (32 rows); the grid covers ceil(nr / 32) x K planes. PAIR: one plane, two sums
+// in one pass (out[0] = sum of |v|, out[1] = sum of v, each in the same order).
+template <class TIn, int STAGES, bool PAIR>
 __global__ void __launch_bounds__(32)
     k_ordered_sum(const TIn* __restrict__ vals, std::size_t plane_stride, int ld, int nr, int nc,
                   double* __restrict__ rows, unsigned int* counter, double* __restrict__ out,
@@ -65,7 +66,8 @@ __global__ void __launch_bounds__(32)
     };
     for (int k = 0; k < STAGES - 1; ++k) issue(k);
 
-    double s = 0.0; // this lane's row: r0 + lane
+    double s = 0.0;  // this lane's row: r0 + lane
+    double sa = 0.0; // PAIR: the sum of |v| of the same row
     for (int k = 0; k < ntiles; ++k) {
         issue(k + STAGES - 1);
         cp_async_wait<STAGES - 1>(); // tile k has landed (this lane's copies)
@@ -77,14 +79,28 @@ __global__ void __launch_bounds__(32)
 #pragma unroll
             for (int c = 0; c < kTile; ++c) v[c] = static_cast<double>(t[c]); // loads first
 #pragma unroll
-            for (int c = 0; c < kTile; ++c) s += v[c];
+            for (int c = 0; c < kTile; ++c) {
+                s += v[c];
+                if (PAIR) sa += fabs(v[c]);
+            }
         } else {
-            for (int c = 0; c < cnt; ++c) s += static_cast<double>(t[c]);
+            for (int c = 0; c < cnt; ++c) {
+                const double x = static_cast<double>(t[c]);
+                s += x;
+                if (PAIR) sa += fabs(x);
+            }
         }
         __syncwarp(); // the slot is refilled by the next issue
     }
     cp_async_wait<0>();
-    if (lane < nrow) rows[static_cast<std::size_t>(m) * nr + r0 + lane] = s;
+    if (lane < nrow) {
+        if (PAIR) {
+            rows[r0 + lane] = sa;
+            rows[static_cast<std::size_t>(nr) + r0 + lane] = s;
+        } else {
+            rows[static_cast<std::size_t>(m) * nr + r0 + lane] = s;
+        }
+    }
 
     // The last CTA to finish adds every plane's row sums in row order.
     __threadfence();
@@ -99,7 +115,7 @@ __global__ void __launch_bounds__(32)
     // The chain over the rows is serial, so it must not wait on L2 for each term: the warp stages
     // chunks of every plane's row sums in shared memory (the tile ring is free now; many
     // independent loads per lane in flight), then lane m adds plane m's chunk from registers.
-    const int K = static_cast<int>(gridDim.y);
+    const int K = PAIR ? 2 : static_cast<int>(gridDim.y);
     double* buf = reinterpret_cast<double*>(tile_raw);
     const int cs = chunk + 1; // plane stride in buf: lanes reading one row index hit distinct banks
     double acc = 0.0;
@@ -129,26 +145,27 @@ __global__ void __launch_bounds__(32)
     if (lane == 0) *counter = 0u; // ready for the next launch on this stream
 }
 
-template <class TIn, int STAGES>
+template <class TIn, int STAGES, bool PAIR = false>
 void launch_sum(const TIn* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
                 double* out, const SumScratch& s, const int* skip, cudaStream_t st) {
-    if (K < 1 || K > 32 || K > s.max_k || nr > s.max_rows)
+    const int kout = PAIR ? 2 : K;
+    if (K < 1 || K > 32 || kout > s.max_k || nr > s.max_rows || (PAIR && K != 1))
         throw Error(SGPU_E_INVALID, "ordered sum: sizes exceed the scratch");
     if (nr <= 0) {
-        SGPU_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * K, st));
+        SGPU_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * kout, st));
         return;
     }
     const dim3 grid((nr + kTile - 1) / kTile, K);
     constexpr int smem = STAGES * kTile * kPitch * static_cast<int>(sizeof(TIn));
     static bool attr = false; // per process
     if (!attr) {
-        SGPU_CUDA(cudaFuncSetAttribute(k_ordered_sum<TIn, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        SGPU_CUDA(cudaFuncSetAttribute(k_ordered_sum<TIn, STAGES, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         attr = true;
     }
     // Rows per staged chunk of the final pass: K planes of (chunk + 1) doubles fit the tile ring.
-    const int chunk = std::min(2048, (smem / (static_cast<int>(sizeof(double)) * K) - 1) / kTile * kTile);
-    k_ordered_sum<TIn, STAGES><<<grid, 32, smem, st>>>(vals, plane_stride, ld, nr, nc, s.rows, s.counter, out,
-                                                        skip, chunk);
+    const int chunk = std::min(2048, (smem / (static_cast<int>(sizeof(double)) * kout) - 1) / kTile * kTile);
+    k_ordered_sum<TIn, STAGES, PAIR><<<grid, 32, smem, st>>>(vals, plane_stride, ld, nr, nc, s.rows, s.counter,
+                                                              out, skip, chunk);
     SGPU_LAUNCH();
 }
 
@@ -162,6 +179,11 @@ void launch_ordered_sum(const double* vals, std::size_t plane_stride, int ld, in
 void launch_ordered_sum(const float* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
                         double* out, const SumScratch& s, const int* skip, cudaStream_t st) {
     launch_sum<float, kStages>(vals, plane_stride, ld, nr, nc, K, out, s, skip, st);
+}
+
+void launch_ordered_sum_abs_pair(const double* vals, int ld, int nr, int nc, double* out, const SumScratch& s,
+                                 cudaStream_t st) {
+    launch_sum<double, kStages, true>(vals, 0, ld, nr, nc, 1, out, s, nullptr, st);
 }
 
 void launch_ordered_sum_lean(const double* vals, int ld, int nr, int nc, double* out, const SumScratch& s,

@@ -182,6 +182,8 @@ struct Solver {
         default: return nullptr;
         }
     }
+    // Offset of the first p' cell (H, H + 1) in a full-grid array.
+    std::size_t p_origin() const { return static_cast<std::size_t>(prm.H) * g.pitch + prm.H + 1; }
     double* at(double* f, int i, int j) const {
         return f + static_cast<std::size_t>(i) * g.pitch + j;
     }
@@ -274,8 +276,9 @@ struct Solver {
         fast_momentum(true, res3 + 1);
         join_sums();
         mark(SGPU_PH_ASSEMBLE_P);
-        launch_assemble_p_fused(dp, cu.a[8], cv.a[8], u, v, w, cells, nullptr, st);
-        launch_ordered_sum(cells, 0, prm.NY, prm.NX, prm.NY, 1, res3 + 2, ss, nullptr, st);
+        launch_assemble_p_fused(dp, cu.a[8], cv.a[8], u, v, w, nullptr, nullptr, st);
+        // res_p = the ordered sum of |b| over the p' cells, read from b itself (res3[3] gets the sum of b)
+        launch_ordered_sum_abs_pair(w.b + p_origin(), g.pitch, prm.NX, prm.NY, res3 + 2, ss, st);
         mark(SGPU_PH_SOLVE_P);
         solve_p();
         mark(SGPU_PH_CORRECT);
@@ -342,7 +345,13 @@ struct Solver {
     // The mixed iteration keeps the p' operator in FP32 only; the FP64 links and APP are formed from
     // APU / APV when a caller downloads one of them.
     bool p_links_stale = false;
+    bool pc_stale = false; // the mixed iteration keeps p' in FP32; the FP64 field is formed on download
     void form_p_links_if_stale(int id) {
+        if (pc_stale && id == SGPU_F_PC) { // p' of the last mixed iteration, kept in FP32
+            launch_pc_from32(dp, lv32[0], sums + 26, w.pc, st);
+            pc_stale = false;
+            return;
+        }
         if (!p_links_stale || id < SGPU_F_AEP || id > SGPU_F_APP) return;
         launch_p_links_app(dp, cu.a[8], cv.a[8], w, st);
         p_links_stale = false;
@@ -379,12 +388,14 @@ struct Solver {
 
     void mixed_iteration_enqueue(double* res3) {
         p_links_stale = true;
+        pc_stale = true;
         mixed_momentum(false, res3 + 0);
         mixed_momentum(true, res3 + 1);
         join_sums();
         mark(SGPU_PH_ASSEMBLE_P);
-        launch_assemble_p_mixed(dp, cu.a[8], cv.a[8], u, v, w.b, lv32[0], cells, cells + plane, st);
-        launch_ordered_sum(cells, plane, prm.NY, prm.NX, prm.NY, 2, sums + 24, ss, nullptr, st);
+        launch_assemble_p_mixed(dp, cu.a[8], cv.a[8], u, v, w.b, lv32[0], nullptr, nullptr, st);
+        // sum of |b| (res_p) and sum of b (its mean) in one pass over b
+        launch_ordered_sum_abs_pair(w.b + p_origin(), g.pitch, prm.NX, prm.NY, sums + 24, ss, st);
         SGPU_CUDA(cudaMemcpyAsync(res3 + 2, sums + 24, sizeof(double), cudaMemcpyDeviceToDevice, st));
         mark(SGPU_PH_SOLVE_P);
         for (std::size_t l = 1; l < lv32.size(); ++l) launch_mg_build<float>(lv32[l - 1], lv32[l], st);
@@ -406,7 +417,7 @@ struct Solver {
         last_vcycles = run_cycles(L0, !guess, vcycle32);
         launch_ordered_sum(L0.x, 0, L0.stride, L0.nx, L0.ny, 1, sums + 26, ss, nullptr, st);
         mark(SGPU_PH_CORRECT);
-        launch_correct_mixed(dp, L0, sums + 26, cu.a[8], cv.a[8], u, v, pf, w.pc, st);
+        launch_correct_mixed(dp, L0, sums + 26, cu.a[8], cv.a[8], u, v, pf, nullptr, st);
         mark(SGPU_PH_COUNT);
     }
 
@@ -916,6 +927,7 @@ void Solver::mg_vcycle_fast(bool x_is_zero) {
 }
 
 void Solver::solve_p() {
+    pc_stale = false; // the FP64 p' field is written by this solve
     switch (prm.pressure_solver) {
     case SGPU_P_JACOBI: solve_jacobi(); break;
     case SGPU_P_GS_REDBLACK: solve_redblack(); break;

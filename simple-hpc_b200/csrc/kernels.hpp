@@ -157,11 +157,10 @@ void launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x
                            const double* pf, double* AP, double* cells, MomRec32 rec,
                            cudaStream_t st);
 // One FP32 multicolour correction sweep e_in -> e_out (e_zero: e_in is zero and not read).
+// xfinal != null: the last sweep of a component adds e to the FP64 field x over the update range
+// (x += e in FP64) instead of writing eout.
 void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, float* eout,
-                       MomRec32 rec, bool e_zero, int seg_rows, cudaStream_t st);
-// x += e over the component's update range.
-void launch_add_correction(const DevParams& p, bool v_component, double* x, const float* e,
-                           cudaStream_t st);
+                       MomRec32 rec, bool e_zero, int seg_rows, cudaStream_t st, double* xfinal = nullptr);
 void launch_assemble_p_mixed(const DevParams& p, const double* APU, const double* APV,
                              const double* u, const double* v, double* bfield,
                              const LevelView32& L0, double* cabs, double* cb, cudaStream_t st);

@@ -94,7 +94,7 @@ struct Rec {
 template <int NCOL, bool V, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     k_corr_stream(DevParams p, const float* __restrict__ ein, float* __restrict__ eout,
-                  MomRec32 rec, int e_zero, int seg_rows) {
+                  MomRec32 rec, int e_zero, int seg_rows, double* __restrict__ xfinal) {
     constexpr int SPB = NCOL == 5 ? 2 : 1;
     constexpr int HC = 2 * NCOL;
     constexpr int W = NT - 2 * HC;
@@ -112,6 +112,9 @@ __global__ void __launch_bounds__(NT, MINB)
     const int ld = p.pitch;
     const bool col_in = col >= 0 && col < p.ncols;
     const bool col_out = col_in && col >= j0 && col < j0 + W;
+    // the update range (xfinal: the last sweep adds e to the FP64 field there, x += e)
+    const int ui0 = V ? p.H + 1 : p.H, ui1 = p.NX + p.H - 1;
+    const int uj0 = p.H + 1, uj1 = V ? p.NY + p.H : p.NY + p.H - 1;
     const int H = p.H;
     if (tid < NCOL) {
         const int c = tid;
@@ -208,7 +211,12 @@ __global__ void __launch_bounds__(NT, MINB)
 #pragma unroll
         for (int s = 0; s < SPB; ++s) {
             const int rw = t - 2 * NCOL + 1 - (SPB - 1) + s;
-            if (rw >= R0 && rw < R1 && col_out) eout[col + rw * ld] = ringc[(rw & (kRing - 1)) * NT];
+            if (rw >= R0 && rw < R1 && col_out) {
+                const float ev = ringc[(rw & (kRing - 1)) * NT];
+                if (!xfinal) eout[col + rw * ld] = ev;
+                else if (rw >= ui0 && rw <= ui1 && col >= uj0 && col <= uj1) // the last sweep: x += e
+                    xfinal[static_cast<std::size_t>(rw) * ld + col] += static_cast<double>(ev);
+            }
         }
         return cn;
     };
@@ -218,16 +226,6 @@ __global__ void __launch_bounds__(NT, MINB)
         if (t + SPB <= t_last) c0 = super_step(t + SPB, c0, bufB, rB, okB, bufA, rA, okA);
     }
     cp_async_wait<0>();
-}
-
-// x += e over the update range (the FP64 field update).
-__global__ void k_add_correction(DevParams p, double* __restrict__ x, const float* __restrict__ e,
-                                 Range ur) {
-    const int j = ur.j0 + static_cast<int>(blockIdx.x * 32 + threadIdx.x);
-    const int i = ur.i0 + static_cast<int>(blockIdx.y * 8 + threadIdx.y);
-    if (i > ur.i1 || j > ur.j1) return;
-    const std::size_t q = ix(p, i, j);
-    x[q] += static_cast<double>(e[q]);
 }
 
 // assemble_p (pressure.cpp:14-54) in FP64 with the p' operator stored in FP32 (level 0 of the FP32
@@ -322,19 +320,20 @@ int corr_minb() {
 
 template <int NCOL, bool V, int NT, int MINB>
 void launch_corr(const DevParams& p, const float* ein, float* eout, MomRec32 rec, bool e_zero,
-                 int seg_rows, cudaStream_t st) {
+                 int seg_rows, double* xfinal, cudaStream_t st) {
     constexpr int W = NT - 4 * NCOL;
     const dim3 grid((p.ncols + W - 1) / W, (p.nrows + seg_rows - 1) / seg_rows);
     constexpr int smem = kRing * NT * static_cast<int>(sizeof(float));
-    k_corr_stream<NCOL, V, NT, MINB><<<grid, NT, smem, st>>>(p, ein, eout, rec, e_zero ? 1 : 0, seg_rows);
+    k_corr_stream<NCOL, V, NT, MINB><<<grid, NT, smem, st>>>(p, ein, eout, rec, e_zero ? 1 : 0, seg_rows,
+                                                              xfinal);
     SGPU_LAUNCH();
 }
 
 template <int NCOL, bool V>
 void launch_corr_m(const DevParams& p, const float* ein, float* eout, MomRec32 rec, bool e_zero,
-                   int seg_rows, cudaStream_t st) {
-    if (corr_minb() == 4) launch_corr<NCOL, V, 256, 4>(p, ein, eout, rec, e_zero, seg_rows, st);
-    else launch_corr<NCOL, V, 256, 3>(p, ein, eout, rec, e_zero, seg_rows, st);
+                   int seg_rows, double* xfinal, cudaStream_t st) {
+    if (corr_minb() == 4) launch_corr<NCOL, V, 256, 4>(p, ein, eout, rec, e_zero, seg_rows, xfinal, st);
+    else launch_corr<NCOL, V, 256, 3>(p, ein, eout, rec, e_zero, seg_rows, xfinal, st);
 }
 
 } // namespace
@@ -350,15 +349,6 @@ void launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x
     const dim3 grid((ur.cols() + 31) / 32, (ur.rows() + 7) / 8);
     if (v_component) k_mom_prep_mixed<true><<<grid, dim3(32, 8), 0, st>>>(p, x, oth, pf, AP, cells, rec, ur);
     else k_mom_prep_mixed<false><<<grid, dim3(32, 8), 0, st>>>(p, x, oth, pf, AP, cells, rec, ur);
-    SGPU_LAUNCH();
-}
-
-void launch_add_correction(const DevParams& p, bool v_component, double* x, const float* e,
-                           cudaStream_t st) {
-    const Range ur = update_range(p, v_component);
-    if (ur.rows() <= 0 || ur.cols() <= 0) return;
-    const dim3 grid((ur.cols() + 31) / 32, (ur.rows() + 7) / 8);
-    k_add_correction<<<grid, dim3(32, 8), 0, st>>>(p, x, e, ur);
     SGPU_LAUNCH();
 }
 
@@ -394,13 +384,13 @@ void launch_correct_mixed(const DevParams& p, const LevelView32& L0, const doubl
 
 #else
 void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, float* eout,
-                       MomRec32 rec, bool e_zero, int seg_rows, cudaStream_t st) {
+                       MomRec32 rec, bool e_zero, int seg_rows, cudaStream_t st, double* xfinal) {
     if (p.ncol == 5) {
-        if (v_component) launch_corr_m<5, true>(p, ein, eout, rec, e_zero, seg_rows, st);
-        else launch_corr_m<5, false>(p, ein, eout, rec, e_zero, seg_rows, st);
+        if (v_component) launch_corr_m<5, true>(p, ein, eout, rec, e_zero, seg_rows, xfinal, st);
+        else launch_corr_m<5, false>(p, ein, eout, rec, e_zero, seg_rows, xfinal, st);
     } else {
-        if (v_component) launch_corr_m<2, true>(p, ein, eout, rec, e_zero, seg_rows, st);
-        else launch_corr_m<2, false>(p, ein, eout, rec, e_zero, seg_rows, st);
+        if (v_component) launch_corr_m<2, true>(p, ein, eout, rec, e_zero, seg_rows, xfinal, st);
+        else launch_corr_m<2, false>(p, ein, eout, rec, e_zero, seg_rows, xfinal, st);
     }
 }
 

@@ -379,11 +379,11 @@ struct Solver {
         int cur = 0; // e32[cur] holds the current correction (zero before the first sweep)
         sweep_mark(vcomp, 0, n);
         for (int k = 0; k < n; ++k) {
-            launch_corr_sweep(dp, vcomp, e32[cur], e32[1 - cur], rec32, k == 0, seg_rows, st);
+            launch_corr_sweep(dp, vcomp, e32[cur], e32[1 - cur], rec32, k == 0, seg_rows, st,
+                              k == n - 1 ? x : nullptr); // the last sweep adds e into x
             cur = 1 - cur;
         }
         sweep_mark(vcomp, 1, n);
-        if (n > 0) launch_add_correction(dp, vcomp, x, e32[cur], st);
     }
 
     void mixed_iteration_enqueue(double* res3) {

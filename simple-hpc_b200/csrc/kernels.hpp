@@ -33,6 +33,17 @@ void launch_ordered_sum_abs_pair(const double* vals, int ld, int nr, int nc, dou
 void launch_ordered_sum(const float* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
                         double* out, const SumScratch& s, const int* skip, cudaStream_t st);
 
+// Deterministic FP64 tree sums (the mixed-precision path, which is not tied to the reference's
+// rounding): a fixed shuffle tree per block, the blocks' partial sums added by one CTA in a fixed
+// order. The same inputs and sizes give the same bits on every run.
+// out0 = the sum of part[0 .. n), and for K = 2 also out1 = the sum of part[plane .. plane + n).
+void launch_sum_partials(const double* part, int n, int K, int plane, double* out0, double* out1,
+                         cudaStream_t st);
+// *out = the sum of an nr x nc FP32 array (row stride ld) in FP64; part holds tree_sum_partials(nr,
+// nc) doubles of scratch.
+int tree_sum_partials(int nr, int nc);
+void launch_tree_sum(const float* vals, int ld, int nr, int nc, double* part, double* out, cudaStream_t st);
+
 // ---- momentum and pressure phases, reference-shaped (phases.cu) ----
 struct Coef9Ptr {
     double* a[9]; // AE AW AN AS AEE AWW ANN ASS AP
@@ -152,18 +163,22 @@ struct MomRec32 {
     float4* far_links;
     float2* diag;
 };
-// FP64 prep: |R| into cells, AP (FP64), and the cell's FP32 record, over the update range.
-void launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x, const double* oth,
-                           const double* pf, double* AP, double* cells, MomRec32 rec,
-                           cudaStream_t st);
+// FP64 prep over the update range: AP (FP64), the cell's FP32 record, and one partial sum of |R|
+// per block into part; returns the number of partial sums (for launch_sum_partials).
+int launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x, const double* oth,
+                          const double* pf, double* AP, double* part, MomRec32 rec, cudaStream_t st);
 // One FP32 multicolour correction sweep e_in -> e_out (e_zero: e_in is zero and not read).
 // xfinal != null: the last sweep of a component adds e to the FP64 field x over the update range
 // (x += e in FP64) instead of writing eout.
 void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, float* eout,
                        MomRec32 rec, bool e_zero, int seg_rows, cudaStream_t st, double* xfinal = nullptr);
-void launch_assemble_p_mixed(const DevParams& p, const double* APU, const double* APV,
-                             const double* u, const double* v, double* bfield,
-                             const LevelView32& L0, double* cabs, double* cb, cudaStream_t st);
+// assemble_p with the FP32 level-0 operator; per block one partial sum of |b| into part[k] and one
+// of b into part[n + k] (n = the returned number of blocks).
+int launch_assemble_p_mixed(const DevParams& p, const double* APU, const double* APV, const double* u,
+                            const double* v, double* bfield, const LevelView32& L0, double* part,
+                            cudaStream_t st);
+// Doubles of partial-sum scratch the two launchers above need at most.
+int mixed_partials(const DevParams& p);
 void launch_b_to_f32(const DevParams& p, const double* bfield, const double* sum_b,
                      const LevelView32& L0, cudaStream_t st);
 // pc64 = FP32 p' minus its FP64 mean over the p' cells (the field correct_mixed applied).

@@ -3,20 +3,22 @@
 // Defect correction around FP32 inner solves; everything SIMPLE's stability and stopping test
 // depend on stays FP64:
 //  * Momentum. The FP64 prep pass computes each cell's coefficients and the residual
-//    R = nb(u) + pressure term - AP u exactly as the FP64 path does (momentum_u.cpp:43-59), so
-//    res_u / res_v and their ordered sums are FP64. It also stores, per cell, a 40-byte FP32
+//    R = nb(u) + pressure term - AP u exactly as the FP64 path does (momentum_u.cpp:43-59), and
+//    sums |R| into res_u / res_v in FP64 (a fixed tree, not the reference's row-by-row chain: the
+//    same value to rounding, and no serial pass over the cells). It also stores, per cell, a 40-byte FP32
 //    record in three arrays: the 8 neighbour coefficients, 1/AP and R. The maxit_inner
 //    multicolour sweeps then run on the correction e = u_new - u in FP32: the reference's update
 //    u <- a (nb(u) + pt) / AP + (1 - a) u (momentum_u.cpp:136-137) is, for u = u0 + e, exactly
 //    e <- e + a ((R(u0) + nb(e)) / AP - e), applied in the same colour order by the same
 //    time-skewed streaming scheme as the FP64 sweep. The field update u += e is FP64.
 //  * Pressure correction. assemble_p (pressure.cpp:14-54) stays FP64 for b, its |b| sum (res_p)
-//    and its mean; the p' system's operator is stored in FP32 and solved by the FP32 V-cycle
+//    and its mean (FP64 trees as above); the p' system's operator is stored in FP32 and solved by the FP32 V-cycle
 //    (mg_fast.cu / mg.cu, float instantiation). The mean of p' and the velocity / pressure
 //    correction (pressure.cpp:136-157) are FP64.
 // Fixed points are those of the FP64 iteration: when R and the continuity residual vanish, e and
 // p' vanish too, whatever their precision.
 #include "kernels.hpp"
+#include "blocksum.cuh"
 #include "stencil.cuh"
 
 #include <cstdlib>
@@ -41,16 +43,11 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// FP64 prep over the update range: |R| for the ordered residual sum, AP (FP64, for assemble_p and
-// correct), and the cell's FP32 record {AE AW AN AS | AEE AWW ANN ASS | 1/AP R 0 0}.
+// One cell of the prep; returns |R|.
 template <bool V>
-__global__ void k_mom_prep_mixed(DevParams p, const double* __restrict__ x,
-                                 const double* __restrict__ oth, const double* __restrict__ pf,
-                                 double* __restrict__ AP, double* __restrict__ cells,
-                                 MomRec32 rec, Range ur) {
-    const int j = ur.j0 + static_cast<int>(blockIdx.x * 32 + threadIdx.x);
-    const int i = ur.i0 + static_cast<int>(blockIdx.y * 8 + threadIdx.y);
-    if (i > ur.i1 || j > ur.j1) return;
+__device__ __forceinline__ double prep_cell(const DevParams& p, const double* __restrict__ x,
+                                            const double* __restrict__ oth, const double* __restrict__ pf,
+                                            double* __restrict__ AP, MomRec32 rec, int i, int j) {
     const std::size_t q = ix(p, i, j), ld = p.pitch;
     double ue, uw, vn, vs;
     if (!V) {
@@ -70,13 +67,41 @@ __global__ void k_mom_prep_mixed(DevParams p, const double* __restrict__ x,
                        c.ASS * x[q + 2 * ld]);
     const double pt = V ? (pf[q] - pf[q - ld]) * p.dx : (pf[q] - pf[q + 1]) * p.dy;
     const double R = nb + pt - c.AP * x[q];
-    cells[static_cast<std::size_t>(i - ur.i0) * ur.cols() + (j - ur.j0)] = fabs(R);
     AP[q] = c.AP;
     rec.near_links[q] = make_float4(static_cast<float>(c.AE), static_cast<float>(c.AW),
                                     static_cast<float>(c.AN), static_cast<float>(c.AS));
     rec.far_links[q] = make_float4(static_cast<float>(c.AEE), static_cast<float>(c.AWW),
                                    static_cast<float>(c.ANN), static_cast<float>(c.ASS));
     rec.diag[q] = make_float2(static_cast<float>(1.0 / c.AP), static_cast<float>(R));
+    return fabs(R);
+}
+
+// Rows per thread of the blocks that also form partial sums: a block of 32 x 8 threads covers 32 x 32
+// cells, so the block tree's tail (one thread adding the warps' sums) is paid once per 1024 cells.
+constexpr int kRowsPerThread = 4;
+
+// FP64 prep over the update range: AP (FP64, for assemble_p and correct), the cell's FP32 record
+// {AE AW AN AS | AEE AWW ANN ASS | 1/AP R}, and the block's FP64 sum of |R| (each thread's cells in
+// row order, then the deterministic tree of blocksum.cuh) into part[block]; k_sum_partials adds the
+// blocks' sums into res_u / res_v.
+template <bool V>
+__global__ void __launch_bounds__(256)
+    k_mom_prep_mixed(DevParams p, const double* __restrict__ x, const double* __restrict__ oth,
+                     const double* __restrict__ pf, double* __restrict__ AP, double* __restrict__ part,
+                     MomRec32 rec, Range ur) {
+    __shared__ double s_sum[8];
+    const int j = ur.j0 + static_cast<int>(blockIdx.x * 32 + threadIdx.x);
+    const int i0 = ur.i0 + static_cast<int>(blockIdx.y * 8 * kRowsPerThread + threadIdx.y);
+    double a = 0.0;
+    if (j <= ur.j1) {
+#pragma unroll 1
+        for (int k = 0; k < kRowsPerThread; ++k) {
+            const int i = i0 + 8 * k;
+            if (i <= ur.i1) a += prep_cell<V>(p, x, oth, pf, AP, rec, i, j);
+        }
+    }
+    const double t = block_sum<8>(a, s_sum, static_cast<int>(threadIdx.y * 32 + threadIdx.x));
+    if (threadIdx.x == 0 && threadIdx.y == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = t;
 }
 
 constexpr int kRing = 32;
@@ -229,32 +254,45 @@ __global__ void __launch_bounds__(NT, MINB)
 }
 
 // assemble_p (pressure.cpp:14-54) in FP64 with the p' operator stored in FP32 (level 0 of the FP32
-// hierarchy) and |b|, b per cell for the ordered sums (res_p and the mean of b).
-__global__ void k_assemble_p_mixed(DevParams p, const double* __restrict__ APU,
-                                   const double* __restrict__ APV, const double* __restrict__ u,
-                                   const double* __restrict__ v, double* __restrict__ bfield,
-                                   LevelView32 L0, double* __restrict__ cabs,
-                                   double* __restrict__ cb) {
+// hierarchy), and the block's FP64 sums of |b| (res_p) and of b (its mean) into part[block] and
+// part[nblocks + block] (deterministic trees, blocksum.cuh).
+__global__ void __launch_bounds__(256)
+    k_assemble_p_mixed(DevParams p, const double* __restrict__ APU, const double* __restrict__ APV,
+                       const double* __restrict__ u, const double* __restrict__ v,
+                       double* __restrict__ bfield, LevelView32 L0, double* __restrict__ part) {
+    __shared__ double s_abs[8], s_b[8];
     const int H = p.H;
     const int J = static_cast<int>(blockIdx.x * 32 + threadIdx.x);
-    const int I = static_cast<int>(blockIdx.y * 8 + threadIdx.y);
-    if (I >= p.NX || J >= p.NY) return;
-    const int i = H + I, j = H + 1 + J;
-    const std::size_t q = ix(p, i, j), ld = p.pitch;
-    const double dx = p.dx, dy = p.dy;
-    const double aep = (j == p.NY + H) ? 0.0 : dy * dy / APU[q];
-    const double awp = (j == H + 1) ? 0.0 : dy * dy / APU[q - 1];
-    const double anp = (i == H) ? 0.0 : dx * dx / APV[q];
-    const double asp = (i == p.NX + H - 1) ? 0.0 : dx * dx / APV[q + ld];
-    const int lq = I * L0.stride + J;
-    set_links(L0, lq, static_cast<float>(aep), static_cast<float>(awp), static_cast<float>(anp),
-              static_cast<float>(asp));
-    L0.AP[lq] = static_cast<float>(aep + awp + anp + asp);
-    const double b = -dx * (-v[q + ld] + v[q]) - dy * (-u[q - 1] + u[q]);
-    bfield[q] = b;
-    const std::size_t c = static_cast<std::size_t>(I) * p.NY + J;
-    if (cabs) cabs[c] = fabs(b);
-    if (cb) cb[c] = b;
+    const int I0 = static_cast<int>(blockIdx.y * 8 * kRowsPerThread + threadIdx.y);
+    double sa = 0.0, sb = 0.0;
+#pragma unroll 1
+    for (int k = 0; k < kRowsPerThread; ++k) {
+        const int I = I0 + 8 * k;
+        if (I >= p.NX || J >= p.NY) break;
+        const int i = H + I, j = H + 1 + J;
+        const std::size_t q = ix(p, i, j), ld = p.pitch;
+        const double dx = p.dx, dy = p.dy;
+        const double aep = (j == p.NY + H) ? 0.0 : dy * dy / APU[q];
+        const double awp = (j == H + 1) ? 0.0 : dy * dy / APU[q - 1];
+        const double anp = (i == H) ? 0.0 : dx * dx / APV[q];
+        const double asp = (i == p.NX + H - 1) ? 0.0 : dx * dx / APV[q + ld];
+        const int lq = I * L0.stride + J;
+        set_links(L0, lq, static_cast<float>(aep), static_cast<float>(awp), static_cast<float>(anp),
+                  static_cast<float>(asp));
+        L0.AP[lq] = static_cast<float>(aep + awp + anp + asp);
+        const double b = -dx * (-v[q + ld] + v[q]) - dy * (-u[q - 1] + u[q]);
+        bfield[q] = b;
+        sa += fabs(b);
+        sb += b;
+    }
+    const int tid = static_cast<int>(threadIdx.y * 32 + threadIdx.x);
+    const double ta = block_sum<8>(sa, s_abs, tid);
+    const double tb = block_sum<8>(sb, s_b, tid);
+    if (tid == 0) {
+        const unsigned nb = gridDim.x * gridDim.y, k = blockIdx.y * gridDim.x + blockIdx.x;
+        part[k] = ta;
+        part[nb + k] = tb;
+    }
 }
 
 // b32 = b - mean(b), rounded to FP32 (remove_mean0, multigrid.cpp:327-345, in FP64 first).
@@ -341,23 +379,28 @@ void launch_corr_m(const DevParams& p, const float* ein, float* eout, MomRec32 r
 // This file alone defines the FP64 launchers (built without contraction); mixed32.cu includes it
 // with SGPU_FLOAT_UNIT for the FP32 correction sweep (contraction allowed).
 #ifndef SGPU_FLOAT_UNIT
-void launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x, const double* oth,
-                           const double* pf, double* AP, double* cells, MomRec32 rec,
-                           cudaStream_t st) {
+int launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x, const double* oth,
+                          const double* pf, double* AP, double* part, MomRec32 rec, cudaStream_t st) {
     const Range ur = update_range(p, v_component);
-    if (ur.rows() <= 0 || ur.cols() <= 0) return;
-    const dim3 grid((ur.cols() + 31) / 32, (ur.rows() + 7) / 8);
-    if (v_component) k_mom_prep_mixed<true><<<grid, dim3(32, 8), 0, st>>>(p, x, oth, pf, AP, cells, rec, ur);
-    else k_mom_prep_mixed<false><<<grid, dim3(32, 8), 0, st>>>(p, x, oth, pf, AP, cells, rec, ur);
+    if (ur.rows() <= 0 || ur.cols() <= 0) return 0;
+    const dim3 grid((ur.cols() + 31) / 32, (ur.rows() + 8 * kRowsPerThread - 1) / (8 * kRowsPerThread));
+    if (v_component) k_mom_prep_mixed<true><<<grid, dim3(32, 8), 0, st>>>(p, x, oth, pf, AP, part, rec, ur);
+    else k_mom_prep_mixed<false><<<grid, dim3(32, 8), 0, st>>>(p, x, oth, pf, AP, part, rec, ur);
     SGPU_LAUNCH();
+    return static_cast<int>(grid.x * grid.y);
 }
 
-void launch_assemble_p_mixed(const DevParams& p, const double* APU, const double* APV,
-                             const double* u, const double* v, double* bfield,
-                             const LevelView32& L0, double* cabs, double* cb, cudaStream_t st) {
-    const dim3 grid((p.NY + 31) / 32, (p.NX + 7) / 8);
-    k_assemble_p_mixed<<<grid, dim3(32, 8), 0, st>>>(p, APU, APV, u, v, bfield, L0, cabs, cb);
+int launch_assemble_p_mixed(const DevParams& p, const double* APU, const double* APV, const double* u,
+                            const double* v, double* bfield, const LevelView32& L0, double* part,
+                            cudaStream_t st) {
+    const dim3 grid((p.NY + 31) / 32, (p.NX + 8 * kRowsPerThread - 1) / (8 * kRowsPerThread));
+    k_assemble_p_mixed<<<grid, dim3(32, 8), 0, st>>>(p, APU, APV, u, v, bfield, L0, part);
     SGPU_LAUNCH();
+    return static_cast<int>(grid.x * grid.y);
+}
+
+int mixed_partials(const DevParams& p) {
+    return 2 * ((p.NY + 32) / 32) * ((p.NX + 8 * kRowsPerThread) / (8 * kRowsPerThread));
 }
 
 void launch_b_to_f32(const DevParams& p, const double* bfield, const double* sum_b,

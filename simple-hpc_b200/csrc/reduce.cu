@@ -12,6 +12,7 @@
 // to finish adds the row sums in row order. Inputs may be FP64 or FP32 (widened to FP64 when
 // added); the sums are FP64.
 #include "kernels.hpp"
+#include "blocksum.cuh"
 
 #include <algorithm>
 
@@ -169,7 +170,65 @@ void launch_sum(const TIn* vals, std::size_t plane_stride, int ld, int nr, int n
     SGPU_LAUNCH();
 }
 
+// ---- deterministic FP64 tree sums (the mixed-precision path) ----
+
+// out_k = the sum of the n partial sums of plane k (block k): thread t adds values t, t + 1024, ...
+// in order, then the block tree.
+__global__ void __launch_bounds__(1024)
+    k_sum_partials(const double* __restrict__ part, int n, int plane, double* out0, double* out1) {
+    __shared__ double s[32];
+    const double* src = part + static_cast<std::size_t>(blockIdx.x) * plane;
+    double a = 0.0;
+#pragma unroll 8
+    for (int i = static_cast<int>(threadIdx.x); i < n; i += 1024) a += src[i];
+    const double t = block_sum<32>(a, s, static_cast<int>(threadIdx.x));
+    if (threadIdx.x == 0) *(blockIdx.x == 0 ? out0 : out1) = t;
+}
+
+constexpr int kTileRows = 32; // rows per block of k_tile_sum
+
+// Block (bx, by) of an nr x nc array (row stride ld): columns 256 bx .. +255, rows 32 by .. +31.
+// Each thread adds its column's values top to bottom in FP64, then the block tree; one partial sum
+// per block.
+template <class T>
+__global__ void __launch_bounds__(256)
+    k_tile_sum(const T* __restrict__ vals, int ld, int nr, int nc, double* __restrict__ part) {
+    __shared__ double s[8];
+    const int c = static_cast<int>(blockIdx.x * 256 + threadIdx.x);
+    const int r0 = static_cast<int>(blockIdx.y) * kTileRows, r1 = min(r0 + kTileRows, nr);
+    double a = 0.0;
+    if (c < nc) {
+        const T* src = vals + static_cast<std::size_t>(r0) * ld + c;
+#pragma unroll 8
+        for (int r = r0; r < r1; ++r, src += ld) a += static_cast<double>(*src);
+    }
+    const double t = block_sum<8>(a, s, static_cast<int>(threadIdx.x));
+    if (threadIdx.x == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = t;
+}
+
 } // namespace
+
+void launch_sum_partials(const double* part, int n, int K, int plane, double* out0, double* out1,
+                         cudaStream_t st) {
+    if (K < 1 || K > 2 || (K == 2 && !out1)) throw Error(SGPU_E_INVALID, "partial sums: 1 or 2 planes");
+    k_sum_partials<<<K, 1024, 0, st>>>(part, n, plane, out0, out1);
+    SGPU_LAUNCH();
+}
+
+int tree_sum_partials(int nr, int nc) {
+    return ((nc + 255) / 256) * ((nr + kTileRows - 1) / kTileRows);
+}
+
+void launch_tree_sum(const float* vals, int ld, int nr, int nc, double* part, double* out, cudaStream_t st) {
+    if (nr <= 0 || nc <= 0) {
+        SGPU_CUDA(cudaMemsetAsync(out, 0, sizeof(double), st));
+        return;
+    }
+    const dim3 grid((nc + 255) / 256, (nr + kTileRows - 1) / kTileRows);
+    k_tile_sum<float><<<grid, 256, 0, st>>>(vals, ld, nr, nc, part);
+    SGPU_LAUNCH();
+    launch_sum_partials(part, static_cast<int>(grid.x * grid.y), 1, 0, out, nullptr, st);
+}
 
 void launch_ordered_sum(const double* vals, std::size_t plane_stride, int ld, int nr, int nc, int K,
                         double* out, const SumScratch& s, const int* skip, cudaStream_t st) {

@@ -357,6 +357,7 @@ struct Solver {
         p_links_stale = false;
     }
     MomRec32 rec32{};                 // per-cell FP32 records: coefficients, 1/AP, R
+    double* part = nullptr;           // per-block partial sums of the FP64 tree sums
     float* e32[2] = {nullptr, nullptr}; // correction ping-pong
     std::vector<LevelView32> lv32;    // FP32 multigrid hierarchy (level 0: the p' operator)
     std::vector<float*> mg32_x2;
@@ -370,10 +371,9 @@ struct Solver {
         if (vcomp) launch_bc_v(dp, v, st);
         else launch_bc_u(dp, u, st);
         mark(vcomp ? SGPU_PH_ASSEMBLE_V : SGPU_PH_ASSEMBLE_U);
-        double* cplane = cells + (vcomp ? plane : 0);
-        launch_mom_prep_mixed(dp, vcomp, x, oth, pf, AP, cplane, rec32, st);
+        const int nparts = launch_mom_prep_mixed(dp, vcomp, x, oth, pf, AP, part, rec32, st);
         mark(vcomp ? SGPU_PH_RESIDUAL_V : SGPU_PH_RESIDUAL_U);
-        momentum_sum(vcomp, res, cplane);
+        launch_sum_partials(part, nparts, 1, 0, res, nullptr, st); // res_u / res_v: FP64 tree
         mark(vcomp ? SGPU_PH_SWEEP_V : SGPU_PH_SWEEP_U);
         const int n = vcomp ? prm.maxit_inner_v : prm.maxit_inner_u;
         int cur = 0; // e32[cur] holds the current correction (zero before the first sweep)
@@ -391,12 +391,10 @@ struct Solver {
         pc_stale = true;
         mixed_momentum(false, res3 + 0);
         mixed_momentum(true, res3 + 1);
-        join_sums();
         mark(SGPU_PH_ASSEMBLE_P);
-        launch_assemble_p_mixed(dp, cu.a[8], cv.a[8], u, v, w.b, lv32[0], nullptr, nullptr, st);
-        // sum of |b| (res_p) and sum of b (its mean) in one pass over b
-        launch_ordered_sum_abs_pair(w.b + p_origin(), g.pitch, prm.NX, prm.NY, sums + 24, ss, st);
-        SGPU_CUDA(cudaMemcpyAsync(res3 + 2, sums + 24, sizeof(double), cudaMemcpyDeviceToDevice, st));
+        const int nparts = launch_assemble_p_mixed(dp, cu.a[8], cv.a[8], u, v, w.b, lv32[0], part, st);
+        // res_p = the sum of |b|, and the sum of b (its mean), from the blocks' partial sums
+        launch_sum_partials(part, nparts, 2, nparts, res3 + 2, sums + 25, st);
         mark(SGPU_PH_SOLVE_P);
         for (std::size_t l = 1; l < lv32.size(); ++l) launch_mg_build<float>(lv32[l - 1], lv32[l], st);
         launch_b_to_f32(dp, w.b, sums + 25, lv32[0], st);
@@ -415,7 +413,7 @@ struct Solver {
                                     prm.mg_post, sms, min_seg, st);
         };
         last_vcycles = run_cycles(L0, !guess, vcycle32);
-        launch_ordered_sum(L0.x, 0, L0.stride, L0.nx, L0.ny, 1, sums + 26, ss, nullptr, st);
+        launch_tree_sum(L0.x, L0.stride, L0.nx, L0.ny, part, sums + 26, st); // the mean of p'
         mark(SGPU_PH_CORRECT);
         launch_correct_mixed(dp, L0, sums + 26, cu.a[8], cv.a[8], u, v, pf, nullptr, st);
         mark(SGPU_PH_COUNT);
@@ -694,6 +692,7 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
         rec32.near_links = dalloc<float4>(g.elems());
         rec32.far_links = dalloc<float4>(g.elems());
         rec32.diag = dalloc<float2>(g.elems());
+        part = dalloc<double>(static_cast<std::size_t>(std::max(mixed_partials(dp), tree_sum_partials(p.NX, p.NY))));
         e32[0] = dalloc<float>(g.elems());
         e32[1] = dalloc<float>(g.elems());
         const int nl = static_cast<int>(lv.size());

@@ -5,8 +5,9 @@ the FP64 oracle and check that it converges like the FP64 method:
 * the 32 x 32, Re 100, QUICK / 2, gs_multicolour + mg case (494 FP64 iterations to 1e-5) converges
   in about as many iterations and to the FP64 fields within a small relative error;
 * fixed work on the 32 x 40 snapshot case stays close to the FP64 trajectory;
-* the residuals the stopping test reads are computed in FP64 (the first iteration's res_u and res_v,
-  which do not depend on any inner solve, are bit-identical to the oracle's).
+* the residuals the stopping test reads are computed in FP64: the first iteration's res_u and res_v,
+  which do not depend on any inner solve, equal the oracle's to FP64 rounding (the mixed path adds
+  the per-cell |R| in a fixed tree instead of the reference's row-by-row chain).
 Errors are reported as max |a - b| / max |b| (relative to the field's scale) and L2 relative.
 """
 from __future__ import annotations
@@ -57,8 +58,11 @@ def test_mixed_fixed_work_close_to_fp64(sgpu_mod, oracle_mod):
     with sgpu_mod.Solver(p) as s:
         res, log = s.run(60)
         fields = {k: s.download(f) for k, f in (("u", 0), ("v", 1), ("p", 2))}
-    # The first iteration's momentum residuals are computed before any inner solve: FP64, exact.
-    assert log[0, 1] == olog[0, 1] and log[0, 2] == olog[0, 2]
+    # The first iteration's momentum residuals are computed before any inner solve: FP64 values,
+    # summed in a different order than the oracle's chain (each of 1280 terms rounds once).
+    diff = np.abs(log[0, 1:3] - olog[0, 1:3])
+    print(f"first-iteration res_u, res_v: {log[0, 1:3]} vs {olog[0, 1:3]}")
+    assert np.all(diff <= 1e-13 * np.abs(olog[0, 1:3]))
     for k, f in (("u", 0), ("v", 1), ("p", 2)):
         mx, l2 = rel_errors(fields[k], o.get(f))
         print(f"{k}: max rel {mx:.3e}, L2 rel {l2:.3e}")

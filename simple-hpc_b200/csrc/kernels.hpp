@@ -155,9 +155,12 @@ void launch_cg_dir(const DevParams& p, CgPtr cg, const CgScalars* sc, cudaStream
 void init_mixed_kernels();
 // Resident CTAs per SM of the FP32 correction sweep (its register and shared-memory footprint).
 int corr_blocks_per_sm(int ncol);
-// Per-cell FP32 momentum records of the mixed path, three arrays indexed like the fields
-// (i * pitch + j): the near links {AE AW AN AS}, the far links {AEE AWW ANN ASS}, and {1/AP, R}.
-// 40 bytes per cell; a warp's load of each array is contiguous.
+// Per-cell FP32 momentum records of the mixed path in three arrays: the near links {AE AW AN AS},
+// the far links {AEE AWW ANN ASS}, and {1/AP, R}; 40 bytes per cell. They are stored by sweep step:
+// the record of cell (i, j) of colour c (c = (i + 3j) mod 5 for five colours, (i + j) mod 2 for
+// two) sits at (i + 2c) * pitch + j, so the cells the streaming sweep updates at one step, one per
+// column, are contiguous. The arrays have kRecExtraRows rows more than the fields.
+constexpr int kRecExtraRows = 8;
 struct MomRec32 {
     float4* near_links;
     float4* far_links;

@@ -43,11 +43,18 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// One cell of the prep; returns |R|.
+// The tile of one prep block: 32 columns x kTileRows rows, 32 x 8 threads, kTileRows / 8 cells per
+// thread. The block's partial sum (a block tree's tail: one thread adding the warps' sums) is paid
+// once per tile.
+constexpr int kRowsPerThread = 4;
+constexpr int kTileRows = 8 * kRowsPerThread;
+
+// One cell of the prep: AP (FP64) and the cell's FP32 record into the tile in shared memory; returns |R|.
 template <bool V>
 __device__ __forceinline__ double prep_cell(const DevParams& p, const double* __restrict__ x,
                                             const double* __restrict__ oth, const double* __restrict__ pf,
-                                            double* __restrict__ AP, MomRec32 rec, int i, int j) {
+                                            double* __restrict__ AP, float4& near, float4& far, float2& diag,
+                                            int i, int j) {
     const std::size_t q = ix(p, i, j), ld = p.pitch;
     double ue, uw, vn, vs;
     if (!V) {
@@ -68,64 +75,105 @@ __device__ __forceinline__ double prep_cell(const DevParams& p, const double* __
     const double pt = V ? (pf[q] - pf[q - ld]) * p.dx : (pf[q] - pf[q + 1]) * p.dy;
     const double R = nb + pt - c.AP * x[q];
     AP[q] = c.AP;
-    rec.near_links[q] = make_float4(static_cast<float>(c.AE), static_cast<float>(c.AW),
-                                    static_cast<float>(c.AN), static_cast<float>(c.AS));
-    rec.far_links[q] = make_float4(static_cast<float>(c.AEE), static_cast<float>(c.AWW),
-                                   static_cast<float>(c.ANN), static_cast<float>(c.ASS));
-    rec.diag[q] = make_float2(static_cast<float>(1.0 / c.AP), static_cast<float>(R));
+    near = make_float4(static_cast<float>(c.AE), static_cast<float>(c.AW), static_cast<float>(c.AN),
+                       static_cast<float>(c.AS));
+    far = make_float4(static_cast<float>(c.AEE), static_cast<float>(c.AWW), static_cast<float>(c.ANN),
+                      static_cast<float>(c.ASS));
+    diag = make_float2(static_cast<float>(1.0 / c.AP), static_cast<float>(R));
     return fabs(R);
 }
-
-// Rows per thread of the blocks that also form partial sums: a block of 32 x 8 threads covers 32 x 32
-// cells, so the block tree's tail (one thread adding the warps' sums) is paid once per 1024 cells.
-constexpr int kRowsPerThread = 4;
 
 // FP64 prep over the update range: AP (FP64, for assemble_p and correct), the cell's FP32 record
 // {AE AW AN AS | AEE AWW ANN ASS | 1/AP R}, and the block's FP64 sum of |R| (each thread's cells in
 // row order, then the deterministic tree of blocksum.cuh) into part[block]; k_sum_partials adds the
 // blocks' sums into res_u / res_v.
+// The records are stored by sweep step (MomRec32): the block stages its tile's records in shared
+// memory, then each warp writes whole step rows, the cells of one step row lying on up to five
+// field rows of the tile; a step row the tile shares with its neighbour is written in part by each.
 template <bool V>
 __global__ void __launch_bounds__(256)
     k_mom_prep_mixed(DevParams p, const double* __restrict__ x, const double* __restrict__ oth,
                      const double* __restrict__ pf, double* __restrict__ AP, double* __restrict__ part,
                      MomRec32 rec, Range ur) {
     __shared__ double s_sum[8];
-    const int j = ur.j0 + static_cast<int>(blockIdx.x * 32 + threadIdx.x);
-    const int i0 = ur.i0 + static_cast<int>(blockIdx.y * 8 * kRowsPerThread + threadIdx.y);
+    __shared__ float4 s_near[kTileRows][32], s_far[kTileRows][32];
+    __shared__ float2 s_diag[kTileRows][32];
+    const int lane = static_cast<int>(threadIdx.x), wy = static_cast<int>(threadIdx.y);
+    const int j = ur.j0 + static_cast<int>(blockIdx.x) * 32 + lane;
+    const int ib = ur.i0 + static_cast<int>(blockIdx.y) * kTileRows; // the tile's first row
     double a = 0.0;
     if (j <= ur.j1) {
 #pragma unroll 1
         for (int k = 0; k < kRowsPerThread; ++k) {
-            const int i = i0 + 8 * k;
-            if (i <= ur.i1) a += prep_cell<V>(p, x, oth, pf, AP, rec, i, j);
+            const int ti = wy + 8 * k;
+            if (ib + ti <= ur.i1)
+                a += prep_cell<V>(p, x, oth, pf, AP, s_near[ti][lane], s_far[ti][lane], s_diag[ti][lane],
+                                  ib + ti, j);
         }
     }
-    const double t = block_sum<8>(a, s_sum, static_cast<int>(threadIdx.y * 32 + threadIdx.x));
-    if (threadIdx.x == 0 && threadIdx.y == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = t;
+    const double t = block_sum<8>(a, s_sum, wy * 32 + lane); // its barrier also publishes the tile
+    if (lane == 0 && wy == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = t;
+    // step rows ib .. ib + kTileRows - 1 + 2 (ncol - 1): cell (i, j) of colour c is updated at step
+    // i + 2c, and the cell updated at step s in column j has colour (2s + j) mod 5 (five colours) or
+    // (s + j) mod 2 (two)
+    const int nsteps = kTileRows + 2 * (p.ncol - 1);
+    if (j > ur.j1) return;
+    for (int k = wy; k < nsteps; k += 8) {
+        const int st = ib + k;
+        const int c = p.ncol == 5 ? (2 * st + j) % 5 : (st + j) & 1;
+        const int ti = k - 2 * c; // the cell's row in the tile
+        if (ti < 0 || ti >= kTileRows || ib + ti > ur.i1) continue;
+        const std::size_t q = static_cast<std::size_t>(st) * p.pitch + j;
+        rec.near_links[q] = s_near[ti][lane];
+        rec.far_links[q] = s_far[ti][lane];
+        rec.diag[q] = s_diag[ti][lane];
+    }
 }
 
-constexpr int kRing = 32;
-constexpr int kPrefetch = 8;
+constexpr int kRing = 32;    // rows of the e ring (a power of two)
+constexpr int kRecAhead = 2; // super-steps whose records are in flight (cp.async into shared memory)
 
-struct Rec {
-    float4 a, b;
-    float2 c; // 1/AP, R
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+// Shared memory of k_corr_stream: the e ring (kRing rows of NT floats), then kRecAhead x SPB record
+// slots of NT cells each in three arrays (near links, far links for five colours, {1/AP, R}).
+template <int NCOL, int NT> struct CorrSmem {
+    static constexpr int SPB = NCOL == 5 ? 2 : 1;
+    static constexpr int slots = kRecAhead * SPB;
+    static constexpr int ring = kRing * NT * 4;
+    static constexpr int near = slots * NT * 16;
+    static constexpr int far = NCOL == 5 ? slots * NT * 16 : 0;
+    static constexpr int diag = slots * NT * 8;
+    static constexpr int bytes = ring + near + far + diag;
 };
 
 // One FP32 multicolour correction sweep e_in -> e_out from the stored records; the time-skewed
-// streaming of k_mom_stream (fused.cu): cell (r, j) of colour c at step r + 2c, two steps per
-// barrier for five colours, strip halo 2 per colour. The next super-step's records are loaded one
-// super-step ahead into the other of two register sets. e_zero: e_in is zero and is not read.
+// streaming of k_mom_stream (fused.cu): cell (r, j) of colour c at step r + 2c, SPB steps per
+// barrier (two for five colours), strip halo 2 per colour.
+// Pipeline: super-step k (steps L0 + SPB k ..) waits for the copy group committed kRecAhead
+// super-steps earlier, which holds the records of its cells and e rows far enough ahead; after its
+// updates each thread issues, as one group, the next SPB e rows and the records of super-step
+// k + kRecAhead into the slots it has just read (its own: no other thread touches them). Keeping
+// the records out of registers lets kRecAhead x 20 KB of them per CTA be in flight.
+// e_zero: e_in is zero and is not read.
 template <int NCOL, bool V, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     k_corr_stream(DevParams p, const float* __restrict__ ein, float* __restrict__ eout,
                   MomRec32 rec, int e_zero, int seg_rows, double* __restrict__ xfinal) {
-    constexpr int SPB = NCOL == 5 ? 2 : 1;
+    using S = CorrSmem<NCOL, NT>;
+    constexpr int SPB = S::SPB;
     constexpr int HC = 2 * NCOL;
     constexpr int W = NT - 2 * HC;
-    constexpr int A = kPrefetch + SPB + 2;
+    constexpr int D = kRecAhead;
+    constexpr int E0 = SPB * D + 2; // e rows issued before the first super-step
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* ring_mem = reinterpret_cast<float*>(smem_raw);
+    float4* s_near = reinterpret_cast<float4*>(smem_raw + S::ring);
+    float4* s_far = reinterpret_cast<float4*>(smem_raw + S::ring + S::near);
+    float2* s_diag = reinterpret_cast<float2*>(smem_raw + S::ring + S::near + S::far);
     __shared__ int s_rmin[NCOL], s_rmax[NCOL];
     const int tid = threadIdx.x;
     const int j0 = blockIdx.x * W;
@@ -166,73 +214,77 @@ __global__ void __launch_bounds__(NT, MINB)
     const float4* __restrict__ rfar = rec.far_links + col;
     const float2* __restrict__ rdiag = rec.diag + col;
     int next = L0;
-    auto issue = [&]() {
+    auto issue_row = [&]() {
         if (next < L1 && col_in) {
             float* dst = ringc + (next & (kRing - 1)) * NT;
             if (e_zero) *dst = 0.0f;
             else cp_async(dst, ein + col + next * ld);
         }
-        cp_async_commit();
         ++next;
     };
     auto step_cell = [&](int c, int t, int& r) -> bool {
         r = t - 2 * c;
         return ((colmask >> c) & 1u) && r >= s_rmin[c] && r <= s_rmax[c];
     };
-    auto load_rec = [&](int r, Rec& x) {
-        const int o = r * ld;
-        x.a = __ldg(rnear + o);
-        if (NCOL == 5) x.b = __ldg(rfar + o);
-        x.c = __ldg(rdiag + o);
+    auto next_colour = [&](int c, int steps) {
+        return NCOL == 5 ? (c + 2 * steps) % 5 : (c + steps) & 1;
     };
-    auto update = [&](int r, const Rec& x) {
+    // the records of super-step k's cells (first colour c0k) into its slots
+    auto issue_rec = [&](int k, int c0k) {
+        const int t = L0 + SPB * k;
+#pragma unroll
+        for (int s = 0; s < SPB; ++s) {
+            int r;
+            if (step_cell(next_colour(c0k, s), t + s, r)) {
+                const int q = ((k % D) * SPB + s) * NT + tid;
+                const int o = (t + s) * ld; // records are stored by step: a warp reads one row
+                cp_async16(s_near + q, rnear + o);
+                if (NCOL == 5) cp_async16(s_far + q, rfar + o);
+                cp_async(s_diag + q, rdiag + o);
+            }
+        }
+    };
+    auto update = [&](int r, int q) {
+        const float4 a = s_near[q];
+        const float2 dg = s_diag[q];
         float* rc = ringc + (r & (kRing - 1)) * NT;
         const float ee = rc[1], ew = rc[-1];
         const float en = ringc[((r - 1) & (kRing - 1)) * NT];
         const float es = ringc[((r + 1) & (kRing - 1)) * NT];
-        float nb = x.a.x * ee + x.a.y * ew + x.a.z * en + x.a.w * es;
+        float nb = a.x * ee + a.y * ew + a.z * en + a.w * es;
         if (NCOL == 5) {
+            const float4 b = s_far[q];
             const float eee = rc[2], eww = rc[-2];
             const float enn = ringc[((r - 2) & (kRing - 1)) * NT];
             const float ess = ringc[((r + 2) & (kRing - 1)) * NT];
-            nb += x.b.x * eee + x.b.y * eww + x.b.z * enn + x.b.w * ess;
+            nb += b.x * eee + b.y * eww + b.z * enn + b.w * ess;
         }
         const float e0 = rc[0];
-        rc[0] = e0 + relax * ((x.c.y + nb) * x.c.x - e0);
-    };
-    auto next_colour = [&](int c, int steps) {
-        return NCOL == 5 ? (c + 2 * steps) % 5 : (c + steps) & 1;
+        rc[0] = e0 + relax * ((dg.y + nb) * dg.x - e0);
     };
 
-    for (int k = 0; k < A; ++k) issue();
-    __syncthreads();
+    __syncthreads(); // s_rmin / s_rmax
     const int c_start = NCOL == 5 ? (2 * L0 + col + 1000) % 5 : (L0 + col + 1000) & 1;
     const int t_last = R1 + 2 * NCOL - 2 + (SPB - 1);
-
-    Rec bufA[SPB], bufB[SPB];
-    int rA[SPB], rB[SPB];
-    bool okA[SPB], okB[SPB];
-#pragma unroll
-    for (int s = 0; s < SPB; ++s) {
-        okA[s] = step_cell(next_colour(c_start, s), L0 + s, rA[s]);
-        if (okA[s]) load_rec(rA[s], bufA[s]);
+    // prologue: D groups, the first with E0 e rows; group k holds super-step k's records
+    int c_iss = c_start;
+    for (int i = 0; i < E0; ++i) issue_row();
+    for (int k = 0; k < D; ++k) {
+        issue_rec(k, c_iss);
+        cp_async_commit();
+        c_iss = next_colour(c_iss, SPB);
     }
-    auto super_step = [&](int t, int c0, const Rec (&cur)[SPB], const int (&rcur)[SPB],
-                          const bool (&okcur)[SPB], Rec (&nxt)[SPB], int (&rnxt)[SPB],
-                          bool (&oknxt)[SPB]) {
-        cp_async_wait<kPrefetch>();
-        __syncthreads();
-#pragma unroll
-        for (int s = 0; s < SPB; ++s) issue();
-        const int cn = next_colour(c0, SPB);
+    int c_cur = c_start;
+    for (int k = 0;; ++k) {
+        const int t = L0 + SPB * k;
+        if (t > t_last) break;
+        cp_async_wait<D - 1>(); // this thread's group of super-step k has landed
+        __syncthreads();         // ... and everyone's
 #pragma unroll
         for (int s = 0; s < SPB; ++s) {
-            oknxt[s] = step_cell(next_colour(cn, s), t + SPB + s, rnxt[s]);
-            if (oknxt[s]) load_rec(rnxt[s], nxt[s]);
+            int r;
+            if (step_cell(next_colour(c_cur, s), t + s, r)) update(r, ((k % D) * SPB + s) * NT + tid);
         }
-#pragma unroll
-        for (int s = 0; s < SPB; ++s)
-            if (okcur[s]) update(rcur[s], cur[s]);
 #pragma unroll
         for (int s = 0; s < SPB; ++s) {
             const int rw = t - 2 * NCOL + 1 - (SPB - 1) + s;
@@ -243,12 +295,15 @@ __global__ void __launch_bounds__(NT, MINB)
                     xfinal[static_cast<std::size_t>(rw) * ld + col] += static_cast<double>(ev);
             }
         }
-        return cn;
-    };
-    int c0 = c_start;
-    for (int t = L0; t <= t_last; t += 2 * SPB) {
-        c0 = super_step(t, c0, bufA, rA, okA, bufB, rB, okB);
-        if (t + SPB <= t_last) c0 = super_step(t + SPB, c0, bufB, rB, okB, bufA, rA, okA);
+        // The slots just read are refilled only after this thread's updates have consumed them
+        // (each update's store depends on its record loads); e rows land in ring rows no one reads
+        // before the next barriers.
+#pragma unroll
+        for (int s = 0; s < SPB; ++s) issue_row();
+        issue_rec(k + D, c_iss);
+        cp_async_commit();
+        c_cur = next_colour(c_cur, SPB);
+        c_iss = next_colour(c_iss, SPB);
     }
     cp_async_wait<0>();
 }
@@ -361,7 +416,7 @@ void launch_corr(const DevParams& p, const float* ein, float* eout, MomRec32 rec
                  int seg_rows, double* xfinal, cudaStream_t st) {
     constexpr int W = NT - 4 * NCOL;
     const dim3 grid((p.ncols + W - 1) / W, (p.nrows + seg_rows - 1) / seg_rows);
-    constexpr int smem = kRing * NT * static_cast<int>(sizeof(float));
+    constexpr int smem = CorrSmem<NCOL, NT>::bytes;
     k_corr_stream<NCOL, V, NT, MINB><<<grid, NT, smem, st>>>(p, ein, eout, rec, e_zero ? 1 : 0, seg_rows,
                                                               xfinal);
     SGPU_LAUNCH();
@@ -438,16 +493,16 @@ void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, f
 }
 
 void init_mixed_kernels() {
-    const int smem = kRing * 256 * static_cast<int>(sizeof(float));
-#define SGPU_SMEM(NC, V, M) \
-    SGPU_CUDA(cudaFuncSetAttribute(k_corr_stream<NC, V, 256, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))
+#define SGPU_SMEM(NC, V, M)                                                                            \
+    SGPU_CUDA(cudaFuncSetAttribute(k_corr_stream<NC, V, 256, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                   CorrSmem<NC, 256>::bytes))
     SGPU_SMEM(5, false, 3); SGPU_SMEM(5, true, 3); SGPU_SMEM(2, false, 3); SGPU_SMEM(2, true, 3);
     SGPU_SMEM(5, false, 4); SGPU_SMEM(5, true, 4); SGPU_SMEM(2, false, 4); SGPU_SMEM(2, true, 4);
 #undef SGPU_SMEM
 }
 
 int corr_blocks_per_sm(int ncol) {
-    const int smem = kRing * 256 * static_cast<int>(sizeof(float));
+    const int smem = ncol == 5 ? CorrSmem<5, 256>::bytes : CorrSmem<2, 256>::bytes;
     int n = 0;
     const bool four = corr_minb() == 4;
     if (ncol == 5)

@@ -689,9 +689,10 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
         mixed = true;
         init_mixed_kernels();
         seg_rows = stream_seg_rows(dp, sms, corr_blocks_per_sm(dp.ncol), min_seg);
-        rec32.near_links = dalloc<float4>(g.elems());
-        rec32.far_links = dalloc<float4>(g.elems());
-        rec32.diag = dalloc<float2>(g.elems());
+        const std::size_t nrec = g.elems() + static_cast<std::size_t>(kRecExtraRows) * g.pitch;
+        rec32.near_links = dalloc<float4>(nrec);
+        rec32.far_links = dalloc<float4>(nrec);
+        rec32.diag = dalloc<float2>(nrec);
         part = dalloc<double>(static_cast<std::size_t>(std::max(mixed_partials(dp), tree_sum_partials(p.NX, p.NY))));
         e32[0] = dalloc<float>(g.elems());
         e32[1] = dalloc<float>(g.elems());

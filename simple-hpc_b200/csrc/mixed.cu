@@ -91,7 +91,7 @@ __device__ __forceinline__ double prep_cell(const DevParams& p, const double* __
 // memory, then each warp writes whole step rows, the cells of one step row lying on up to five
 // field rows of the tile; a step row the tile shares with its neighbour is written in part by each.
 template <bool V>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
     k_mom_prep_mixed(DevParams p, const double* __restrict__ x, const double* __restrict__ oth,
                      const double* __restrict__ pf, double* __restrict__ AP, double* __restrict__ part,
                      MomRec32 rec, Range ur) {

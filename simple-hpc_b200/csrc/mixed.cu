@@ -210,17 +210,21 @@ __global__ void __launch_bounds__(NT, MINB)
     }
     const float relax = static_cast<float>(V ? p.av : p.au);
     float* ringc = ring_mem + tid;
-    const float4* __restrict__ rnear = rec.near_links + col;
-    const float4* __restrict__ rfar = rec.far_links + col;
-    const float2* __restrict__ rdiag = rec.diag + col;
+    static_assert(D == 2, "the step loop is unrolled over the two record slots");
+    // Running offsets: the next e row to issue, the step row of the next records to issue, and the
+    // row the next super-step writes out.
     int next = L0;
+    int eo = col + L0 * ld;
+    int ro = col + L0 * ld;
+    int wo = col + (L0 - 2 * NCOL + 1 - (SPB - 1)) * ld;
     auto issue_row = [&]() {
         if (next < L1 && col_in) {
             float* dst = ringc + (next & (kRing - 1)) * NT;
             if (e_zero) *dst = 0.0f;
-            else cp_async(dst, ein + col + next * ld);
+            else cp_async(dst, ein + eo);
         }
         ++next;
+        eo += ld;
     };
     auto step_cell = [&](int c, int t, int& r) -> bool {
         r = t - 2 * c;
@@ -229,20 +233,24 @@ __global__ void __launch_bounds__(NT, MINB)
     auto next_colour = [&](int c, int steps) {
         return NCOL == 5 ? (c + 2 * steps) % 5 : (c + steps) & 1;
     };
-    // the records of super-step k's cells (first colour c0k) into its slots
-    auto issue_rec = [&](int k, int c0k) {
-        const int t = L0 + SPB * k;
+    // The records of the super-step whose first step is t (first colour c0k) into record slot
+    // `slot`; rs[s] keeps the row of its s-th cell (-1: none) for the update SPB * D steps later.
+    auto issue_rec = [&](int slot, int t, int c0k, int (&rs)[SPB]) {
 #pragma unroll
         for (int s = 0; s < SPB; ++s) {
             int r;
             if (step_cell(next_colour(c0k, s), t + s, r)) {
-                const int q = ((k % D) * SPB + s) * NT + tid;
-                const int o = (t + s) * ld; // records are stored by step: a warp reads one row
-                cp_async16(s_near + q, rnear + o);
-                if (NCOL == 5) cp_async16(s_far + q, rfar + o);
-                cp_async(s_diag + q, rdiag + o);
+                const int q = (slot * SPB + s) * NT + tid;
+                const int o = ro + s * ld; // records are stored by step: a warp reads one row
+                cp_async16(s_near + q, rec.near_links + o);
+                if (NCOL == 5) cp_async16(s_far + q, rec.far_links + o);
+                cp_async(s_diag + q, rec.diag + o);
+                rs[s] = r;
+            } else {
+                rs[s] = -1;
             }
         }
+        ro += SPB * ld;
     };
     auto update = [&](int r, int q) {
         const float4 a = s_near[q];
@@ -262,37 +270,54 @@ __global__ void __launch_bounds__(NT, MINB)
         const float e0 = rc[0];
         rc[0] = e0 + relax * ((dg.y + nb) * dg.x - e0);
     };
+    // The last sweep (xfinal) adds e into x: x of the rows a super-step writes is loaded one
+    // super-step ahead, so the read-modify-write does not wait on memory inside the step.
+    auto x_row = [&](int rw) {
+        return rw >= R0 && rw < R1 && col_out && rw >= ui0 && rw <= ui1 && col >= uj0 && col <= uj1;
+    };
+    double xpre[SPB];
 
     __syncthreads(); // s_rmin / s_rmax
     const int c_start = NCOL == 5 ? (2 * L0 + col + 1000) % 5 : (L0 + col + 1000) & 1;
     const int t_last = R1 + 2 * NCOL - 2 + (SPB - 1);
     // prologue: D groups, the first with E0 e rows; group k holds super-step k's records
     int c_iss = c_start;
+    int rs0[SPB], rs1[SPB];
     for (int i = 0; i < E0; ++i) issue_row();
-    for (int k = 0; k < D; ++k) {
-        issue_rec(k, c_iss);
-        cp_async_commit();
-        c_iss = next_colour(c_iss, SPB);
+    issue_rec(0, L0, c_iss, rs0);
+    cp_async_commit();
+    c_iss = next_colour(c_iss, SPB);
+    issue_rec(1, L0 + SPB, c_iss, rs1);
+    cp_async_commit();
+    c_iss = next_colour(c_iss, SPB);
+#pragma unroll
+    for (int s = 0; s < SPB; ++s) {
+        const int rw = L0 - 2 * NCOL + 1 - (SPB - 1) + s;
+        xpre[s] = (xfinal && x_row(rw)) ? xfinal[wo + s * ld] : 0.0;
     }
-    int c_cur = c_start;
-    for (int k = 0;; ++k) {
-        const int t = L0 + SPB * k;
-        if (t > t_last) break;
-        cp_async_wait<D - 1>(); // this thread's group of super-step k has landed
+
+    auto super_step = [&](int t, int slot, int (&rs)[SPB]) {
+        cp_async_wait<D - 1>(); // this thread's group of this super-step has landed
         __syncthreads();         // ... and everyone's
 #pragma unroll
-        for (int s = 0; s < SPB; ++s) {
-            int r;
-            if (step_cell(next_colour(c_cur, s), t + s, r)) update(r, ((k % D) * SPB + s) * NT + tid);
-        }
+        for (int s = 0; s < SPB; ++s)
+            if (rs[s] >= 0) update(rs[s], (slot * SPB + s) * NT + tid);
 #pragma unroll
         for (int s = 0; s < SPB; ++s) {
             const int rw = t - 2 * NCOL + 1 - (SPB - 1) + s;
-            if (rw >= R0 && rw < R1 && col_out) {
-                const float ev = ringc[(rw & (kRing - 1)) * NT];
-                if (!xfinal) eout[col + rw * ld] = ev;
-                else if (rw >= ui0 && rw <= ui1 && col >= uj0 && col <= uj1) // the last sweep: x += e
-                    xfinal[static_cast<std::size_t>(rw) * ld + col] += static_cast<double>(ev);
+            const float ev = ringc[(rw & (kRing - 1)) * NT];
+            if (!xfinal) {
+                if (rw >= R0 && rw < R1 && col_out) eout[wo + s * ld] = ev;
+            } else if (x_row(rw)) { // the last sweep: x += e
+                xfinal[wo + s * ld] = xpre[s] + static_cast<double>(ev);
+            }
+        }
+        wo += SPB * ld;
+        if (xfinal) {
+#pragma unroll
+            for (int s = 0; s < SPB; ++s) { // the rows the next super-step writes
+                const int rw = t + SPB - 2 * NCOL + 1 - (SPB - 1) + s;
+                if (x_row(rw)) xpre[s] = xfinal[wo + s * ld];
             }
         }
         // The slots just read are refilled only after this thread's updates have consumed them
@@ -300,10 +325,13 @@ __global__ void __launch_bounds__(NT, MINB)
         // before the next barriers.
 #pragma unroll
         for (int s = 0; s < SPB; ++s) issue_row();
-        issue_rec(k + D, c_iss);
+        issue_rec(slot, t + SPB * D, c_iss, rs);
         cp_async_commit();
-        c_cur = next_colour(c_cur, SPB);
         c_iss = next_colour(c_iss, SPB);
+    };
+    for (int t = L0; t <= t_last; t += 2 * SPB) {
+        super_step(t, 0, rs0);
+        if (t + SPB <= t_last) super_step(t + SPB, 1, rs1);
     }
     cp_async_wait<0>();
 }

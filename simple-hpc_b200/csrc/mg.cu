@@ -8,6 +8,7 @@
 // needs no host round trip. Every kernel is a template on the element type: double gives the
 // reference's bits; float is the mixed-precision mode's V-cycle (sums and norms still in double).
 #include "kernels.hpp"
+#include "blocksum.cuh"
 
 namespace sgpu {
 
@@ -210,6 +211,88 @@ __device__ void cta_coarse_solve(const LevelViewT<T>& L, double* rowbuf, double 
     if (threadIdx.x == 0 && sweeps_out) *sweeps_out = sweeps;
 }
 
+// The float V-cycle's coarse_solve in one warp, with the level (x, b, AP and links, zero ring
+// included) copied to shared memory: the same red-black sweeps, stopping test (||b - A x|| <
+// tol ||b|| or 200 sweeps) and mean removals as cta_coarse_solve, but no block barrier per pass,
+// which on a level of a few cells is most of a pass's cost. Its sums are FP64: each lane adds its
+// cells in order and a fixed xor-shuffle tree combines the lanes (not the reference's row chain,
+// which only the FP64 V-cycle needs). Levels of up to kWarpCoarseCells cells with their ring.
+constexpr int kWarpCoarseCells = 1024;
+
+__device__ void warp_coarse_solve(const LevelViewT<float>& L, double tol, int* sweeps_out) {
+    __shared__ float sx[kWarpCoarseCells], sb[kWarpCoarseCells], sap[kWarpCoarseCells];
+    __shared__ float4 sl[kWarpCoarseCells];
+    const int lane = static_cast<int>(threadIdx.x) & 31;
+    const int S = L.ny + 2, n2 = (L.nx + 2) * S, n = L.nx * L.ny;
+    for (int k = lane; k < n2; k += 32) { // (I, J) in [-1, nx] x [-1, ny]
+        const int I = k / S - 1, J = k % S - 1;
+        const int q = I * L.stride + J;
+        sx[k] = L.x[q];
+        const bool in = I >= 0 && I < L.nx && J >= 0 && J < L.ny;
+        sb[k] = in ? L.b[q] : 0.0f;
+        sap[k] = in ? L.AP[q] : 0.0f;
+        if (in) {
+            const Links<float> a = links(L, q);
+            sl[k] = make_float4(a.e, a.w, a.n, a.s);
+        }
+    }
+    __syncwarp();
+    // cell k of the interior (row-major) at smem index (I + 1) * S + J + 1
+    auto at = [&](int k) {
+        const int I = k / L.ny;
+        return (I + 1) * S + (k - I * L.ny) + 1;
+    };
+    auto sum = [&](auto f) {
+        double a = 0.0;
+        for (int k = lane; k < n; k += 32) a += f(at(k));
+        return warp_sum(a);
+    };
+    auto smooth = [&](int colour) {
+        for (int k = lane; k < n; k += 32) {
+            const int I = k / L.ny, J = k - I * L.ny;
+            if (((I + J) & 1) != colour) continue;
+            const int q = (I + 1) * S + J + 1;
+            const float4 a = sl[q];
+            sx[q] = rb_value(sb[q], a.x * sx[q + 1] + a.y * sx[q - 1] + a.w * sx[q + S] + a.z * sx[q - S], sap[q]);
+        }
+        __syncwarp();
+    };
+    const double dn = static_cast<double>(L.nx) * L.ny;
+    const double mb = sum([&](int q) { return static_cast<double>(sb[q]); }) / dn;
+    for (int k = lane; k < n; k += 32) {
+        const int q = at(k);
+        sb[q] = static_cast<float>(sb[q] - mb);
+    }
+    __syncwarp();
+    const double bb = sum([&](int q) {
+        const double v = sb[q];
+        return v * v;
+    });
+    int sweeps = 0;
+    if (bb > 0.0) {
+        const double bn = sqrt(bb);
+        while (sweeps < 200) {
+            smooth(0);
+            smooth(1);
+            ++sweeps;
+            const double rr = sum([&](int q) {
+                const float4 a = sl[q];
+                const double r = sb[q] - (sap[q] * sx[q] - (a.x * sx[q + 1] + a.y * sx[q - 1] + a.w * sx[q + S] +
+                                                            a.z * sx[q - S]));
+                return r * r;
+            });
+            if (sqrt(rr) < tol * bn) break;
+        }
+    }
+    const double mx = sum([&](int q) { return static_cast<double>(sx[q]); }) / dn;
+    for (int k = lane; k < n; k += 32) {
+        const int I = k / L.ny, J = k - I * L.ny, q = (I + 1) * S + J + 1;
+        L.x[I * L.stride + J] = static_cast<float>(sx[q] - mx);
+        L.b[I * L.stride + J] = sb[q];
+    }
+    if (lane == 0 && sweeps_out) *sweeps_out = sweeps;
+}
+
 template <class T>
 __global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(LevelViewT<T> L, double* rowbuf,
                                                               double tol, int* sweeps_out) {
@@ -231,7 +314,16 @@ __global__ void __launch_bounds__(kCoarseThreads)
         cta_residual(lv.L[l]);
         cta_restrict(lv.L[l], lv.L[l + 1]);
     }
-    cta_coarse_solve(lv.L[nl - 1], rowbuf, tol, sweeps_out);
+    bool warp_solve = false;
+    if constexpr (sizeof(T) == 4)
+        warp_solve = (lv.L[nl - 1].nx + 2) * (lv.L[nl - 1].ny + 2) <= kWarpCoarseCells;
+    if (warp_solve) {
+        if constexpr (sizeof(T) == 4)
+            if (threadIdx.x < 32) warp_coarse_solve(lv.L[nl - 1], tol, sweeps_out);
+        __syncthreads();
+    } else {
+        cta_coarse_solve(lv.L[nl - 1], rowbuf, tol, sweeps_out);
+    }
     for (int l = nl - 2; l >= first; --l) {
         cta_prolong(lv.L[l + 1], lv.L[l], omega);
         for (int s = 0; s < post; ++s) {

@@ -382,10 +382,14 @@ __global__ void __launch_bounds__(256)
 __global__ void k_b_to_f32(DevParams p, const double* __restrict__ bfield, const double* __restrict__ sum_b,
                            LevelView32 L0) {
     const int J = static_cast<int>(blockIdx.x * 32 + threadIdx.x);
-    const int I = static_cast<int>(blockIdx.y * 8 + threadIdx.y);
-    if (I >= p.NX || J >= p.NY) return;
+    const int I0 = static_cast<int>(blockIdx.y * kTileRows + threadIdx.y);
+    if (J >= p.NY) return;
     const double m = *sum_b / (static_cast<double>(p.NX) * p.NY);
-    L0.b[I * L0.stride + J] = static_cast<float>(bfield[ix(p, p.H + I, p.H + 1 + J)] - m);
+#pragma unroll
+    for (int k = 0; k < kRowsPerThread; ++k) { // rows I0, I0 + 8, ...: more loads in flight per thread
+        const int I = I0 + 8 * k;
+        if (I < p.NX) L0.b[I * L0.stride + J] = static_cast<float>(bfield[ix(p, p.H + I, p.H + 1 + J)] - m);
+    }
 }
 
 // correct (pressure.cpp:136-157) in FP64 from the FP32 p' minus its FP64 mean; also stores that
@@ -488,7 +492,7 @@ int mixed_partials(const DevParams& p) {
 
 void launch_b_to_f32(const DevParams& p, const double* bfield, const double* sum_b,
                      const LevelView32& L0, cudaStream_t st) {
-    const dim3 grid((p.NY + 31) / 32, (p.NX + 7) / 8);
+    const dim3 grid((p.NY + 31) / 32, (p.NX + kTileRows - 1) / kTileRows);
     k_b_to_f32<<<grid, dim3(32, 8), 0, st>>>(p, bfield, sum_b, L0);
     SGPU_LAUNCH();
 }

@@ -399,8 +399,13 @@ struct Solver {
         for (std::size_t l = 1; l < lv32.size(); ++l) launch_mg_build<float>(lv32[l - 1], lv32[l], st);
         launch_b_to_f32(dp, w.b, sums + 25, lv32[0], st);
         const LevelView32& L0 = lv32[0];
-        SGPU_CUDA(cudaMemsetAsync(L0.x - (L0.stride + 1), 0,
-                                  sizeof(float) * (L0.nx + 2) * static_cast<std::size_t>(L0.stride), st));
+        // p' starts from zero. The streaming level kernels need no cleared array for that: the
+        // first cycle's k_mg_down does not read x (x_zero), a warm start writes every interior cell,
+        // and the zero ring is never written after allocation. Level 0 inside the tail kernel
+        // (a grid of mg_tail = 0) reads x, so it is cleared there.
+        if (mg_tail == 0)
+            SGPU_CUDA(cudaMemsetAsync(L0.x - (L0.stride + 1), 0,
+                                      sizeof(float) * (L0.nx + 2) * static_cast<std::size_t>(L0.stride), st));
         const bool guess = apply_warm_start(L0);
         auto vcycle32 = [&](bool x_zero) {
             for (int l = 0; l < mg_tail; ++l)

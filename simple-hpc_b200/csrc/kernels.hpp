@@ -159,8 +159,12 @@ int corr_blocks_per_sm(int ncol);
 // the far links {AEE AWW ANN ASS}, and {1/AP, R}; 40 bytes per cell. They are stored by sweep step:
 // the record of cell (i, j) of colour c (c = (i + 3j) mod 5 for five colours, (i + j) mod 2 for
 // two) sits at (i + 2c) * pitch + j, so the cells the streaming sweep updates at one step, one per
-// column, are contiguous. The arrays have kRecExtraRows rows more than the fields.
+// column, are contiguous. The arrays have kRecExtraRows rows more than the fields, and are
+// allocated with kRecFrontCols records before element 0 and kRecBackCols after the last row: the
+// correction sweep copies whole step-row segments of its CTA's columns, which reach up to 2 x the
+// colour count before column 0 and past the last column.
 constexpr int kRecExtraRows = 8;
+constexpr int kRecFrontCols = 16, kRecBackCols = 256;
 struct MomRec32 {
     float4* near_links;
     float4* far_links;
@@ -172,9 +176,11 @@ int launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x,
                           const double* pf, double* AP, double* part, MomRec32 rec, cudaStream_t st);
 // One FP32 multicolour correction sweep e_in -> e_out (e_zero: e_in is zero and not read).
 // xfinal != null: the last sweep of a component adds e to the FP64 field x over the update range
-// (x += e in FP64) instead of writing eout.
+// (x += e in FP64) instead of writing eout. *err (a device word) gets a nonzero bit if one of the
+// kernel's bounded waits for its record copies gave up.
 void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, float* eout,
-                       MomRec32 rec, bool e_zero, int seg_rows, cudaStream_t st, double* xfinal = nullptr);
+                       MomRec32 rec, bool e_zero, int seg_rows, unsigned* err, cudaStream_t st,
+                       double* xfinal = nullptr);
 // assemble_p with the FP32 level-0 operator; per block one partial sum of |b| into part[k] and one
 // of b into part[n + k] (n = the returned number of blocks).
 int launch_assemble_p_mixed(const DevParams& p, const double* APU, const double* APV, const double* u,

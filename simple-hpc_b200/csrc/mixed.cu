@@ -21,6 +21,7 @@
 #include "blocksum.cuh"
 #include "stencil.cuh"
 
+#include <cstdint>
 #include <cstdlib>
 
 namespace sgpu {
@@ -131,15 +132,52 @@ __global__ void __launch_bounds__(256, 4)
 }
 
 constexpr int kRing = 32;    // rows of the e ring (a power of two)
-constexpr int kRecAhead = 2; // super-steps whose records are in flight (cp.async into shared memory)
+constexpr int kRecAhead = 2; // record slots: super-steps whose records are in flight
+constexpr int kSpinLimit = 1 << 20; // bounded mbarrier waits (a give-up is reported, never a hang)
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(b)) : "memory");
+}
+// Arrive (count one) and expect `bytes` of bulk copies to complete on b.
+__device__ __forceinline__ void mbar_arrive_expect(unsigned long long* b, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(b)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long* b, unsigned parity) {
+    unsigned done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done)
+                 : "r"(smem_u32(b)), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+// Wait for phase `parity` of b to complete, at most kSpinLimit polls; a give-up sets *err.
+__device__ __forceinline__ void mbar_wait(unsigned long long* b, unsigned parity, unsigned* err) {
+    for (int it = 0; !mbar_test(b, parity); ++it)
+        if (it >= kSpinLimit) {
+            atomicOr(err, 1u);
+            return;
+        }
+}
+// One bulk copy (TMA, no tensor map) of `bytes` from global to this CTA's shared memory, completing
+// on mbarrier b. Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* b) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(b))
+                 : "memory");
 }
 
 // Shared memory of k_corr_stream: the e ring (kRing rows of NT floats), then kRecAhead x SPB record
-// slots of NT cells each in three arrays (near links, far links for five colours, {1/AP, R}).
+// slots, each one step row of NT cells in three arrays (near links, far links for five colours,
+// {1/AP, R}).
 template <int NCOL, int NT> struct CorrSmem {
     static constexpr int SPB = NCOL == 5 ? 2 : 1;
     static constexpr int slots = kRecAhead * SPB;
@@ -148,33 +186,38 @@ template <int NCOL, int NT> struct CorrSmem {
     static constexpr int far = NCOL == 5 ? slots * NT * 16 : 0;
     static constexpr int diag = slots * NT * 8;
     static constexpr int bytes = ring + near + far + diag;
+    // bytes one step row of records brings in
+    static constexpr unsigned row_bytes = NT * (NCOL == 5 ? 40 : 24);
 };
 
 // One FP32 multicolour correction sweep e_in -> e_out from the stored records; the time-skewed
 // streaming of k_mom_stream (fused.cu): cell (r, j) of colour c at step r + 2c, SPB steps per
 // barrier (two for five colours), strip halo 2 per colour.
-// Pipeline: super-step k (steps L0 + SPB k ..) waits for the copy group committed kRecAhead
-// super-steps earlier, which holds the records of its cells and e rows far enough ahead; after its
-// updates each thread issues, as one group, the next SPB e rows and the records of super-step
-// k + kRecAhead into the slots it has just read (its own: no other thread touches them). Keeping
-// the records out of registers lets kRecAhead x 20 KB of them per CTA be in flight.
-// e_zero: e_in is zero and is not read.
+// Records are stored by step (MomRec32), so the records of one step for the CTA's NT columns are
+// three contiguous row segments. Thread 0 fetches them for a whole super-step with bulk copies (TMA)
+// into one of kRecAhead slot sets, completing on that set's `full` mbarrier; every thread arrives
+// on its `empty` mbarrier once it has read the set, and thread 0 refills the set for the super-step
+// kRecAhead later only after that. The e rows are per-thread cp.async copies, one group per
+// super-step, waited for kRecAhead super-steps later. Waits are bounded (kSpinLimit); a give-up
+// sets *err, which the host reports. e_zero: e_in is zero and is not read.
 template <int NCOL, bool V, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     k_corr_stream(DevParams p, const float* __restrict__ ein, float* __restrict__ eout,
-                  MomRec32 rec, int e_zero, int seg_rows, double* __restrict__ xfinal) {
+                  MomRec32 rec, int e_zero, int seg_rows, double* __restrict__ xfinal, unsigned* err) {
     using S = CorrSmem<NCOL, NT>;
     constexpr int SPB = S::SPB;
     constexpr int HC = 2 * NCOL;
     constexpr int W = NT - 2 * HC;
     constexpr int D = kRecAhead;
     constexpr int E0 = SPB * D + 2; // e rows issued before the first super-step
+    static_assert(D == 2, "the step loop is unrolled over the two record slot sets");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* ring_mem = reinterpret_cast<float*>(smem_raw);
     float4* s_near = reinterpret_cast<float4*>(smem_raw + S::ring);
     float4* s_far = reinterpret_cast<float4*>(smem_raw + S::ring + S::near);
     float2* s_diag = reinterpret_cast<float2*>(smem_raw + S::ring + S::near + S::far);
     __shared__ int s_rmin[NCOL], s_rmax[NCOL];
+    __shared__ __align__(8) unsigned long long full[D], empty[D];
     const int tid = threadIdx.x;
     const int j0 = blockIdx.x * W;
     const int C0 = j0 - HC, C1 = j0 + W + HC;
@@ -197,6 +240,13 @@ __global__ void __launch_bounds__(NT, MINB)
         s_rmin[c] = lo;
         s_rmax[c] = hi;
     }
+    if (tid == 0) {
+        for (int d = 0; d < D; ++d) {
+            mbar_init(&full[d], 1);
+            mbar_init(&empty[d], NT);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
     unsigned colmask = 0;
     {
         const int ju0 = H + 1, ju1 = V ? p.NY + H : p.NY + H - 1;
@@ -210,12 +260,9 @@ __global__ void __launch_bounds__(NT, MINB)
     }
     const float relax = static_cast<float>(V ? p.av : p.au);
     float* ringc = ring_mem + tid;
-    static_assert(D == 2, "the step loop is unrolled over the two record slots");
-    // Running offsets: the next e row to issue, the step row of the next records to issue, and the
-    // row the next super-step writes out.
+    // Running offsets: the next e row to issue and the row the next super-step writes out.
     int next = L0;
     int eo = col + L0 * ld;
-    int ro = col + L0 * ld;
     int wo = col + (L0 - 2 * NCOL + 1 - (SPB - 1)) * ld;
     auto issue_row = [&]() {
         if (next < L1 && col_in) {
@@ -233,24 +280,24 @@ __global__ void __launch_bounds__(NT, MINB)
     auto next_colour = [&](int c, int steps) {
         return NCOL == 5 ? (c + 2 * steps) % 5 : (c + steps) & 1;
     };
-    // The records of the super-step whose first step is t (first colour c0k) into record slot
-    // `slot`; rs[s] keeps the row of its s-th cell (-1: none) for the update SPB * D steps later.
-    auto issue_rec = [&](int slot, int t, int c0k, int (&rs)[SPB]) {
+    // Thread 0: the records of the super-step whose first step is t into slot set `slot`. Step
+    // rows past the arrays' end hold no cell and are not fetched.
+    const int rec_rows = p.nrows + kRecExtraRows;
+    auto fill = [&](int slot, int t) {
+        unsigned bytes = 0;
+#pragma unroll
+        for (int s = 0; s < SPB; ++s)
+            if (t + s < rec_rows) bytes += S::row_bytes;
+        mbar_arrive_expect(&full[slot], bytes);
 #pragma unroll
         for (int s = 0; s < SPB; ++s) {
-            int r;
-            if (step_cell(next_colour(c0k, s), t + s, r)) {
-                const int q = (slot * SPB + s) * NT + tid;
-                const int o = ro + s * ld; // records are stored by step: a warp reads one row
-                cp_async16(s_near + q, rec.near_links + o);
-                if (NCOL == 5) cp_async16(s_far + q, rec.far_links + o);
-                cp_async(s_diag + q, rec.diag + o);
-                rs[s] = r;
-            } else {
-                rs[s] = -1;
-            }
+            if (t + s >= rec_rows) continue;
+            const std::ptrdiff_t o = static_cast<std::ptrdiff_t>(t + s) * ld + C0;
+            const int q = (slot * SPB + s) * NT;
+            bulk_load(s_near + q, rec.near_links + o, NT * 16, &full[slot]);
+            if (NCOL == 5) bulk_load(s_far + q, rec.far_links + o, NT * 16, &full[slot]);
+            bulk_load(s_diag + q, rec.diag + o, NT * 8, &full[slot]);
         }
-        ro += SPB * ld;
     };
     auto update = [&](int r, int q) {
         const float4 a = s_near[q];
@@ -277,31 +324,34 @@ __global__ void __launch_bounds__(NT, MINB)
     };
     double xpre[SPB];
 
-    __syncthreads(); // s_rmin / s_rmax
+    __syncthreads(); // s_rmin / s_rmax and the initialised mbarriers
     const int c_start = NCOL == 5 ? (2 * L0 + col + 1000) % 5 : (L0 + col + 1000) & 1;
     const int t_last = R1 + 2 * NCOL - 2 + (SPB - 1);
-    // prologue: D groups, the first with E0 e rows; group k holds super-step k's records
-    int c_iss = c_start;
-    int rs0[SPB], rs1[SPB];
+    // prologue: D e-row groups, the first with E0 rows; the records of super-steps 0 .. D-1
     for (int i = 0; i < E0; ++i) issue_row();
-    issue_rec(0, L0, c_iss, rs0);
     cp_async_commit();
-    c_iss = next_colour(c_iss, SPB);
-    issue_rec(1, L0 + SPB, c_iss, rs1);
     cp_async_commit();
-    c_iss = next_colour(c_iss, SPB);
+    if (tid == 0) {
+        fill(0, L0);
+        if (L0 + SPB <= t_last) fill(1, L0 + SPB);
+    }
 #pragma unroll
     for (int s = 0; s < SPB; ++s) {
         const int rw = L0 - 2 * NCOL + 1 - (SPB - 1) + s;
         xpre[s] = (xfinal && x_row(rw)) ? xfinal[wo + s * ld] : 0.0;
     }
 
-    auto super_step = [&](int t, int slot, int (&rs)[SPB]) {
-        cp_async_wait<D - 1>(); // this thread's group of this super-step has landed
-        __syncthreads();         // ... and everyone's
+    int c_cur = c_start;
+    auto super_step = [&](int t, int slot, unsigned parity) {
+        cp_async_wait<D - 1>();            // this thread's e rows for this super-step have landed
+        mbar_wait(&full[slot], parity, err); // the slot set's records have landed
+        __syncthreads();                   // ... and everyone's e rows
 #pragma unroll
-        for (int s = 0; s < SPB; ++s)
-            if (rs[s] >= 0) update(rs[s], (slot * SPB + s) * NT + tid);
+        for (int s = 0; s < SPB; ++s) {
+            int r;
+            if (step_cell(next_colour(c_cur, s), t + s, r)) update(r, (slot * SPB + s) * NT + tid);
+        }
+        mbar_arrive(&empty[slot]); // this thread is done with the slot set
 #pragma unroll
         for (int s = 0; s < SPB; ++s) {
             const int rw = t - 2 * NCOL + 1 - (SPB - 1) + s;
@@ -320,18 +370,23 @@ __global__ void __launch_bounds__(NT, MINB)
                 if (x_row(rw)) xpre[s] = xfinal[wo + s * ld];
             }
         }
-        // The slots just read are refilled only after this thread's updates have consumed them
-        // (each update's store depends on its record loads); e rows land in ring rows no one reads
-        // before the next barriers.
+        // e rows land in ring rows no one reads before the next barriers
 #pragma unroll
         for (int s = 0; s < SPB; ++s) issue_row();
-        issue_rec(slot, t + SPB * D, c_iss, rs);
         cp_async_commit();
-        c_iss = next_colour(c_iss, SPB);
+        c_cur = next_colour(c_cur, SPB);
+        // Thread 0 refills the slot set for the super-step D later once every thread has read it;
+        // a super-step past the last is not fetched, so no copy is in flight when the CTA exits.
+        if (tid == 0 && t + SPB * D <= t_last) {
+            mbar_wait(&empty[slot], parity, err);
+            fill(slot, t + SPB * D);
+        }
     };
+    unsigned parity = 0;
     for (int t = L0; t <= t_last; t += 2 * SPB) {
-        super_step(t, 0, rs0);
-        if (t + SPB <= t_last) super_step(t + SPB, 1, rs1);
+        super_step(t, 0, parity);
+        if (t + SPB <= t_last) super_step(t + SPB, 1, parity);
+        parity ^= 1u;
     }
     cp_async_wait<0>();
 }
@@ -445,20 +500,27 @@ int corr_minb() {
 
 template <int NCOL, bool V, int NT, int MINB>
 void launch_corr(const DevParams& p, const float* ein, float* eout, MomRec32 rec, bool e_zero,
-                 int seg_rows, double* xfinal, cudaStream_t st) {
+                 int seg_rows, double* xfinal, unsigned* err, cudaStream_t st) {
+    // The bulk copies start at record (t * pitch + first column): 16-byte aligned for every step
+    // row t and CTA when the arrays are and the pitch and first columns are even (the strips
+    // start at multiples of NT - 4 NCOL, minus 2 NCOL).
+    const auto misaligned = [](const void* q) { return (reinterpret_cast<std::uintptr_t>(q) & 15u) != 0; };
+    if ((p.pitch & 1) || misaligned(rec.near_links) || misaligned(rec.far_links) || misaligned(rec.diag) || !err)
+        throw Error(SGPU_E_INVALID, "correction sweep: records not aligned for bulk copies");
     constexpr int W = NT - 4 * NCOL;
+    static_assert(W % 2 == 0 && (2 * NCOL) % 2 == 0, "strip starts must be even");
     const dim3 grid((p.ncols + W - 1) / W, (p.nrows + seg_rows - 1) / seg_rows);
     constexpr int smem = CorrSmem<NCOL, NT>::bytes;
     k_corr_stream<NCOL, V, NT, MINB><<<grid, NT, smem, st>>>(p, ein, eout, rec, e_zero ? 1 : 0, seg_rows,
-                                                              xfinal);
+                                                              xfinal, err);
     SGPU_LAUNCH();
 }
 
 template <int NCOL, bool V>
 void launch_corr_m(const DevParams& p, const float* ein, float* eout, MomRec32 rec, bool e_zero,
-                   int seg_rows, double* xfinal, cudaStream_t st) {
-    if (corr_minb() == 4) launch_corr<NCOL, V, 256, 4>(p, ein, eout, rec, e_zero, seg_rows, xfinal, st);
-    else launch_corr<NCOL, V, 256, 3>(p, ein, eout, rec, e_zero, seg_rows, xfinal, st);
+                   int seg_rows, double* xfinal, unsigned* err, cudaStream_t st) {
+    if (corr_minb() == 4) launch_corr<NCOL, V, 256, 4>(p, ein, eout, rec, e_zero, seg_rows, xfinal, err, st);
+    else launch_corr<NCOL, V, 256, 3>(p, ein, eout, rec, e_zero, seg_rows, xfinal, err, st);
 }
 
 } // namespace
@@ -514,13 +576,14 @@ void launch_correct_mixed(const DevParams& p, const LevelView32& L0, const doubl
 
 #else
 void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, float* eout,
-                       MomRec32 rec, bool e_zero, int seg_rows, cudaStream_t st, double* xfinal) {
+                       MomRec32 rec, bool e_zero, int seg_rows, unsigned* err, cudaStream_t st,
+                       double* xfinal) {
     if (p.ncol == 5) {
-        if (v_component) launch_corr_m<5, true>(p, ein, eout, rec, e_zero, seg_rows, xfinal, st);
-        else launch_corr_m<5, false>(p, ein, eout, rec, e_zero, seg_rows, xfinal, st);
+        if (v_component) launch_corr_m<5, true>(p, ein, eout, rec, e_zero, seg_rows, xfinal, err, st);
+        else launch_corr_m<5, false>(p, ein, eout, rec, e_zero, seg_rows, xfinal, err, st);
     } else {
-        if (v_component) launch_corr_m<2, true>(p, ein, eout, rec, e_zero, seg_rows, xfinal, st);
-        else launch_corr_m<2, false>(p, ein, eout, rec, e_zero, seg_rows, xfinal, st);
+        if (v_component) launch_corr_m<2, true>(p, ein, eout, rec, e_zero, seg_rows, xfinal, err, st);
+        else launch_corr_m<2, false>(p, ein, eout, rec, e_zero, seg_rows, xfinal, err, st);
     }
 }
 

@@ -357,6 +357,19 @@ struct Solver {
         p_links_stale = false;
     }
     MomRec32 rec32{};                 // per-cell FP32 records: coefficients, 1/AP, R
+    unsigned* corr_err = nullptr;     // device word: a correction sweep's bounded wait gave up
+    // Raises SGPU_E_TIMEOUT if a correction sweep since the last check gave up waiting for its
+    // record copies (its results are then not to be trusted); clears the word.
+    void check_pipeline() {
+        if (!corr_err) return;
+        unsigned h = 0;
+        SGPU_CUDA(cudaMemcpyAsync(&h, corr_err, sizeof h, cudaMemcpyDeviceToHost, st));
+        sync();
+        if (h) {
+            SGPU_CUDA(cudaMemsetAsync(corr_err, 0, sizeof h, st));
+            throw Error(SGPU_E_TIMEOUT, "correction sweep: a bounded wait for its record copies ran out");
+        }
+    }
     double* part = nullptr;           // per-block partial sums of the FP64 tree sums
     float* e32[2] = {nullptr, nullptr}; // correction ping-pong
     std::vector<LevelView32> lv32;    // FP32 multigrid hierarchy (level 0: the p' operator)
@@ -379,7 +392,7 @@ struct Solver {
         int cur = 0; // e32[cur] holds the current correction (zero before the first sweep)
         sweep_mark(vcomp, 0, n);
         for (int k = 0; k < n; ++k) {
-            launch_corr_sweep(dp, vcomp, e32[cur], e32[1 - cur], rec32, k == 0, seg_rows, st,
+            launch_corr_sweep(dp, vcomp, e32[cur], e32[1 - cur], rec32, k == 0, seg_rows, corr_err, st,
                               k == n - 1 ? x : nullptr); // the last sweep adds e into x
             cur = 1 - cur;
         }
@@ -694,10 +707,12 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
         mixed = true;
         init_mixed_kernels();
         seg_rows = stream_seg_rows(dp, sms, corr_blocks_per_sm(dp.ncol), min_seg);
-        const std::size_t nrec = g.elems() + static_cast<std::size_t>(kRecExtraRows) * g.pitch;
-        rec32.near_links = dalloc<float4>(nrec);
-        rec32.far_links = dalloc<float4>(nrec);
-        rec32.diag = dalloc<float2>(nrec);
+        const std::size_t nrec =
+            g.elems() + static_cast<std::size_t>(kRecExtraRows) * g.pitch + kRecFrontCols + kRecBackCols;
+        rec32.near_links = dalloc<float4>(nrec) + kRecFrontCols;
+        rec32.far_links = dalloc<float4>(nrec) + kRecFrontCols;
+        rec32.diag = dalloc<float2>(nrec) + kRecFrontCols;
+        corr_err = dalloc<unsigned>(1);
         part = dalloc<double>(static_cast<std::size_t>(std::max(mixed_partials(dp), tree_sum_partials(p.NX, p.NY))));
         e32[0] = dalloc<float>(g.elems());
         e32[1] = dalloc<float>(g.elems());
@@ -1395,6 +1410,7 @@ int sgpu_run(sgpu_handle* h, int maxit, double* log, int print_every, sgpu_resul
         const auto t0 = std::chrono::steady_clock::now();
         if (run_graphed(s, maxit, log, print_every, out)) {
             out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            s.check_pipeline();
             if (result) *result = out;
             return;
         }
@@ -1446,6 +1462,7 @@ int sgpu_run(sgpu_handle* h, int maxit, double* log, int print_every, sgpu_resul
         }
         out.seconds =
             std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        s.check_pipeline();
         if (result) *result = out;
     });
 }
@@ -1827,7 +1844,9 @@ int sgpu_batch_autotune(sgpu_batch* b, int* chosen) {
                 SGPU_CUDA(cudaEventCreate(&e0));
                 SGPU_CUDA(cudaEventCreate(&e1));
                 auto sweep = [&](int seg) {
-                    if (sv.mixed) sgpu::launch_corr_sweep(sv.dp, false, sv.e32[0], sv.e32[1], sv.rec32, true, seg, sv.st);
+                    if (sv.mixed)
+                        sgpu::launch_corr_sweep(sv.dp, false, sv.e32[0], sv.e32[1], sv.rec32, true, seg,
+                                                sv.corr_err, sv.st);
                     else sgpu::launch_mom_sweep(sv.dp, false, sv.u, sv.tmp, sv.xF, sv.v, sv.pf, seg, sv.st);
                 };
                 int pick = heur;
@@ -1894,6 +1913,7 @@ int sgpu_batch_run(sgpu_batch* b, int maxit, int log_cap, double* seconds) {
             }
             b->g->count(rounds, total); // cavities differ in kernels per iteration: an average
         }
+        for (auto& p : b->s) p->check_pipeline();
         float ms = 0.0f;
         SGPU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
         cudaEventDestroy(e0);

@@ -211,47 +211,56 @@ __device__ void cta_coarse_solve(const LevelViewT<T>& L, double* rowbuf, double 
     if (threadIdx.x == 0 && sweeps_out) *sweeps_out = sweeps;
 }
 
-// The float V-cycle's coarse_solve in one warp, with the level (x, b, AP and links, zero ring
-// included) copied to shared memory: the same red-black sweeps, stopping test (||b - A x|| <
-// tol ||b|| or 200 sweeps) and mean removals as cta_coarse_solve, but no block barrier per pass,
-// which on a level of a few cells is most of a pass's cost. Its sums are FP64: each lane adds its
-// cells in order and a fixed xor-shuffle tree combines the lanes (not the reference's row chain,
-// which only the FP64 V-cycle needs). Levels of up to kWarpCoarseCells cells with their ring.
-constexpr int kWarpCoarseCells = 1024;
+// A float level held in shared memory: (nx + 2) x (ny + 2) cells with the zero ring, row stride S,
+// interior cell (I, J) at index (I + 1) * S + J + 1; links {e, w, n, s}, AP, b and x per cell.
+struct SLevel {
+    int nx, ny, S;
+    float4* l4;
+    float *x, *b, *ap;
+    __device__ int at(int I, int J) const { return (I + 1) * S + J + 1; }
+};
+// Bytes of one SLevel block (links first, 16-byte aligned).
+__host__ __device__ inline int slevel_bytes(int nx, int ny) {
+    const int n2 = (nx + 2) * (ny + 2);
+    return ((n2 * 28) + 15) / 16 * 16;
+}
+__device__ inline SLevel slevel_at(unsigned char* base, int nx, int ny) {
+    const int n2 = (nx + 2) * (ny + 2);
+    SLevel v;
+    v.nx = nx;
+    v.ny = ny;
+    v.S = ny + 2;
+    v.l4 = reinterpret_cast<float4*>(base);
+    v.x = reinterpret_cast<float*>(base + 16 * n2);
+    v.b = v.x + n2;
+    v.ap = v.b + n2;
+    return v;
+}
 
-__device__ void warp_coarse_solve(const LevelViewT<float>& L, double tol, int* sweeps_out) {
-    __shared__ float sx[kWarpCoarseCells], sb[kWarpCoarseCells], sap[kWarpCoarseCells];
-    __shared__ float4 sl[kWarpCoarseCells];
+// The float V-cycle's coarse_solve in one warp on a shared-memory level: the same red-black
+// sweeps, stopping test (||b - A x|| < tol ||b|| or 200 sweeps) and mean removals as
+// cta_coarse_solve, but no block barrier per pass, which on a level of a few cells is most of a
+// pass's cost. Its sums are FP64: each lane adds its cells in order and a fixed xor-shuffle tree
+// combines the lanes (not the reference's row chain, which only the FP64 V-cycle needs).
+__device__ void warp_coarse_core(const SLevel& L, double tol, int* sweeps_out) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
-    const int S = L.ny + 2, n2 = (L.nx + 2) * S, n = L.nx * L.ny;
-    for (int k = lane; k < n2; k += 32) { // (I, J) in [-1, nx] x [-1, ny]
-        const int I = k / S - 1, J = k % S - 1;
-        const int q = I * L.stride + J;
-        sx[k] = L.x[q];
-        const bool in = I >= 0 && I < L.nx && J >= 0 && J < L.ny;
-        sb[k] = in ? L.b[q] : 0.0f;
-        sap[k] = in ? L.AP[q] : 0.0f;
-        if (in) {
-            const Links<float> a = links(L, q);
-            sl[k] = make_float4(a.e, a.w, a.n, a.s);
-        }
-    }
-    __syncwarp();
-    // cell k of the interior (row-major) at smem index (I + 1) * S + J + 1
+    const int n = L.nx * L.ny, S = L.S;
     auto at = [&](int k) {
         const int I = k / L.ny;
-        return (I + 1) * S + (k - I * L.ny) + 1;
+        return L.at(I, k - I * L.ny);
     };
     auto sum = [&](auto f) {
         double a = 0.0;
         for (int k = lane; k < n; k += 32) a += f(at(k));
         return warp_sum(a);
     };
+    float *sx = L.x, *sb = L.b, *sap = L.ap;
+    const float4* sl = L.l4;
     auto smooth = [&](int colour) {
         for (int k = lane; k < n; k += 32) {
             const int I = k / L.ny, J = k - I * L.ny;
             if (((I + J) & 1) != colour) continue;
-            const int q = (I + 1) * S + J + 1;
+            const int q = L.at(I, J);
             const float4 a = sl[q];
             sx[q] = rb_value(sb[q], a.x * sx[q + 1] + a.y * sx[q - 1] + a.w * sx[q + S] + a.z * sx[q - S], sap[q]);
         }
@@ -286,11 +295,154 @@ __device__ void warp_coarse_solve(const LevelViewT<float>& L, double tol, int* s
     }
     const double mx = sum([&](int q) { return static_cast<double>(sx[q]); }) / dn;
     for (int k = lane; k < n; k += 32) {
-        const int I = k / L.ny, J = k - I * L.ny, q = (I + 1) * S + J + 1;
-        L.x[I * L.stride + J] = static_cast<float>(sx[q] - mx);
-        L.b[I * L.stride + J] = sb[q];
+        const int q = at(k);
+        sx[q] = static_cast<float>(sx[q] - mx);
     }
+    __syncwarp();
     if (lane == 0 && sweeps_out) *sweeps_out = sweeps;
+}
+
+// Global level L into the shared level s (links, AP; b and x when `values`; zero elsewhere,
+// the ring included), by all threads of the block.
+__device__ void slevel_load(const LevelViewT<float>& L, const SLevel& s, bool values) {
+    const int n2 = (L.nx + 2) * s.S;
+    for (int k = threadIdx.x; k < n2; k += blockDim.x) {
+        const int I = k / s.S - 1, J = k % s.S - 1;
+        const bool in = I >= 0 && I < L.nx && J >= 0 && J < L.ny;
+        const int q = I * L.stride + J;
+        float4 l = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (in) {
+            const Links<float> a = links(L, q);
+            l = make_float4(a.e, a.w, a.n, a.s);
+        }
+        s.l4[k] = l;
+        s.ap[k] = in ? L.AP[q] : 0.0f;
+        s.b[k] = (in && values) ? L.b[q] : 0.0f;
+        s.x[k] = (in && values) ? L.x[q] : 0.0f;
+    }
+}
+// The interior x and b of the shared level back to L.
+__device__ void slevel_store(const LevelViewT<float>& L, const SLevel& s) {
+    const int n = L.nx * L.ny;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const int I = k / L.ny, J = k - I * L.ny;
+        L.x[I * L.stride + J] = s.x[s.at(I, J)];
+        L.b[I * L.stride + J] = s.b[s.at(I, J)];
+    }
+}
+
+// The coarsest level of the float V-cycle in a global-memory tail: copied to shared memory, solved
+// by one warp, copied back. Levels of up to kWarpCoarseCells cells with their ring.
+constexpr int kWarpCoarseCells = 1024;
+
+__device__ void warp_coarse_solve(const LevelViewT<float>& L, double tol, int* sweeps_out) {
+    __shared__ __align__(16) unsigned char sm[kWarpCoarseCells * 28];
+    const SLevel s = slevel_at(sm, L.nx, L.ny);
+    if (threadIdx.x < 32) {
+        const int S = s.S, n2 = (L.nx + 2) * S;
+        for (int k = threadIdx.x; k < n2; k += 32) {
+            const int I = k / S - 1, J = k % S - 1;
+            const bool in = I >= 0 && I < L.nx && J >= 0 && J < L.ny;
+            const int q = I * L.stride + J;
+            float4 l = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (in) {
+                const Links<float> a = links(L, q);
+                l = make_float4(a.e, a.w, a.n, a.s);
+            }
+            s.l4[k] = l;
+            s.ap[k] = in ? L.AP[q] : 0.0f;
+            s.b[k] = in ? L.b[q] : 0.0f;
+            s.x[k] = in ? L.x[q] : 0.0f;
+        }
+        __syncwarp();
+        warp_coarse_core(s, tol, sweeps_out);
+        const int n = L.nx * L.ny;
+        for (int k = threadIdx.x; k < n; k += 32) {
+            const int I = k / L.ny, J = k - I * L.ny;
+            L.x[I * L.stride + J] = s.x[s.at(I, J)];
+            L.b[I * L.stride + J] = s.b[s.at(I, J)];
+        }
+    }
+}
+
+// ---- the float tail with every level in shared memory ----
+
+// Byte offset of each tail level's SLevel block in dynamic shared memory, and the total.
+struct TailSmem {
+    int off[24];
+    int bytes;
+};
+
+// One colour of smooth on a shared level: warps take rows, lanes the colour's cells of a row.
+__device__ void s_smooth(const SLevel& L, int colour) {
+    const int w = static_cast<int>(threadIdx.x) >> 5, lane = static_cast<int>(threadIdx.x) & 31;
+    const int nw = static_cast<int>(blockDim.x) >> 5, S = L.S;
+    for (int I = w; I < L.nx; I += nw)
+        for (int J = ((I + colour) & 1) + 2 * lane; J < L.ny; J += 64) {
+            const int q = L.at(I, J);
+            const float4 a = L.l4[q];
+            L.x[q] = rb_value(L.b[q], a.x * L.x[q + 1] + a.y * L.x[q - 1] + a.w * L.x[q + S] + a.z * L.x[q - S],
+                              L.ap[q]);
+        }
+    __syncthreads();
+}
+// Residual of F (multigrid.cpp:84-85 form) restricted 2x2 into C.b (multigrid.cpp:90-103), C.x = 0.
+__device__ void s_residual_restrict(const SLevel& F, const SLevel& C) {
+    const int w = static_cast<int>(threadIdx.x) >> 5, lane = static_cast<int>(threadIdx.x) & 31;
+    const int nw = static_cast<int>(blockDim.x) >> 5, S = F.S;
+    auto r = [&](int q) {
+        const float4 a = F.l4[q];
+        return F.b[q] - (F.ap[q] * F.x[q] - (a.x * F.x[q + 1] + a.y * F.x[q - 1] + a.w * F.x[q + S] + a.z * F.x[q - S]));
+    };
+    for (int I = w; I < C.nx; I += nw)
+        for (int J = lane; J < C.ny; J += 32) {
+            const int f = F.at(2 * I, 2 * J), c = C.at(I, J);
+            C.b[c] = r(f) + r(f + 1) + r(f + S) + r(f + S + 1);
+            C.x[c] = 0.0f;
+        }
+    __syncthreads();
+}
+// prolong (multigrid.cpp:106-116): F.x += omega * C.x of the parent cell.
+__device__ void s_prolong(const SLevel& C, const SLevel& F, float om) {
+    const int w = static_cast<int>(threadIdx.x) >> 5, lane = static_cast<int>(threadIdx.x) & 31;
+    const int nw = static_cast<int>(blockDim.x) >> 5;
+    for (int i = w; i < F.nx; i += nw)
+        for (int j = lane; j < F.ny; j += 32) F.x[F.at(i, j)] += om * C.x[C.at(i >> 1, j >> 1)];
+    __syncthreads();
+}
+
+// Levels [first, nl) of one float V-cycle (mg_vcycle, multigrid.cpp:299-323) in one CTA with every
+// level in shared memory: the links, AP, b and x of the first tail level are read once, the passes
+// run against shared memory with a block barrier between them, and x and b of every tail level are
+// written back at the end. Same passes and per-cell expressions as k_mg_tail.
+__global__ void __launch_bounds__(kCoarseThreads)
+    k_mg_tail_smem(MgLevelsT<float> lv, int first, int pre, int post, double omega, double tol, TailSmem ts,
+                   int* sweeps_out) {
+    extern __shared__ __align__(16) unsigned char tail_sm[];
+    const int nl = lv.n;
+    auto sl = [&](int l) { return slevel_at(tail_sm + ts.off[l], lv.L[l].nx, lv.L[l].ny); };
+    for (int l = first; l < nl; ++l) slevel_load(lv.L[l], sl(l), l == first);
+    __syncthreads();
+    for (int l = first; l + 1 < nl; ++l) {
+        const SLevel L = sl(l);
+        for (int s = 0; s < pre; ++s) {
+            s_smooth(L, 0);
+            s_smooth(L, 1);
+        }
+        s_residual_restrict(L, sl(l + 1));
+    }
+    if (threadIdx.x < 32) warp_coarse_core(sl(nl - 1), tol, sweeps_out);
+    __syncthreads();
+    const float om = static_cast<float>(omega);
+    for (int l = nl - 2; l >= first; --l) {
+        const SLevel L = sl(l);
+        s_prolong(sl(l + 1), L, om);
+        for (int s = 0; s < post; ++s) {
+            s_smooth(L, 0);
+            s_smooth(L, 1);
+        }
+    }
+    for (int l = first; l < nl; ++l) slevel_store(lv.L[l], sl(l));
 }
 
 template <class T>
@@ -335,9 +487,34 @@ __global__ void __launch_bounds__(kCoarseThreads)
 
 } // namespace
 
+// The float tail runs with every level in shared memory when they fit (the 64^2-and-below levels
+// of a square grid take about 170 KB); otherwise, and for double, through global memory.
+constexpr int kTailSmemMax = 200 * 1024;
+
 template <class T>
 void launch_mg_tail(const MgLevelsT<T>& lv, int first, int pre, int post, double omega, double tol,
                     double* rowbuf, int* sweeps_out, cudaStream_t st) {
+    if constexpr (sizeof(T) == 4) {
+        TailSmem ts{};
+        int bytes = 0;
+        for (int l = first; l < lv.n && l < 24; ++l) {
+            ts.off[l] = bytes;
+            bytes += slevel_bytes(lv.L[l].nx, lv.L[l].ny);
+        }
+        ts.bytes = bytes;
+        const int nc = lv.L[lv.n - 1].nx * lv.L[lv.n - 1].ny;
+        if (lv.n <= 24 && bytes <= kTailSmemMax && nc <= kWarpCoarseCells) {
+            static bool attr = false; // per process
+            if (!attr) {
+                SGPU_CUDA(cudaFuncSetAttribute(k_mg_tail_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               kTailSmemMax));
+                attr = true;
+            }
+            k_mg_tail_smem<<<1, kCoarseThreads, bytes, st>>>(lv, first, pre, post, omega, tol, ts, sweeps_out);
+            SGPU_LAUNCH();
+            return;
+        }
+    }
     k_mg_tail<T><<<1, kCoarseThreads, 0, st>>>(lv, first, pre, post, omega, tol, rowbuf, sweeps_out);
     SGPU_LAUNCH();
 }

@@ -220,7 +220,7 @@ struct SLevel {
     __device__ int at(int I, int J) const { return (I + 1) * S + J + 1; }
 };
 // Bytes of one SLevel block (links first, 16-byte aligned).
-__host__ __device__ inline int slevel_bytes(int nx, int ny) {
+[[maybe_unused]] __host__ __device__ inline int slevel_bytes(int nx, int ny) {
     const int n2 = (nx + 2) * (ny + 2);
     return ((n2 * 28) + 15) / 16 * 16;
 }
@@ -335,7 +335,7 @@ __device__ void slevel_store(const LevelViewT<float>& L, const SLevel& s) {
 // by one warp, copied back. Levels of up to kWarpCoarseCells cells with their ring.
 constexpr int kWarpCoarseCells = 1024;
 
-__device__ void warp_coarse_solve(const LevelViewT<float>& L, double tol, int* sweeps_out) {
+[[maybe_unused]] __device__ void warp_coarse_solve(const LevelViewT<float>& L, double tol, int* sweeps_out) {
     __shared__ __align__(16) unsigned char sm[kWarpCoarseCells * 28];
     const SLevel s = slevel_at(sm, L.nx, L.ny);
     if (threadIdx.x < 32) {

@@ -32,6 +32,8 @@ __device__ __forceinline__ std::size_t ix(const DevParams& p, int i, int j) {
     return static_cast<std::size_t>(i) * p.pitch + j;
 }
 
+// The correction sweep (k_corr_stream and its launchers) is built in the FP32 unit only.
+#ifdef SGPU_FLOAT_UNIT
 template <class T> __device__ __forceinline__ void cp_async(T* smem, const T* gmem) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
     if (sizeof(T) == 8)
@@ -43,6 +45,8 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N> __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
+
+#endif
 
 // The tile of one prep block: 32 columns x kTileRows rows, 32 x 8 threads, kTileRows / 8 cells per
 // thread. The block's partial sum (a block tree's tail: one thread adding the warps' sums) is paid
@@ -131,6 +135,7 @@ __global__ void __launch_bounds__(256, 4)
     }
 }
 
+#ifdef SGPU_FLOAT_UNIT
 constexpr int kRing = 32;    // rows of the e ring (a power of two)
 constexpr int kRecAhead = 2; // record slots: super-steps whose records are in flight
 constexpr int kSpinLimit = 1 << 20; // bounded mbarrier waits (a give-up is reported, never a hang)
@@ -391,6 +396,8 @@ __global__ void __launch_bounds__(NT, MINB)
     cp_async_wait<0>();
 }
 
+#endif // SGPU_FLOAT_UNIT
+
 // assemble_p (pressure.cpp:14-54) in FP64 with the p' operator stored in FP32 (level 0 of the FP32
 // hierarchy), and the block's FP64 sums of |b| (res_p) and of b (its mean) into part[block] and
 // part[nblocks + block] (deterministic trees, blocksum.cuh).
@@ -488,6 +495,7 @@ Range update_range(const DevParams& p, bool v) {
     return v ? Range{H + 1, p.NX + H - 1, H + 1, p.NY + H} : Range{H, p.NX + H - 1, H + 1, p.NY + H - 1};
 }
 
+#ifdef SGPU_FLOAT_UNIT
 // Resident CTAs per SM the correction sweep's registers are bounded for: 3, or 4 when
 // SGPU_CORR_MINB=4 (a tuning switch: the arithmetic is the same).
 int corr_minb() {
@@ -522,6 +530,8 @@ void launch_corr_m(const DevParams& p, const float* ein, float* eout, MomRec32 r
     if (corr_minb() == 4) launch_corr<NCOL, V, 256, 4>(p, ein, eout, rec, e_zero, seg_rows, xfinal, err, st);
     else launch_corr<NCOL, V, 256, 3>(p, ein, eout, rec, e_zero, seg_rows, xfinal, err, st);
 }
+
+#endif // SGPU_FLOAT_UNIT
 
 } // namespace
 

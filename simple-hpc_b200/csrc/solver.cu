@@ -231,7 +231,8 @@ struct Solver {
         double* cplane = cells + (vcomp ? plane : 0);
         launch_mom_prep(dp, vcomp, x, oth, pf, xF, AP, cplane, st);
         mark(vcomp ? SGPU_PH_RESIDUAL_V : SGPU_PH_RESIDUAL_U);
-        momentum_sum(vcomp, res, cplane);
+        const bool deferred = defer_sums();
+        if (!deferred) momentum_sum(vcomp, res, cplane, false);
         mark(vcomp ? SGPU_PH_SWEEP_V : SGPU_PH_SWEEP_U);
         const int n = vcomp ? prm.maxit_inner_v : prm.maxit_inner_u;
         double* in = x;
@@ -243,38 +244,49 @@ struct Solver {
         }
         sweep_mark(vcomp, 1, n);
         if (in != x) launch_copy(in, x, g.elems(), st);
+        if (deferred) momentum_sum(vcomp, res, cplane, true); // beside the next prep / assemble_p
     }
 
-    // res_u / res_v: the ordered sum of |R| over the residual range, on the solver's stream. The sums
-    // feed only the stopping test, and SGPU_SIDE_SUMS=1 runs them on a side stream beside the sweeps
-    // (lean sum kernel; u and v |R| in separate planes; joined before assemble_p). Measured at
-    // 4096^2 that is slower: a co-resident sum CTA stops the sweep's one-wave grid of 3 CTAs/SM
-    // from fitting (sweeps 1.9 -> 2.7 ms against 0.2 ms of sums), so the default is off.
+    // res_u / res_v: the ordered sum of |R| over the residual range. The sums feed only the stopping
+    // test at the end of the iteration, so on the FP64 fast path they run on a side stream, forked
+    // after the component's sweeps: res_u beside the v prep, res_v beside assemble_p and the
+    // V-cycle, joined before the iteration ends. Beside the sweeps themselves they would cost more
+    // than they save: a co-resident sum CTA stops the sweep's one-wave grid from fitting. The side
+    // sums have their own scratch (the main stream's sums run at the same time) and read the |R|
+    // planes, which nothing else writes until the next iteration's prep when the pressure solve is
+    // a fixed-cycle multigrid without a warm start; otherwise the sums stay on the solver's stream.
+    // SGPU_SIDE_SUMS=0 keeps them there always (a tuning switch: the bits are the same).
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork[2] = {}, ev_done[2] = {};
-    bool side_sums = false;
-    void momentum_sum(bool vcomp, double* res, const double* vals) {
+    bool side_sums = true;
+    bool side_pending = false;
+    SumScratch ss_side;
+    bool defer_sums() const {
+        return side_sums && side && prm.pressure_solver == SGPU_P_MG && prm.mg_mode == SGPU_MG_FIXED && !net;
+    }
+    void momentum_sum(bool vcomp, double* res, const double* vals, bool on_side) {
         const int nr = vcomp ? prm.NX - 1 : prm.NX, nc = vcomp ? prm.NY : prm.NY - 1;
-        if (!side_sums || !side) {
+        if (!on_side) {
             launch_ordered_sum(vals, 0, nc, nr, nc, 1, res, ss, nullptr, st);
             return;
         }
         const int k = vcomp ? 1 : 0;
         SGPU_CUDA(cudaEventRecord(ev_fork[k], st));
         SGPU_CUDA(cudaStreamWaitEvent(side, ev_fork[k], 0));
-        launch_ordered_sum_lean(vals, nc, nr, nc, res, ss, side);
+        launch_ordered_sum_lean(vals, nc, nr, nc, res, ss_side, side);
         SGPU_CUDA(cudaEventRecord(ev_done[k], side));
+        side_pending = true;
     }
     void join_sums() {
-        if (!side_sums || !side) return;
+        if (!side_pending) return;
         SGPU_CUDA(cudaStreamWaitEvent(st, ev_done[0], 0));
         SGPU_CUDA(cudaStreamWaitEvent(st, ev_done[1], 0));
+        side_pending = false;
     }
 
     void fast_iteration_enqueue(double* res3) {
         fast_momentum(false, res3 + 0);
         fast_momentum(true, res3 + 1);
-        join_sums();
         mark(SGPU_PH_ASSEMBLE_P);
         launch_assemble_p_fused(dp, cu.a[8], cv.a[8], u, v, w, nullptr, nullptr, st);
         // res_p = the ordered sum of |b| over the p' cells, read from b itself (res3[3] gets the sum of b)
@@ -283,6 +295,7 @@ struct Solver {
         solve_p();
         mark(SGPU_PH_CORRECT);
         correct();
+        join_sums(); // res_u, res_v from the side stream
         mark(SGPU_PH_COUNT);
     }
 
@@ -523,6 +536,7 @@ struct Solver {
         solve_p();
         mark(SGPU_PH_CORRECT);
         correct();
+        join_sums(); // res_u, res_v from the side stream
         mark(SGPU_PH_COUNT);
     }
     void sync() { SGPU_CUDA(cudaStreamSynchronize(st)); }
@@ -606,6 +620,10 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
         SGPU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         seg_rows = stream_seg_rows(dp, sms, 2, min_seg);
         if (const char* e = std::getenv("SGPU_SIDE_SUMS")) side_sums = std::atoi(e) != 0;
+        ss_side.max_rows = p.nrows;
+        ss_side.max_k = 1;
+        ss_side.rows = dalloc<double>(static_cast<std::size_t>(p.nrows));
+        ss_side.counter = dalloc<unsigned int>(1);
         SGPU_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
         for (int k = 0; k < 2; ++k) {
             SGPU_CUDA(cudaEventCreateWithFlags(&ev_fork[k], cudaEventDisableTiming));

@@ -216,7 +216,12 @@ struct Solver {
     void solve_cg();
     void solve_mg();
     void mg_vcycle();
-    void remove_mean0(double* f);
+    // remove_mean0 (multigrid.cpp:327-345). known_sum: the ordered sum of f's p' cells if it is
+    // already formed (it is then not summed again).
+    void remove_mean0(double* f, const double* known_sum = nullptr);
+    // Set while the fast iteration's pressure solve runs: the ordered sum of b, formed by the |b| / b
+    // pair sum in the same order, for the multigrid's mean removal of b.
+    const double* b_sum = nullptr;
 
     // One momentum phase on the fused path: bc, residual + AP + frozen copy, n streaming sweeps.
     void fast_momentum(bool vcomp, double* res) {
@@ -292,7 +297,9 @@ struct Solver {
         // res_p = the ordered sum of |b| over the p' cells, read from b itself (res3[3] gets the sum of b)
         launch_ordered_sum_abs_pair(w.b + p_origin(), g.pitch, prm.NX, prm.NY, res3 + 2, ss, st);
         mark(SGPU_PH_SOLVE_P);
+        b_sum = res3 + 3; // the multigrid's mean of b reuses the pair's sum of b
         solve_p();
+        b_sum = nullptr;
         mark(SGPU_PH_CORRECT);
         correct();
         join_sums(); // res_u, res_v from the side stream
@@ -880,12 +887,15 @@ void Solver::solve_cg() {
 }
 
 // remove_mean0 (multigrid.cpp:327-345) on the p' interior.
-void Solver::remove_mean0(double* f) {
+void Solver::remove_mean0(double* f, const double* known_sum) {
     double* f0 = at(f, prm.H, prm.H + 1);
-    launch_ordered_sum(f0, 0, g.pitch, prm.NX, prm.NY, 1, sums + 16, ss, nullptr, st);
+    if (!known_sum) {
+        launch_ordered_sum(f0, 0, g.pitch, prm.NX, prm.NY, 1, sums + 16, ss, nullptr, st);
+        known_sum = sums + 16;
+    }
     LevelView L0{prm.NX, prm.NY, g.pitch, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
                  nullptr, nullptr};
-    launch_mg_sub_mean(L0, f0, sums + 16, st);
+    launch_mg_sub_mean(L0, f0, known_sum, st);
 }
 
 // mg_vcycle (multigrid.cpp:299-323).
@@ -913,7 +923,7 @@ void Solver::mg_vcycle() {
 void Solver::solve_mg() {
     for (std::size_t l = 1; l < lv.size(); ++l) launch_mg_build(lv[l - 1], lv[l], st);
     SGPU_CUDA(cudaMemsetAsync(w.pc, 0, g.bytes(), st));
-    remove_mean0(w.b);
+    remove_mean0(w.b, b_sum);
     const bool guess = apply_warm_start(lv[0]);
     last_vcycles = run_cycles(lv[0], !guess, [&](bool x_zero) {
         if (mg_fast) mg_vcycle_fast(x_zero);

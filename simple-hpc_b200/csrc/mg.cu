@@ -7,6 +7,8 @@
 // norms (coarse_solve, :120-140), which runs inside one CTA so its data-dependent sweep count
 // needs no host round trip. Every kernel is a template on the element type: double gives the
 // reference's bits; float is the mixed-precision mode's V-cycle (sums and norms still in double).
+// The float V-cycle also has its own tail: the small levels held in shared memory
+// (k_mg_tail_smem), the coarsest solve in one warp with FP64 tree sums (warp_coarse_core).
 #include "kernels.hpp"
 #include "blocksum.cuh"
 

@@ -34,7 +34,8 @@ enum {
     SGPU_E_INVALID = -1,     /* bad argument, unsupported solver combination, bad config */
     SGPU_E_CUDA = -2,        /* a CUDA runtime call failed (message holds cudaGetErrorString) */
     SGPU_E_NOMEM = -3,       /* device allocation failed or the handle's memory budget is exceeded */
-    SGPU_E_TIMEOUT = -4,     /* a bounded device-side wait ran out (persistent kernels) */
+    SGPU_E_TIMEOUT = -4,     /* a bounded device-side wait ran out (persistent kernels; the mixed
+                                mode's correction sweep waiting for its record copies) */
     SGPU_E_NONFINITE = -5,   /* a residual became NaN or Inf (diverged run) */
     SGPU_E_NODEVICE = -6     /* no CUDA device is visible */
 };

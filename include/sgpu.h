@@ -188,6 +188,11 @@ int sgpu_download(sgpu_handle* h, int field_id, double* host);
 int sgpu_upload(sgpu_handle* h, int field_id, const double* host);
 /* Device bytes held by the handle. */
 int sgpu_memory_bytes(sgpu_handle* h, size_t* bytes);
+/* Diagnostic of the device-side failure detection (no counterpart in the reference): one warp on the
+ * current device waits, at most `polls` polls (1 .. 1 << 20), on an mbarrier that nothing completes,
+ * through the same bounded-wait helper the mixed mode's correction sweep uses. *gave_up = 1 when the
+ * wait ended by giving up and reported it, as it must; the GPU context stays usable. */
+int sgpu_selftest_bounded_wait(int polls, int* gave_up);
 /* Number of multigrid levels and the dims of level l (mg_level_dims, multigrid.cpp:143-151). */
 int sgpu_mg_levels(int NX, int NY, int* nlevels, int* dims /* 2 * 64 ints, may be NULL */);
 /* Statistics of the last solve_p: CG iterations, MG V-cycles, coarsest-level sweeps. */

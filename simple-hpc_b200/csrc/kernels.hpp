@@ -155,6 +155,9 @@ void launch_cg_dir(const DevParams& p, CgPtr cg, const CgScalars* sc, cudaStream
 void init_mixed_kernels();
 // Resident CTAs per SM of the FP32 correction sweep (its register and shared-memory footprint).
 int corr_blocks_per_sm(int ncol);
+// Diagnostic: one warp's bounded wait on an mbarrier that never completes (the correction sweep's
+// wait helper); it gives up after `polls` polls and sets *err.
+void launch_wait_selftest(int polls, unsigned* err, cudaStream_t st);
 // Per-cell FP32 momentum records of the mixed path in three arrays: the near links {AE AW AN AS},
 // the far links {AEE AWW ANN ASS}, and {1/AP, R}; 40 bytes per cell. They are stored by sweep step:
 // the record of cell (i, j) of colour c (c = (i + 3j) mod 5 for five colours, (i + j) mod 2 for

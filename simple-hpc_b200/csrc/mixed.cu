@@ -164,12 +164,26 @@ __device__ __forceinline__ bool mbar_test(unsigned long long* b, unsigned parity
     return done != 0;
 }
 // Wait for phase `parity` of b to complete, at most kSpinLimit polls; a give-up sets *err.
-__device__ __forceinline__ void mbar_wait(unsigned long long* b, unsigned parity, unsigned* err) {
+__device__ __forceinline__ void mbar_wait(unsigned long long* b, unsigned parity, unsigned* err,
+                                          int limit = kSpinLimit) {
     for (int it = 0; !mbar_test(b, parity); ++it)
-        if (it >= kSpinLimit) {
+        if (it >= limit) {
             atomicOr(err, 1u);
             return;
         }
+}
+
+// The give-up path of mbar_wait, exercised on purpose: one warp waits, at most `polls` polls, for a
+// phase of an mbarrier that nothing ever arrives on, so the wait must end by giving up and setting
+// *err. No copy is in flight and nothing else waits on this warp: the kernel returns normally.
+__global__ void k_wait_selftest(int polls, unsigned* err) {
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    mbar_wait(&bar, 0, err, polls);
 }
 // One bulk copy (TMA, no tensor map) of `bytes` from global to this CTA's shared memory, completing
 // on mbarrier b. Both addresses 16-byte aligned, bytes a multiple of 16.
@@ -604,6 +618,11 @@ void init_mixed_kernels() {
     SGPU_SMEM(5, false, 3); SGPU_SMEM(5, true, 3); SGPU_SMEM(2, false, 3); SGPU_SMEM(2, true, 3);
     SGPU_SMEM(5, false, 4); SGPU_SMEM(5, true, 4); SGPU_SMEM(2, false, 4); SGPU_SMEM(2, true, 4);
 #undef SGPU_SMEM
+}
+
+void launch_wait_selftest(int polls, unsigned* err, cudaStream_t st) {
+    k_wait_selftest<<<1, 32, 0, st>>>(polls, err);
+    SGPU_LAUNCH();
 }
 
 int corr_blocks_per_sm(int ncol) {

@@ -1523,6 +1523,27 @@ int sgpu_memory_bytes(sgpu_handle* h, size_t* bytes) {
     return SGPU_OK;
 }
 
+int sgpu_selftest_bounded_wait(int polls, int* gave_up) {
+    if (polls < 1 || polls > (1 << 20) || !gave_up)
+        return sgpu::fail(SGPU_E_INVALID, "sgpu_selftest_bounded_wait: polls in 1 .. 2^20 and an output");
+    return guarded([&] {
+        unsigned* err = nullptr;
+        SGPU_CUDA(cudaMalloc(&err, sizeof(unsigned)));
+        unsigned h = 0;
+        try {
+            SGPU_CUDA(cudaMemset(err, 0, sizeof(unsigned)));
+            sgpu::launch_wait_selftest(polls, err, nullptr);
+            SGPU_CUDA(cudaDeviceSynchronize());
+            SGPU_CUDA(cudaMemcpy(&h, err, sizeof h, cudaMemcpyDeviceToHost));
+        } catch (...) {
+            cudaFree(err);
+            throw;
+        }
+        SGPU_CUDA(cudaFree(err));
+        *gave_up = h != 0 ? 1 : 0;
+    });
+}
+
 int sgpu_mg_levels(int NX, int NY, int* nlevels, int* dims) {
     if (NX < 1 || NY < 1 || !nlevels) return sgpu::fail(SGPU_E_INVALID, "sgpu_mg_levels: bad arguments");
     // mg_level_dims (multigrid.cpp:143-151): halve while both are even and the result is >= 4 x 4.

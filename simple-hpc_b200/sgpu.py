@@ -108,6 +108,7 @@ def lib() -> C.CDLL:
             "sgpu_run": (I, [H, I, D, I, C.POINTER(Result)]),
             "sgpu_download": (I, [H, I, D]), "sgpu_upload": (I, [H, I, D]),
             "sgpu_memory_bytes": (I, [H, C.POINTER(C.c_size_t)]),
+            "sgpu_selftest_bounded_wait": (I, [I, C.POINTER(I)]),
             "sgpu_mg_levels": (I, [I, I, C.POINTER(I), C.POINTER(I)]),
             "sgpu_last_solve_stats": (I, [H, C.POINTER(I), C.POINTER(I), C.POINTER(I), D]),
             "sgpu_ordered_sum": (I, [D, I, I, D]),
@@ -349,6 +350,14 @@ def read_fields(p: Params, directory) -> tuple[np.ndarray, np.ndarray, np.ndarra
 
 def launch_count() -> int:
     return int(lib().sgpu_launch_count())
+
+
+def selftest_bounded_wait(polls: int = 4096) -> bool:
+    """Run the device-side failure-detection diagnostic (sgpu_selftest_bounded_wait): True when a
+    bounded wait on an mbarrier that never completes gave up and reported it."""
+    out = C.c_int(0)
+    _check(lib().sgpu_selftest_bounded_wait(int(polls), C.byref(out)))
+    return bool(out.value)
 
 
 def ordered_sum(values: np.ndarray) -> float:

@@ -479,8 +479,8 @@ void launch_stream_v(const DevParams& p, const double* xin, double* xout, const 
 
 // Rows per CTA segment of the streaming sweep: enough segments to fill the GPU with one wave of
 // 2 CTAs per SM, but never so short that the 2 * NCOL-row halo dominates.
-int stream_seg_rows(const DevParams& p, int sms, int blocks_per_sm, int min_seg) {
-    const int W = 256 - 4 * p.ncol;
+int stream_seg_rows(const DevParams& p, int sms, int blocks_per_sm, int min_seg, int nt) {
+    const int W = nt - 4 * p.ncol;
     const int strips = (p.ncols + W - 1) / W;
     const int want = std::max(1, (blocks_per_sm * sms) / strips); // one wave of resident CTAs
     int seg = (p.nrows + want - 1) / want;

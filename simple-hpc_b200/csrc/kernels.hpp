@@ -155,6 +155,8 @@ void launch_cg_dir(const DevParams& p, CgPtr cg, const CgScalars* sc, cudaStream
 void init_mixed_kernels();
 // Resident CTAs per SM of the FP32 correction sweep (its register and shared-memory footprint).
 int corr_blocks_per_sm(int ncol);
+// Threads per CTA of the FP32 correction sweep (its strips are this wide, halos included).
+int corr_threads();
 // Diagnostic: one warp's bounded wait on an mbarrier that never completes (the correction sweep's
 // wait helper); it gives up after `polls` polls and sets *err.
 void launch_wait_selftest(int polls, unsigned* err, cudaStream_t st);
@@ -164,10 +166,10 @@ void launch_wait_selftest(int polls, unsigned* err, cudaStream_t st);
 // two) sits at (i + 2c) * pitch + j, so the cells the streaming sweep updates at one step, one per
 // column, are contiguous. The arrays have kRecExtraRows rows more than the fields, and are
 // allocated with kRecFrontCols records before element 0 and kRecBackCols after the last row: the
-// correction sweep copies whole step-row segments of its CTA's columns, which reach up to 2 x the
-// colour count before column 0 and past the last column.
+// correction sweep copies whole step-row segments of its CTA's NT columns (NT <= 512), which reach up
+// to 2 x the colour count before column 0 and up to NT past the last column.
 constexpr int kRecExtraRows = 8;
-constexpr int kRecFrontCols = 16, kRecBackCols = 256;
+constexpr int kRecFrontCols = 16, kRecBackCols = 512;
 struct MomRec32 {
     float4* near_links;
     float4* far_links;
@@ -203,7 +205,7 @@ void launch_correct_mixed(const DevParams& p, const LevelView32& L0, const doubl
 // ---- fused fast path (fused.cu) ----
 // Rows per CTA segment of the streaming sweeps: one wave of blocks_per_sm resident CTAs per SM, at
 // least min_seg rows (min_seg <= 0: 8 x the colour count).
-int stream_seg_rows(const DevParams& p, int sms, int blocks_per_sm = 2, int min_seg = 0);
+int stream_seg_rows(const DevParams& p, int sms, int blocks_per_sm = 2, int min_seg = 0, int nt = 256);
 // Momentum prep: |R| into cells, AP over the update range, frozen copy xF of x.
 void launch_mom_prep(const DevParams& p, bool v_component, const double* x, const double* oth,
                      const double* pf, double* xF, double* AP, double* cells, cudaStream_t st);

@@ -510,15 +510,10 @@ Range update_range(const DevParams& p, bool v) {
 }
 
 #ifdef SGPU_FLOAT_UNIT
-// Resident CTAs per SM the correction sweep's registers are bounded for: 3, or 4 when
-// SGPU_CORR_MINB=4 (a tuning switch: the arithmetic is the same).
-int corr_minb() {
-    static const int v = [] {
-        const char* e = std::getenv("SGPU_CORR_MINB");
-        return e && std::atoi(e) == 4 ? 4 : 3;
-    }();
-    return v;
-}
+// Threads per CTA of the correction sweep and the resident CTAs per SM its registers are bounded
+// for (shared memory allows that many: the e ring and two record slot sets per CTA).
+constexpr int kCorrNT = 256;
+constexpr int kCorrMinb = kCorrNT <= 256 ? 3 : 2;
 
 template <int NCOL, bool V, int NT, int MINB>
 void launch_corr(const DevParams& p, const float* ein, float* eout, MomRec32 rec, bool e_zero,
@@ -531,6 +526,7 @@ void launch_corr(const DevParams& p, const float* ein, float* eout, MomRec32 rec
         throw Error(SGPU_E_INVALID, "correction sweep: records not aligned for bulk copies");
     constexpr int W = NT - 4 * NCOL;
     static_assert(W % 2 == 0 && (2 * NCOL) % 2 == 0, "strip starts must be even");
+    static_assert(2 * NCOL <= kRecFrontCols && NT <= kRecBackCols, "copy windows must stay in the margins");
     const dim3 grid((p.ncols + W - 1) / W, (p.nrows + seg_rows - 1) / seg_rows);
     constexpr int smem = CorrSmem<NCOL, NT>::bytes;
     k_corr_stream<NCOL, V, NT, MINB><<<grid, NT, smem, st>>>(p, ein, eout, rec, e_zero ? 1 : 0, seg_rows,
@@ -541,8 +537,7 @@ void launch_corr(const DevParams& p, const float* ein, float* eout, MomRec32 rec
 template <int NCOL, bool V>
 void launch_corr_m(const DevParams& p, const float* ein, float* eout, MomRec32 rec, bool e_zero,
                    int seg_rows, double* xfinal, unsigned* err, cudaStream_t st) {
-    if (corr_minb() == 4) launch_corr<NCOL, V, 256, 4>(p, ein, eout, rec, e_zero, seg_rows, xfinal, err, st);
-    else launch_corr<NCOL, V, 256, 3>(p, ein, eout, rec, e_zero, seg_rows, xfinal, err, st);
+    launch_corr<NCOL, V, kCorrNT, kCorrMinb>(p, ein, eout, rec, e_zero, seg_rows, xfinal, err, st);
 }
 
 #endif // SGPU_FLOAT_UNIT
@@ -612,13 +607,14 @@ void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, f
 }
 
 void init_mixed_kernels() {
-#define SGPU_SMEM(NC, V, M)                                                                            \
-    SGPU_CUDA(cudaFuncSetAttribute(k_corr_stream<NC, V, 256, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                   CorrSmem<NC, 256>::bytes))
-    SGPU_SMEM(5, false, 3); SGPU_SMEM(5, true, 3); SGPU_SMEM(2, false, 3); SGPU_SMEM(2, true, 3);
-    SGPU_SMEM(5, false, 4); SGPU_SMEM(5, true, 4); SGPU_SMEM(2, false, 4); SGPU_SMEM(2, true, 4);
+#define SGPU_SMEM(NC, V)                                                                               \
+    SGPU_CUDA(cudaFuncSetAttribute(k_corr_stream<NC, V, kCorrNT, kCorrMinb>,                           \
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, CorrSmem<NC, kCorrNT>::bytes))
+    SGPU_SMEM(5, false); SGPU_SMEM(5, true); SGPU_SMEM(2, false); SGPU_SMEM(2, true);
 #undef SGPU_SMEM
 }
+
+int corr_threads() { return kCorrNT; }
 
 void launch_wait_selftest(int polls, unsigned* err, cudaStream_t st) {
     k_wait_selftest<<<1, 32, 0, st>>>(polls, err);
@@ -626,15 +622,14 @@ void launch_wait_selftest(int polls, unsigned* err, cudaStream_t st) {
 }
 
 int corr_blocks_per_sm(int ncol) {
-    const int smem = ncol == 5 ? CorrSmem<5, 256>::bytes : CorrSmem<2, 256>::bytes;
+    const int smem = ncol == 5 ? CorrSmem<5, kCorrNT>::bytes : CorrSmem<2, kCorrNT>::bytes;
     int n = 0;
-    const bool four = corr_minb() == 4;
     if (ncol == 5)
-        SGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &n, four ? k_corr_stream<5, false, 256, 4> : k_corr_stream<5, false, 256, 3>, 256, smem));
+        SGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_corr_stream<5, false, kCorrNT, kCorrMinb>,
+                                                                kCorrNT, smem));
     else
-        SGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &n, four ? k_corr_stream<2, false, 256, 4> : k_corr_stream<2, false, 256, 3>, 256, smem));
+        SGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_corr_stream<2, false, kCorrNT, kCorrMinb>,
+                                                                kCorrNT, smem));
     return n > 0 ? n : 1;
 }
 

@@ -118,7 +118,9 @@ struct Solver {
     int min_seg = 8;
     void use_batch_shape() {
         min_seg = 0;
-        if (fast) seg_rows = stream_seg_rows(dp, sms, mixed ? corr_blocks_per_sm(dp.ncol) : 2, 0);
+        if (fast)
+            seg_rows = mixed ? stream_seg_rows(dp, sms, corr_blocks_per_sm(dp.ncol), 0, corr_threads())
+                             : stream_seg_rows(dp, sms, 2, 0);
     }
 
     int ncol = 5;
@@ -731,7 +733,7 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
                         "mg and 1 <= mg_pre <= 4, 0 <= mg_post <= 4");
         mixed = true;
         init_mixed_kernels();
-        seg_rows = stream_seg_rows(dp, sms, corr_blocks_per_sm(dp.ncol), min_seg);
+        seg_rows = stream_seg_rows(dp, sms, corr_blocks_per_sm(dp.ncol), min_seg, corr_threads());
         const std::size_t nrec =
             g.elems() + static_cast<std::size_t>(kRecExtraRows) * g.pitch + kRecFrontCols + kRecBackCols;
         rec32.near_links = dalloc<float4>(nrec) + kRecFrontCols;

@@ -246,6 +246,8 @@ def measure(sgpu, torch, n: int, precision: str, steps: int, warmup: int, world:
     prof = solver.run(steps)[0].iterations
     ph1 = solver.phase_seconds()
     sw1 = solver.sweep_seconds()
+    # final u, v, p (after warmup + 2 x steps iterations, the same count in every arm)
+    fields = [solver.download(f) for f in (sgpu.F_U, sgpu.F_V, sgpu.F_P)]
     solver.close()
     secs = allmax(e0.elapsed_time(e1) * 1e-3, world)
     iters = res.iterations
@@ -253,7 +255,18 @@ def measure(sgpu, torch, n: int, precision: str, steps: int, warmup: int, world:
             "ms_per_step": 1e3 * secs / max(iters, 1), "launches": launches, "clocks": clk_info,
             "phases": {k: (ph1[k] - ph0[k]) * iters / max(prof, 1) for k in ph1 if k != "output"},
             "sweep_s": sw1[0] - sw0[0], "sweep_launches": sw1[1] - sw0[1],
-            "converged": bool(res.converged)}
+            "converged": bool(res.converged), "fields": fields,
+            "iterations_total": warmup + iters + prof}
+
+
+def field_errors(a_fields, b_fields) -> dict:
+    """max |a - b| / max |b| and ||a - b|| / ||b|| of u, v, p (b: the plain FP64 run)."""
+    import numpy as np
+    out = {}
+    for name, a, b in zip("uvp", a_fields, b_fields):
+        out[name] = {"max_rel": float(np.max(np.abs(a - b)) / np.max(np.abs(b))),
+                     "l2_rel": float(np.linalg.norm(a - b) / np.linalg.norm(b))}
+    return out
 
 
 def e2e_measure(sgpu, torch, p, steps: int, world: int) -> dict:
@@ -499,7 +512,12 @@ def main() -> None:
                        "converged_in_timed_region": head["converged"]},
             "plain_fp64": None if plain is None else {
                 "value": plain["value"], "ms_per_step": plain["ms_per_step"],
-                "note": "bit-identical to the reference; same K steps, same run"},
+                "note": "bit-identical to the reference (tests/test_gpu_scale.py checks 4096^2 x 3 and "
+                        "1024^2 x 50 iterations against the reference's own build); same K steps, same run"},
+            "errors_vs_fp64": None if plain is None else {
+                "after_iterations": head["iterations_total"],
+                "fields": field_errors(head["fields"], plain["fields"]),
+                "note": "mixed arm against the plain FP64 arm of this run, same iteration count"},
             "timing": "sgpu_run replays the captured outer-iteration graph (WHILE node, device-side "
                       "stopping test); per-phase times come from a separate profiled pass",
             "mixed_vs_fp64": None if plain is None else head["value"] / plain["value"],

@@ -33,10 +33,10 @@ enum {
     SGPU_OK = 0,
     SGPU_E_INVALID = -1,     /* bad argument, unsupported solver combination, bad config */
     SGPU_E_CUDA = -2,        /* a CUDA runtime call failed (message holds cudaGetErrorString) */
-    SGPU_E_NOMEM = -3,       /* device allocation failed or the handle's memory budget is exceeded */
+    SGPU_E_NOMEM = -3,       /* a device allocation failed */
     SGPU_E_TIMEOUT = -4,     /* a bounded device-side wait ran out (persistent kernels; the mixed
                                 mode's correction sweep waiting for its record copies) */
-    SGPU_E_NONFINITE = -5,   /* a residual became NaN or Inf (diverged run) */
+    SGPU_E_NONFINITE = -5,   /* a residual became NaN or Inf: sgpu_run stopped the diverged run */
     SGPU_E_NODEVICE = -6     /* no CUDA device is visible */
 };
 
@@ -179,6 +179,9 @@ typedef struct sgpu_result {
  * [iter, res_u, res_v, res_p] and must hold 4 * maxit doubles. If print_every > 0, the
  * reference's "iter k  res_u ..." lines are printed at iteration 1 and every print_every
  * iterations. Replaces run_simple_hip's loop (solver_hip.hip:538-550).
+ * A residual that becomes NaN or Inf stops the run after that iteration: *result and log cover the
+ * iterations run, and the call returns SGPU_E_NONFINITE (the reference has no such test and runs a
+ * diverged case on to maxit).
  */
 int sgpu_run(sgpu_handle* h, int maxit, double* log, int print_every, sgpu_result_t* result);
 
@@ -213,9 +216,10 @@ int sgpu_ordered_sum(const double* values, int nrows_v, int ncols_v, double* out
  * at values + k * ld; *out receives the sum. stream is a cudaStream_t (NULL = legacy default). The
  * call allocates nothing: its scratch is a fixed array inside the library (16384 rows at most;
  * larger blocks are refused with SGPU_E_INVALID), fetched per device by the first call made on that
- * device, which should come before any stream capture. The call is asynchronous on stream; calls
- * that overlap on the GPU (other streams, other host threads) share that scratch and race, so
- * serialise them.
+ * device, which should come before any stream capture. That address is kept for the life of the
+ * process: a cudaDeviceReset after the first call on a device is not supported. The call is
+ * asynchronous on stream; calls that overlap on the GPU (other streams, other host threads) share
+ * that scratch and race, so serialise them.
  */
 int sgpu_ordered_sum_noalloc(const double* values, int nrows_v, int ncols_v, int ld, double* out,
                              void* stream);
@@ -332,7 +336,8 @@ int sgpu_batch_autotune(sgpu_batch* b, int* chosen);
  * the first log_cap (iteration, res_u, res_v, res_p) rows of every cavity (sgpu_batch_log).
  * *seconds = device time of the launch. */
 int sgpu_batch_run(sgpu_batch* b, int maxit, int log_cap, double* seconds);
-/* Per cavity: iterations run, converged flag, last res_u, res_v, res_p (3 per cavity). */
+/* Per cavity: iterations run, converged flag (1 converged, 0 not, -1 stopped because a residual became
+ * NaN or Inf), last res_u, res_v, res_p (3 per cavity). */
 int sgpu_batch_results(sgpu_batch* b, int* iterations, int* converged, double* residuals);
 /* count x log_cap x 4 doubles; rows past a cavity's iteration count are zero. */
 int sgpu_batch_log(sgpu_batch* b, double* host);

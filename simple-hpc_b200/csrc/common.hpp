@@ -3,8 +3,10 @@
 
 #include "../../include/sgpu.h"
 
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 
@@ -48,6 +50,32 @@ void params_from_config(const std::string& text, sgpu_params_t& p);
         ::sgpu::count_launch();                                                               \
         SGPU_CUDA(cudaGetLastError());                                                        \
     } while (0)
+
+// Once-per-device set-up of a kernel: function attributes (cudaFuncSetAttribute) and occupancy
+// queries. CUDA keeps a function's attributes in each device's context, so a process that runs on
+// several GPUs must set them on every one. The state is one bit per device ordinal; the first call
+// on a device runs init() with that device current, under a mutex, so first calls from several
+// host threads are safe. init() returns an int that later calls on that device get back (e.g. the
+// resident blocks per SM).
+struct PerDeviceOnce {
+    static constexpr int kMaxDevices = 64;
+    std::mutex mu;
+    std::atomic<std::uint64_t> done{0};
+    int value[kMaxDevices] = {};
+    template <class F> int get(F&& init) {
+        int dev = 0;
+        SGPU_CUDA(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= kMaxDevices) throw Error(SGPU_E_INVALID, "device ordinal above 63");
+        const std::uint64_t bit = std::uint64_t{1} << dev;
+        if (done.load(std::memory_order_acquire) & bit) return value[dev];
+        std::lock_guard<std::mutex> lock(mu);
+        if (!(done.load(std::memory_order_relaxed) & bit)) {
+            value[dev] = init();
+            done.fetch_or(bit, std::memory_order_release);
+        }
+        return value[dev];
+    }
+};
 #endif
 
 // ---- device layout ----

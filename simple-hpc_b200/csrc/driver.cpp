@@ -118,7 +118,11 @@ int main(int argc, char** argv) {
         check(sgpu_set_profiling(h.h, 1));
         std::vector<double> log(4 * static_cast<std::size_t>(p.maxit > 0 ? p.maxit : 1));
         sgpu_result_t r{};
-        check(sgpu_run(h.h, p.maxit, log.data(), 100, &r));
+        // A diverged run (a residual became NaN or Inf) stops early; its outputs are still written,
+        // as the reference writes those of a run that reached maxit, and the exit status is 1.
+        const int rc = sgpu_run(h.h, p.maxit, log.data(), 100, &r);
+        const std::string diverged = rc == SGPU_E_NONFINITE ? sgpu_last_error() : "";
+        if (rc != SGPU_E_NONFINITE) check(rc);
         check(sgpu_download(h.h, SGPU_F_U, u.data()));
         check(sgpu_download(h.h, SGPU_F_V, v.data()));
         check(sgpu_download(h.h, SGPU_F_P, pf.data()));
@@ -126,6 +130,7 @@ int main(int argc, char** argv) {
                                  argv[1], SIMPLE_GIT_HASH, SIMPLE_COMPILER));
         std::cout << (r.converged ? "converged" : "not converged") << " after " << r.iterations
                   << " iterations in " << r.seconds << " s\n";
+        if (!diverged.empty()) throw std::runtime_error(diverged);
     } catch (const std::exception& e) {
         std::cerr << "error (rank 0): " << e.what() << "\n";
         return 1;

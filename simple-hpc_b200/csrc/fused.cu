@@ -456,12 +456,12 @@ void launch_stream(const DevParams& p, const double* xin, double* xout, const do
     constexpr int W = NT - 4 * NCOL;
     const dim3 grid((p.ncols + W - 1) / W, (p.nrows + seg_rows - 1) / seg_rows);
     constexpr int smem = kRing * NT * static_cast<int>(sizeof(double));
-    static bool attr_set = false; // per process; the attribute applies to every device
-    if (!attr_set) {
+    static PerDeviceOnce attr; // the attribute lives in each device's context
+    attr.get([] {
         SGPU_CUDA(cudaFuncSetAttribute(k_mom_stream<NCOL, V, NT, QUICK, ORDER, PF>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        attr_set = true;
-    }
+        return 0;
+    });
     k_mom_stream<NCOL, V, NT, QUICK, ORDER, PF><<<grid, NT, smem, st>>>(p, xin, xout, xF, oth, pf, seg_rows);
     SGPU_LAUNCH();
 }

@@ -506,12 +506,12 @@ void launch_mg_tail(const MgLevelsT<T>& lv, int first, int pre, int post, double
         ts.bytes = bytes;
         const int nc = lv.L[lv.n - 1].nx * lv.L[lv.n - 1].ny;
         if (lv.n <= 24 && bytes <= kTailSmemMax && nc <= kWarpCoarseCells) {
-            static bool attr = false; // per process
-            if (!attr) {
+            static PerDeviceOnce attr; // the attribute lives in each device's context
+            attr.get([] {
                 SGPU_CUDA(cudaFuncSetAttribute(k_mg_tail_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                kTailSmemMax));
-                attr = true;
-            }
+                return 0;
+            });
             k_mg_tail_smem<<<1, kCoarseThreads, bytes, st>>>(lv, first, pre, post, omega, tol, ts, sweeps_out);
             SGPU_LAUNCH();
             return;

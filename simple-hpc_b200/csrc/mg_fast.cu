@@ -287,14 +287,15 @@ int seg_for(int nx, int ny, int HC, int sms, int blocks_per_sm, int min_seg) {
     return seg;
 }
 
-template <class K> int prepare_kernel(K kernel, int smem, bool& done, int& blocks) {
-    if (!done) {
+// Sets the kernel's shared-memory attribute on the current device (once per device) and returns its
+// resident CTAs per SM there.
+template <class K> int prepare_kernel(K kernel, int smem, PerDeviceOnce& once) {
+    return once.get([&] {
         SGPU_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        int blocks = 0;
         SGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kNT, smem));
-        if (blocks < 1) blocks = 1;
-        done = true;
-    }
-    return blocks;
+        return blocks < 1 ? 1 : blocks;
+    });
 }
 
 // Register budget of the level kernels: PD register sets in the coefficient pipeline against
@@ -320,10 +321,9 @@ void down_v(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, bool x_zero
             cudaStream_t st) {
     const int HC = 2 * PRE + 2;
     constexpr int smem = kRing * kNT * static_cast<int>(sizeof(T));
-    static bool done = false;
-    static int blocks = 0;
+    static PerDeviceOnce once;
     auto kernel = k_mg_down<kNT, PRE, PD, MINB, T>;
-    const int seg = seg_for(F.nx, F.ny, HC, sms, prepare_kernel(kernel, smem, done, blocks), min_seg);
+    const int seg = seg_for(F.nx, F.ny, HC, sms, prepare_kernel(kernel, smem, once), min_seg);
     const int W = kNT - 2 * HC;
     const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
     kernel<<<grid, kNT, smem, st>>>(F, C, xout, x_zero ? 1 : 0, seg, HC);
@@ -335,10 +335,9 @@ void up_v(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, T* xout,
           int sms, int min_seg, cudaStream_t st) {
     const int HC = 2 * POST + 2;
     constexpr int smem = kRing * kNT * static_cast<int>(sizeof(T));
-    static bool done = false;
-    static int blocks = 0;
+    static PerDeviceOnce once;
     auto kernel = k_mg_up<kNT, POST, PD, MINB, T>;
-    const int seg = seg_for(F.nx, F.ny, HC, sms, prepare_kernel(kernel, smem, done, blocks), min_seg);
+    const int seg = seg_for(F.nx, F.ny, HC, sms, prepare_kernel(kernel, smem, once), min_seg);
     const int W = kNT - 2 * HC;
     const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
     kernel<<<grid, kNT, smem, st>>>(C, F, xin, xout, omega, seg, HC);

@@ -163,14 +163,16 @@ __device__ __forceinline__ bool mbar_test(unsigned long long* b, unsigned parity
                  : "memory");
     return done != 0;
 }
-// Wait for phase `parity` of b to complete, at most kSpinLimit polls; a give-up sets *err.
-__device__ __forceinline__ void mbar_wait(unsigned long long* b, unsigned parity, unsigned* err,
+// Wait for phase `parity` of b to complete, at most kSpinLimit polls. Returns false on a give-up,
+// which also sets *err.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity, unsigned* err,
                                           int limit = kSpinLimit) {
     for (int it = 0; !mbar_test(b, parity); ++it)
         if (it >= limit) {
             atomicOr(err, 1u);
-            return;
+            return false;
         }
+    return true;
 }
 
 // The give-up path of mbar_wait, exercised on purpose: one warp waits, at most `polls` polls, for a
@@ -218,7 +220,10 @@ template <int NCOL, int NT> struct CorrSmem {
 // on its `empty` mbarrier once it has read the set, and thread 0 refills the set for the super-step
 // kRecAhead later only after that. The e rows are per-thread cp.async copies, one group per
 // super-step, waited for kRecAhead super-steps later. Waits are bounded (kSpinLimit); a give-up
-// sets *err, which the host reports. e_zero: e_in is zero and is not read.
+// sets *err, which the host reports as SGPU_E_TIMEOUT, and stops the CTA cleanly: the barrier of the
+// next super-step tells every thread (__syncthreads_or), no further copy is issued and nothing more
+// is written, and thread 0 waits (bounded again) for the record copies it has in flight before the
+// CTA exits. The output of such a sweep is invalid. e_zero: e_in is zero and is not read.
 template <int NCOL, bool V, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     k_corr_stream(DevParams p, const float* __restrict__ ein, float* __restrict__ eout,
@@ -299,10 +304,14 @@ __global__ void __launch_bounds__(NT, MINB)
     auto next_colour = [&](int c, int steps) {
         return NCOL == 5 ? (c + 2 * steps) % 5 : (c + steps) & 1;
     };
-    // Thread 0: the records of the super-step whose first step is t into slot set `slot`. Step
-    // rows past the arrays' end hold no cell and are not fetched.
+    // Thread 0: the records of the super-step whose first step is t into slot set `slot`, completing
+    // phase `parity` of full[slot]. Step rows past the arrays' end hold no cell and are not fetched.
+    // `inflight` (thread 0 only) marks the slot sets whose copies thread 0 has not yet seen land.
     const int rec_rows = p.nrows + kRecExtraRows;
-    auto fill = [&](int slot, int t) {
+    unsigned inflight = 0, inflight_parity = 0;
+    auto fill = [&](int slot, int t, unsigned parity) {
+        inflight |= 1u << slot;
+        inflight_parity = (inflight_parity & ~(1u << slot)) | (parity << slot);
         unsigned bytes = 0;
 #pragma unroll
         for (int s = 0; s < SPB; ++s)
@@ -351,8 +360,8 @@ __global__ void __launch_bounds__(NT, MINB)
     cp_async_commit();
     cp_async_commit();
     if (tid == 0) {
-        fill(0, L0);
-        if (L0 + SPB <= t_last) fill(1, L0 + SPB);
+        fill(0, L0, 0u);
+        if (L0 + SPB <= t_last) fill(1, L0 + SPB, 0u);
     }
 #pragma unroll
     for (int s = 0; s < SPB; ++s) {
@@ -361,10 +370,16 @@ __global__ void __launch_bounds__(NT, MINB)
     }
 
     int c_cur = c_start;
-    auto super_step = [&](int t, int slot, unsigned parity) {
-        cp_async_wait<D - 1>();            // this thread's e rows for this super-step have landed
-        mbar_wait(&full[slot], parity, err); // the slot set's records have landed
-        __syncthreads();                   // ... and everyone's e rows
+    bool gave_up = false; // a bounded wait of this thread ran out
+    // One super-step; false when a wait of any thread has given up (the CTA then stops).
+    auto super_step = [&](int t, int slot, unsigned parity) -> bool {
+        cp_async_wait<D - 1>(); // this thread's e rows for this super-step have landed
+        if (mbar_wait(&full[slot], parity, err)) { // the slot set's records have landed
+            if (tid == 0) inflight &= ~(1u << slot);
+        } else {
+            gave_up = true;
+        }
+        if (__syncthreads_or(gave_up ? 1 : 0)) return false; // ... and everyone's e rows
 #pragma unroll
         for (int s = 0; s < SPB; ++s) {
             int r;
@@ -397,16 +412,22 @@ __global__ void __launch_bounds__(NT, MINB)
         // Thread 0 refills the slot set for the super-step D later once every thread has read it;
         // a super-step past the last is not fetched, so no copy is in flight when the CTA exits.
         if (tid == 0 && t + SPB * D <= t_last) {
-            mbar_wait(&empty[slot], parity, err);
-            fill(slot, t + SPB * D);
+            if (mbar_wait(&empty[slot], parity, err)) fill(slot, t + SPB * D, parity ^ 1u);
+            else gave_up = true; // not refilled: the next super-step's barrier stops the CTA
         }
+        return true;
     };
     unsigned parity = 0;
     for (int t = L0; t <= t_last; t += 2 * SPB) {
-        super_step(t, 0, parity);
-        if (t + SPB <= t_last) super_step(t + SPB, 1, parity);
+        if (!super_step(t, 0, parity)) break;
+        if (t + SPB <= t_last && !super_step(t + SPB, 1, parity)) break;
         parity ^= 1u;
     }
+    // After a give-up, record copies may still be in flight into this CTA's shared memory: wait for
+    // them (bounded) before exiting. On the normal path nothing is in flight here.
+    if (tid == 0)
+        for (int sl = 0; sl < D; ++sl)
+            if ((inflight >> sl) & 1u) mbar_wait(&full[sl], (inflight_parity >> sl) & 1u, err);
     cp_async_wait<0>();
 }
 

@@ -11,6 +11,8 @@
 // The array names are host-side stand-ins in host code, not device addresses, so the device
 // addresses are fetched with cudaGetSymbolAddress once per device, with that device current, by
 // the first call made on that device; that first call should come before any stream capture.
+// The addresses are kept for the life of the process, so a cudaDeviceReset after the first call on
+// a device (which unloads the module and may move the arrays) is not supported.
 #include "kernels.hpp"
 
 #include <mutex>

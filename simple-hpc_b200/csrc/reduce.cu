@@ -158,11 +158,11 @@ void launch_sum(const TIn* vals, std::size_t plane_stride, int ld, int nr, int n
     }
     const dim3 grid((nr + kTile - 1) / kTile, K);
     constexpr int smem = STAGES * kTile * kPitch * static_cast<int>(sizeof(TIn));
-    static bool attr = false; // per process
-    if (!attr) {
+    static PerDeviceOnce attr; // the attribute lives in each device's context
+    attr.get([] {
         SGPU_CUDA(cudaFuncSetAttribute(k_ordered_sum<TIn, STAGES, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        attr = true;
-    }
+        return 0;
+    });
     // Rows per staged chunk of the final pass: K planes of (chunk + 1) doubles fit the tile ring.
     const int chunk = std::min(2048, (smem / (static_cast<int>(sizeof(double)) * kout) - 1) / kTile * kTile);
     k_ordered_sum<TIn, STAGES, PAIR><<<grid, 32, smem, st>>>(vals, plane_stride, ld, nr, nc, s.rows, s.counter,

@@ -1002,7 +1002,7 @@ struct BatchDev {
     double* maxr;               // 3 running maxima per cavity
     int* iters;                 // iterations done per cavity
     int* active;                // 1 while a cavity iterates
-    int* converged;
+    int* converged;             // 1 converged, -1 stopped because a residual became NaN or Inf
     double* last;               // 3 residuals of the last iteration per cavity
     double* log;                // log_cap x 4 per cavity (iteration, res_u, res_v, res_p), or null
     int log_cap;
@@ -1020,7 +1020,8 @@ __global__ void k_batch_pre(const BatchDev* bp) {
 
 // End of a batch iteration: the stopping rule of run_outer_loop (solver.cpp:117-129) per active
 // cavity, with the same arithmetic as the host loop of sgpu_run; the loop continues while any
-// cavity is active.
+// cavity is active. A cavity whose residuals are no longer finite stops (converged = -1): the
+// reference would run such a diverged cavity on to maxit (its NaNs never pass the test).
 __global__ void k_batch_step(const BatchDev* bp) {
     const BatchDev& b = *bp;
     __shared__ int any;
@@ -1039,6 +1040,11 @@ __global__ void k_batch_step(const BatchDev* bp) {
             l[1] = ru;
             l[2] = rv;
             l[3] = rp;
+        }
+        if (!(isfinite(ru) && isfinite(rv) && isfinite(rp))) {
+            b.active[c] = 0;
+            b.converged[c] = -1;
+            continue;
         }
         double tu = ru, tv = rv, tp = rp;
         if (b.runmax[c]) {
@@ -1390,7 +1396,8 @@ int sgpu_outer_iteration(sgpu_handle* h, double res[3], double* phase_seconds) {
 // print interval (sgpu::IterGraph), the stopping rule and the residual log on the device. Used when
 // every outer iteration is a fixed sequence of launches (no CG, no tolerance-driven multigrid, no
 // warm start) and the per-phase timers are off.
-static bool run_graphed(sgpu::Solver& s, int maxit, double* log, int print_every, sgpu_result_t& out) {
+static bool run_graphed(sgpu::Solver& s, int maxit, double* log, int print_every, sgpu_result_t& out,
+                        bool& diverged) {
     if (s.profiling || maxit < 1 || s.prm.pressure_solver == SGPU_P_CG || s.prm.mg_mode == SGPU_MG_TOLERANCE ||
         s.net)
         return false;
@@ -1427,9 +1434,18 @@ static bool run_graphed(sgpu::Solver& s, int maxit, double* log, int print_every
                              cudaMemcpyDeviceToHost));
     g.count(done, done);
     out.iterations = done;
-    out.converged = conv;
+    out.converged = conv == 1 ? 1 : 0;
+    diverged = conv < 0;
     if (s.prm.pressure_solver == SGPU_P_MG) out.mg_vcycles = done * s.prm.mg_cycles;
     return true;
+}
+
+// A residual that is NaN or Inf ends the run (the reference has no such test and runs a diverged
+// case on to maxit, src/solver.cpp:106-132): the result and the log hold the iterations up to and
+// including the one that produced it, and the call returns SGPU_E_NONFINITE.
+static void raise_nonfinite(const sgpu_result_t& out) {
+    throw sgpu::Error(SGPU_E_NONFINITE, "a residual became NaN or Inf at outer iteration " +
+                                            std::to_string(out.iterations) + " (the run diverged)");
 }
 
 int sgpu_run(sgpu_handle* h, int maxit, double* log, int print_every, sgpu_result_t* result) {
@@ -1438,10 +1454,12 @@ int sgpu_run(sgpu_handle* h, int maxit, double* log, int print_every, sgpu_resul
         sgpu::Solver& s = *h->s;
         sgpu_result_t out{};
         const auto t0 = std::chrono::steady_clock::now();
-        if (run_graphed(s, maxit, log, print_every, out)) {
+        bool diverged = false;
+        if (run_graphed(s, maxit, log, print_every, out, diverged)) {
             out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
             s.check_pipeline();
             if (result) *result = out;
+            if (diverged) raise_nonfinite(out);
             return;
         }
         double mu = 0.0, mv = 0.0, mp = 0.0;
@@ -1472,6 +1490,10 @@ int sgpu_run(sgpu_handle* h, int maxit, double* log, int print_every, sgpu_resul
             out.iterations = iter;
             if (print_every > 0 && (iter == 1 || iter % print_every == 0))
                 std::printf("iter %d  res_u %.6e  res_v %.6e  res_p %.6e\n", iter, ru, rv, rp);
+            if (!(std::isfinite(ru) && std::isfinite(rv) && std::isfinite(rp))) {
+                diverged = true;
+                break;
+            }
             // Stopping rule of run_outer_loop (solver.cpp:117-129).
             double tu = ru, tv = rv, tp = rp;
             if (s.prm.residual_normalisation == SGPU_NORM_RUNNING_MAX) {
@@ -1494,6 +1516,7 @@ int sgpu_run(sgpu_handle* h, int maxit, double* log, int print_every, sgpu_resul
             std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         s.check_pipeline();
         if (result) *result = out;
+        if (diverged) raise_nonfinite(out);
     });
 }
 

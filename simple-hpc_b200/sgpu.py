@@ -214,7 +214,9 @@ class Batch:
         its, conv = (C.c_int * n)(), (C.c_int * n)()
         res = np.zeros((n, 3))
         _check(lib().sgpu_batch_results(self._h, its, conv, _dptr(res)))
-        return {"iterations": np.array(its), "converged": np.array(conv, bool), "residuals": res}
+        conv = np.array(conv)
+        return {"iterations": np.array(its), "converged": conv == 1, "diverged": conv == -1,
+                "residuals": res}
 
     def log(self) -> np.ndarray:
         out = np.zeros((len(self.params), self.log_cap, 4))

@@ -10,7 +10,8 @@ Two kinds of fixture, both float64 .npz files:
   oracle/_ref/libsimpleref.so (oracle/Makefile), for the GPU backend's solver combinations:
   final u, v, p and the residual log.
 
-Usage:  python tests/golden/make_golden.py [REFERENCE_DIR]
+Usage:  python tests/golden/make_golden.py [REFERENCE_DIR] [TAG ...]
+(with tags, only those run fixtures are written)
 """
 from __future__ import annotations
 
@@ -45,6 +46,12 @@ RUNS = [
      {"N_cells_x": "32", "N_cells_y": "32", "Re": "100", "convection_scheme": "QUICK",
       "diffusion_order": "2", "momentum_solver": "gs_multicolour", "pressure_solver": "mg",
       "error_tolerance": "1e-5", "maxit": "60000"}, 60000),
+    # The converged_32x40 snapshot's own stopping rule (residual_normalisation = running_max,
+    # tolerance 1e-4), run to convergence with the GPU backend's solver combinations.
+    ("runmax_mc_mg_32x40", "converged_32x40",
+     {"momentum_solver": "gs_multicolour", "pressure_solver": "mg"}, 15000),
+    ("runmax_mc_rb_32x40", "converged_32x40",
+     {"momentum_solver": "gs_multicolour", "pressure_solver": "gs_redblack"}, 15000),
 ]
 
 
@@ -66,8 +73,10 @@ def parse_cfg(text: str) -> dict:
     return out
 
 
-def main(ref: Path) -> None:
+def main(ref: Path, tags: list[str]) -> None:
     for name in ("short_16", "converged_32x40"):
+        if tags:
+            break
         d = ref / "tests" / "snapshots" / name
         cfg = (ref / "configs" / "snapshot" / f"{name}.cfg").read_text()
         arrs = {k: np.loadtxt(d / f"{k}.csv", delimiter=",", dtype=np.float64) for k in ("u", "v", "p")}
@@ -77,6 +86,8 @@ def main(ref: Path) -> None:
         print(f"snapshot_{name}.npz", {k: v.shape for k, v in arrs.items()}, alog.shape)
 
     for tag, base, ov, iters in RUNS:
+        if tags and tag not in tags:
+            continue
         text = config_text(ref, base, ov)
         cfg = parse_cfg(text)
         nx, ny = int(cfg.get("N_cells_x", 80)), int(cfg.get("N_cells_y", 80))
@@ -89,4 +100,4 @@ def main(ref: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"), sys.argv[2:])

@@ -122,9 +122,12 @@ def test_fixed_work_200_iterations(sgpu_mod, oracle_mod):
 
 
 @pytest.mark.parametrize("tag", ["mc_rb_quick4_32x40", "mc_mg_quick4_32x40", "mc_cg_uds2_32x40",
-                                 "jac_jac_quick4_16", "cavity32_re100_mc_mg"])
+                                 "jac_jac_quick4_16", "cavity32_re100_mc_mg", "runmax_mc_mg_32x40",
+                                 "runmax_mc_rb_32x40"])
 def test_reference_golden_runs(sgpu_mod, tag):
-    """Runs of the reference's own sources, reproduced bit for bit on the GPU (stopping iteration too)."""
+    """Runs of the reference's own sources, reproduced bit for bit on the GPU (stopping iteration too).
+    The runmax_* runs stop by the running_max rule of run_outer_loop (solver.cpp:117-129) at
+    tolerance 1e-4, the converged_32x40 snapshot's own settings."""
     gd = load_golden(f"run_{tag}.npz")
     p = sgpu_mod.params_from_config(config_text(gd["config"]))
     with sgpu_mod.Solver(p) as g:

@@ -34,7 +34,8 @@ def test_snapshot_bit_exact(sgpu_mod, oracle_mod, name):
 
 
 @pytest.mark.parametrize("tag", ["mc_rb_quick4_32x40", "mc_mg_quick4_32x40", "mc_cg_uds2_32x40",
-                                 "jac_jac_quick4_16", "cavity32_re100_mc_mg"])
+                                 "jac_jac_quick4_16", "cavity32_re100_mc_mg", "runmax_mc_mg_32x40",
+                                 "runmax_mc_rb_32x40"])
 def test_reference_runs_bit_exact(sgpu_mod, oracle_mod, tag):
     g = load_golden(f"run_{tag}.npz")
     cfg = g["config"]

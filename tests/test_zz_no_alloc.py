@@ -56,3 +56,29 @@ def test_noalloc_rejects_oversized_blocks(sgpu_mod):
     rc = _noalloc(sgpu_mod)(dev.data_ptr(), 16385, 4, 4, out.data_ptr(), None)
     assert rc == sgpu_mod.E_INVALID
     assert "exceed the fixed scratch of 16384 rows" in sgpu_mod.lib().sgpu_last_error().decode()
+
+
+def test_noalloc_strided_block_and_empty_shapes(sgpu_mod):
+    """The two things this entry point adds over sgpu_ordered_sum: a row stride ld wider than the
+    summed columns (a column slice of a wider device array), and empty blocks (sum 0.0)."""
+    import torch
+    rng = np.random.default_rng(7)
+    wide = rng.standard_normal((1500, 700)) * 10.0 ** rng.integers(-6, 6, (1500, 700))
+    dev = torch.from_numpy(wide).to("cuda")
+    out = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
+    f = _noalloc(sgpu_mod)
+    stream = torch.cuda.current_stream()
+    for c0, nc in ((0, 700), (13, 517), (699, 1), (250, 0)):
+        rc = f(dev.data_ptr() + 8 * c0, 1500, nc, 700, out.data_ptr(), stream.cuda_stream)
+        assert rc == 0, sgpu_mod.lib().sgpu_last_error().decode()
+        stream.synchronize()
+        got = float(out.cpu().item())
+        want = sgpu_mod.ordered_sum(np.ascontiguousarray(wide[:, c0:c0 + nc])) if nc else 0.0
+        assert np.float64(got).view(np.uint64) == np.float64(want).view(np.uint64), (c0, nc, got, want)
+    out.fill_(float("nan"))
+    rc = f(dev.data_ptr(), 0, 700, 700, out.data_ptr(), stream.cuda_stream)
+    assert rc == 0, sgpu_mod.lib().sgpu_last_error().decode()
+    stream.synchronize()
+    assert float(out.cpu().item()) == 0.0
+    rc = f(dev.data_ptr(), 4, 8, 7, out.data_ptr(), stream.cuda_stream)  # ld < ncols
+    assert rc == sgpu_mod.E_INVALID

@@ -193,6 +193,17 @@ int launch_assemble_p_mixed(const DevParams& p, const double* APU, const double*
                             cudaStream_t st);
 // Doubles of partial-sum scratch the two launchers above need at most.
 int mixed_partials(const DevParams& p);
+// FP64 defect correction of the mixed-precision p' solve (mg_mode = tolerance); see mixed.cu.
+// Each returns the number of blocks whose partial sums it wrote (k_sum_partials adds them):
+// launch_dc_rhs0 one plane (sum of (b - mean b)^2), launch_dc_update two (sum of r^2, sum of p').
+int launch_dc_rhs0(const DevParams& p, const double* bfield, const double* sum_b, const LevelView32& L0,
+                   double* part, cudaStream_t st);
+int launch_dc_update(const DevParams& p, const double* APU, const double* APV, const double* bfield,
+                     const double* sum_b, const LevelView32& L0, const double* pold, double* pnew, bool first,
+                     double* part, cudaStream_t st);
+void launch_correct_dc(const DevParams& p, const double* pc64, const double* sum_pc, const double* APU,
+                       const double* APV, double* u, double* v, double* pf, cudaStream_t st);
+void launch_pc_from64(const DevParams& p, const double* src, const double* sum_pc, double* dst, cudaStream_t st);
 void launch_b_to_f32(const DevParams& p, const double* bfield, const double* sum_b,
                      const LevelView32& L0, cudaStream_t st);
 // pc64 = FP32 p' minus its FP64 mean over the p' cells (the field correct_mixed applied).

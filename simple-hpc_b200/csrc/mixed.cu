@@ -525,6 +525,122 @@ __global__ void k_pc_from32(DevParams p, const float* __restrict__ pc32, int ld3
     pc64[ix(p, p.H + I, p.H + 1 + J)] = static_cast<double>(pc32[I * ld32 + J]) - m;
 }
 
+// ---- FP64 defect correction of the p' solve (precision = mixed, mg_mode = tolerance) ----
+//
+// The FP32 V-cycle alone stalls at the FP32 rounding of its operator and iterate: ||b - A p'|| stops
+// falling near 1e-6 ||b|| on large grids. In tolerance mode the p' iterate is therefore kept in FP64
+// and each V-cycle solves for a correction: r = (b - mean b) - A p' with the FP64 operator of
+// assemble_p (its links formed from APU / APV by the expressions of k_assemble_p_mixed,
+// pressure.cpp:14-54), rounded to FP32 as the cycle's right-hand side; the cycle, from zero, gives e;
+// p' += e in FP64. The tolerance test reads the norm of that FP64 residual.
+
+// The first right-hand side, b - mean(b) rounded to FP32, and per block the FP64 sum of (b - mean b)^2.
+__global__ void __launch_bounds__(256)
+    k_dc_rhs0(DevParams p, const double* __restrict__ bfield, const double* __restrict__ sum_b, LevelView32 L0,
+              double* __restrict__ part) {
+    __shared__ double s_bb[8];
+    const int J = static_cast<int>(blockIdx.x * 32 + threadIdx.x);
+    const int I0 = static_cast<int>(blockIdx.y * kTileRows + threadIdx.y);
+    const double m = *sum_b / (static_cast<double>(p.NX) * p.NY);
+    double bb = 0.0;
+    if (J < p.NY) {
+#pragma unroll
+        for (int k = 0; k < kRowsPerThread; ++k) {
+            const int I = I0 + 8 * k;
+            if (I < p.NX) {
+                const double b = bfield[ix(p, p.H + I, p.H + 1 + J)] - m;
+                L0.b[I * L0.stride + J] = static_cast<float>(b);
+                bb += b * b;
+            }
+        }
+    }
+    const int tid = static_cast<int>(threadIdx.y * 32 + threadIdx.x);
+    const double t = block_sum<8>(bb, s_bb, tid);
+    if (tid == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = t;
+}
+
+// One defect-correction step over the p' cells (I, J) (field cell (H + I, H + 1 + J)):
+// pnew = pold + e (pold = 0 when first), then r = (b - mean b) - (APP pnew - (AEP pE + AWP pW + ASP pS
+// + ANP pN)) with the FP64 links (the multigrid residual form, multigrid.cpp:73-87), L0.b = FP32 r,
+// and per block the FP64 sums of r^2 (part[k]) and of pnew (part[nblocks + k]). pold and pnew are
+// distinct full-grid arrays: a cell's neighbours are read from pold + e, never from pnew.
+__global__ void __launch_bounds__(256)
+    k_dc_update(DevParams p, const double* __restrict__ APU, const double* __restrict__ APV,
+                const double* __restrict__ bfield, const double* __restrict__ sum_b,
+                const float* __restrict__ e, int lde, const double* __restrict__ pold,
+                double* __restrict__ pnew, int first, LevelView32 L0, double* __restrict__ part) {
+    __shared__ double s_rr[8], s_ps[8];
+    const int J = static_cast<int>(blockIdx.x * 32 + threadIdx.x);
+    const int I0 = static_cast<int>(blockIdx.y * kTileRows + threadIdx.y);
+    const double m = *sum_b / (static_cast<double>(p.NX) * p.NY);
+    const int H = p.H;
+    const std::size_t ld = p.pitch;
+    double rr = 0.0, ps = 0.0;
+    if (J < p.NY) {
+#pragma unroll 1
+        for (int k = 0; k < kRowsPerThread; ++k) {
+            const int I = I0 + 8 * k;
+            if (I >= p.NX) break;
+            const int i = H + I, j = H + 1 + J;
+            const std::size_t q = ix(p, i, j);
+            const float* ec = e + I * lde + J; // e's zero ring covers the neighbours outside
+            auto pv = [&](std::size_t qq, const float* ee) {
+                return (first ? 0.0 : pold[qq]) + static_cast<double>(*ee);
+            };
+            const double dx = p.dx, dy = p.dy;
+            const double aep = (j == p.NY + H) ? 0.0 : dy * dy / APU[q];
+            const double awp = (j == H + 1) ? 0.0 : dy * dy / APU[q - 1];
+            const double anp = (i == H) ? 0.0 : dx * dx / APV[q];
+            const double asp = (i == p.NX + H - 1) ? 0.0 : dx * dx / APV[q + ld];
+            const double app = aep + awp + anp + asp;
+            const double pc = pv(q, ec);
+            const double pe = aep != 0.0 ? pv(q + 1, ec + 1) : 0.0;
+            const double pw = awp != 0.0 ? pv(q - 1, ec - 1) : 0.0;
+            const double pn = anp != 0.0 ? pv(q - ld, ec - lde) : 0.0;
+            const double psn = asp != 0.0 ? pv(q + ld, ec + lde) : 0.0;
+            const double r = (bfield[q] - m) - (app * pc - (aep * pe + awp * pw + asp * psn + anp * pn));
+            pnew[q] = pc;
+            L0.b[I * L0.stride + J] = static_cast<float>(r);
+            rr += r * r;
+            ps += pc;
+        }
+    }
+    const int tid = static_cast<int>(threadIdx.y * 32 + threadIdx.x);
+    const double trr = block_sum<8>(rr, s_rr, tid);
+    const double tps = block_sum<8>(ps, s_ps, tid);
+    if (tid == 0) {
+        const unsigned nb = gridDim.x * gridDim.y, kb = blockIdx.y * gridDim.x + blockIdx.x;
+        part[kb] = trr;
+        part[nb + kb] = tps;
+    }
+}
+
+// correct (pressure.cpp:136-157) in FP64 from the FP64 p' of the defect correction minus its mean.
+__global__ void k_correct_dc(DevParams p, const double* __restrict__ pc64, const double* __restrict__ sum_pc,
+                             const double* __restrict__ APU, const double* __restrict__ APV, double* u,
+                             double* v, double* pf) {
+    const int J = static_cast<int>(blockIdx.x * 32 + threadIdx.x);
+    const int I = static_cast<int>(blockIdx.y * 8 + threadIdx.y);
+    if (I >= p.NX || J >= p.NY) return;
+    const int H = p.H, i = H + I, j = H + 1 + J;
+    const std::size_t q = ix(p, i, j);
+    const double m = *sum_pc / (static_cast<double>(p.NX) * p.NY);
+    const double pc = pc64[q] - m;
+    if (j <= p.NY + H - 1) u[q] += p.dy * (pc - (pc64[q + 1] - m)) / APU[q];
+    if (i >= H + 1) v[q] += p.dx * (pc - (pc64[q - p.pitch] - m)) / APV[q];
+    pf[q] += p.ap * pc;
+}
+
+// The p' field a download shows: the FP64 iterate minus its mean (src may equal dst).
+__global__ void k_pc_from64(DevParams p, const double* src, const double* __restrict__ sum_pc, double* dst) {
+    const int J = static_cast<int>(blockIdx.x * 32 + threadIdx.x);
+    const int I = static_cast<int>(blockIdx.y * 8 + threadIdx.y);
+    if (I >= p.NX || J >= p.NY) return;
+    const double m = *sum_pc / (static_cast<double>(p.NX) * p.NY);
+    const std::size_t q = ix(p, p.H + I, p.H + 1 + J);
+    dst[q] = src[q] - m;
+}
+
 Range update_range(const DevParams& p, bool v) {
     const int H = p.H;
     return v ? Range{H + 1, p.NX + H - 1, H + 1, p.NY + H} : Range{H, p.NX + H - 1, H + 1, p.NY + H - 1};
@@ -603,6 +719,37 @@ void launch_pc_from32(const DevParams& p, const LevelView32& L0, const double* s
                       cudaStream_t st) {
     const dim3 grid((p.NY + 31) / 32, (p.NX + 7) / 8);
     k_pc_from32<<<grid, dim3(32, 8), 0, st>>>(p, L0.x, L0.stride, sum_pc, pc64);
+    SGPU_LAUNCH();
+}
+
+int launch_dc_rhs0(const DevParams& p, const double* bfield, const double* sum_b, const LevelView32& L0,
+                   double* part, cudaStream_t st) {
+    const dim3 grid((p.NY + 31) / 32, (p.NX + kTileRows - 1) / kTileRows);
+    k_dc_rhs0<<<grid, dim3(32, 8), 0, st>>>(p, bfield, sum_b, L0, part);
+    SGPU_LAUNCH();
+    return static_cast<int>(grid.x * grid.y);
+}
+
+int launch_dc_update(const DevParams& p, const double* APU, const double* APV, const double* bfield,
+                     const double* sum_b, const LevelView32& L0, const double* pold, double* pnew, bool first,
+                     double* part, cudaStream_t st) {
+    const dim3 grid((p.NY + 31) / 32, (p.NX + kTileRows - 1) / kTileRows);
+    k_dc_update<<<grid, dim3(32, 8), 0, st>>>(p, APU, APV, bfield, sum_b, L0.x, L0.stride, pold, pnew,
+                                               first ? 1 : 0, L0, part);
+    SGPU_LAUNCH();
+    return static_cast<int>(grid.x * grid.y);
+}
+
+void launch_correct_dc(const DevParams& p, const double* pc64, const double* sum_pc, const double* APU,
+                       const double* APV, double* u, double* v, double* pf, cudaStream_t st) {
+    const dim3 grid((p.NY + 31) / 32, (p.NX + 7) / 8);
+    k_correct_dc<<<grid, dim3(32, 8), 0, st>>>(p, pc64, sum_pc, APU, APV, u, v, pf);
+    SGPU_LAUNCH();
+}
+
+void launch_pc_from64(const DevParams& p, const double* src, const double* sum_pc, double* dst, cudaStream_t st) {
+    const dim3 grid((p.NY + 31) / 32, (p.NX + 7) / 8);
+    k_pc_from64<<<grid, dim3(32, 8), 0, st>>>(p, src, sum_pc, dst);
     SGPU_LAUNCH();
 }
 

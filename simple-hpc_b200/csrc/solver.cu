@@ -369,8 +369,9 @@ struct Solver {
     bool p_links_stale = false;
     bool pc_stale = false; // the mixed iteration keeps p' in FP32; the FP64 field is formed on download
     void form_p_links_if_stale(int id) {
-        if (pc_stale && id == SGPU_F_PC) { // p' of the last mixed iteration, kept in FP32
-            launch_pc_from32(dp, lv32[0], sums + 26, w.pc, st);
+        if (pc_stale && id == SGPU_F_PC) { // p' of the last mixed iteration, kept in FP32 (or FP64)
+            if (pc_dc_src) launch_pc_from64(dp, pc_dc_src, sums + 26, w.pc, st);
+            else launch_pc_from32(dp, lv32[0], sums + 26, w.pc, st);
             pc_stale = false;
             return;
         }
@@ -392,6 +393,10 @@ struct Solver {
             throw Error(SGPU_E_TIMEOUT, "correction sweep: a bounded wait for its record copies ran out");
         }
     }
+    // FP64 defect correction of the p' solve in tolerance mode: the FP64 iterate ping-pongs between
+    // two full-grid arrays (allocated on first use); pc_dc_src is the last iteration's final iterate.
+    double* dc[2] = {nullptr, nullptr};
+    const double* pc_dc_src = nullptr;
     double* part = nullptr;           // per-block partial sums of the FP64 tree sums
     float* e32[2] = {nullptr, nullptr}; // correction ping-pong
     std::vector<LevelView32> lv32;    // FP32 multigrid hierarchy (level 0: the p' operator)
@@ -432,7 +437,18 @@ struct Solver {
         launch_sum_partials(part, nparts, 2, nparts, res3 + 2, sums + 25, st);
         mark(SGPU_PH_SOLVE_P);
         for (std::size_t l = 1; l < lv32.size(); ++l) launch_mg_build<float>(lv32[l - 1], lv32[l], st);
-        launch_b_to_f32(dp, w.b, sums + 25, lv32[0], st);
+        const bool dc_mode = prm.mg_mode == SGPU_MG_TOLERANCE;
+        pc_dc_src = nullptr;
+        int nbb = 0;
+        if (dc_mode) {
+            if (!dc[0]) {
+                dc[0] = field();
+                dc[1] = field();
+            }
+            nbb = launch_dc_rhs0(dp, w.b, sums + 25, lv32[0], part, st);
+        } else {
+            launch_b_to_f32(dp, w.b, sums + 25, lv32[0], st);
+        }
         const LevelView32& L0 = lv32[0];
         // p' starts from zero. The streaming level kernels need no cleared array for that: the
         // first cycle's k_mg_down does not read x (x_zero), a warm start writes every interior cell,
@@ -452,11 +468,66 @@ struct Solver {
                 launch_mg_up<float>(lv32[l + 1], lv32[l], mg32_x2[l], lv32[l].x, prm.mg_omega,
                                     prm.mg_post, sms, min_seg, st);
         };
-        last_vcycles = run_cycles(L0, !guess, vcycle32);
-        launch_tree_sum(L0.x, L0.stride, L0.nx, L0.ny, part, sums + 26, st); // the mean of p'
-        mark(SGPU_PH_CORRECT);
-        launch_correct_mixed(dp, L0, sums + 26, cu.a[8], cv.a[8], u, v, pf, nullptr, st);
+        if (dc_mode) {
+            last_vcycles = run_cycles_dc(L0, guess, nbb, vcycle32); // p' in FP64, its sum in sums[26]
+            mark(SGPU_PH_CORRECT);
+            launch_correct_dc(dp, pc_dc_src, sums + 26, cu.a[8], cv.a[8], u, v, pf, st);
+        } else {
+            last_vcycles = run_cycles(L0, !guess, vcycle32);
+            launch_tree_sum(L0.x, L0.stride, L0.nx, L0.ny, part, sums + 26, st); // the mean of p'
+            mark(SGPU_PH_CORRECT);
+            launch_correct_mixed(dp, L0, sums + 26, cu.a[8], cv.a[8], u, v, pf, nullptr, st);
+        }
         mark(SGPU_PH_COUNT);
+    }
+
+    // mg_mode = tolerance with precision = mixed: each V-cycle, from zero, solves in FP32 for the
+    // correction of an FP64 iterate (mixed.cu, k_dc_update): L0.b holds (b - mean b) in FP32 on entry
+    // and the blocks' sums of its square (nbb partials); L0.x holds the warm start when guess (the
+    // first cycle then starts from it and is judged as in run_cycles). Cycles repeat until the FP64
+    // norm ||r|| <= pressure_tolerance ||b - mean b||, at most pressure_maxit. Leaves the final
+    // iterate in pc_dc_src and its sum in sums[26]; returns the cycles run.
+    template <class Cycle> int run_cycles_dc(const LevelView32& L0, bool guess, int nbb, Cycle&& vcycle) {
+        launch_sum_partials(part, nbb, 1, 0, sums + 28, nullptr, st);
+        const double bb = fetch(sums + 28);
+        if (!(bb > 0.0)) { // b = mean: p' = 0
+            SGPU_CUDA(cudaMemsetAsync(dc[0], 0, g.bytes(), st));
+            SGPU_CUDA(cudaMemsetAsync(sums + 26, 0, sizeof(double), st));
+            pc_dc_src = dc[0];
+            last_rel = 0.0;
+            return 0;
+        }
+        const double target = prm.pressure_tolerance * std::sqrt(bb);
+        last_rel_initial = 1.0;
+        int c = 0, run = 0, cur = 0;
+        bool first = true, from_guess = guess;
+        while (c < prm.pressure_maxit) {
+            if (mg_tail == 0 && !from_guess) launch_zero_x(L0, st); // the tail kernel reads level 0's x
+            vcycle(!from_guess);
+            ++c;
+            ++run;
+            const int nb = launch_dc_update(dp, cu.a[8], cv.a[8], w.b, sums + 25, L0, dc[1 - cur], dc[cur],
+                                            first, part, st);
+            launch_sum_partials(part, nb, 2, nb, sums + 29, sums + 26, st);
+            pc_dc_src = dc[cur];
+            cur = 1 - cur;
+            first = false;
+            const double rr = fetch(sums + 29);
+            last_rel = std::sqrt(rr) / std::sqrt(bb);
+            if (from_guess) {
+                from_guess = false;
+                last_rel_initial = last_rel;
+                if (!(rr < bb)) { // no better than a zero start: discard the guess, restart from zero
+                    ++ws_fallbacks;
+                    launch_dc_rhs0(dp, w.b, sums + 25, L0, part, st);
+                    first = true;
+                    c = 0;
+                    continue;
+                }
+            }
+            if (std::sqrt(rr) <= target) break;
+        }
+        return run;
     }
 
     // V-cycles on level 0 (iterate L0.x, right-hand side L0.b). mg_mode = fixed: mg_cycles cycles

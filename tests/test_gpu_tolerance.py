@@ -109,6 +109,8 @@ def test_fixed_mode_equals_tolerance_mode_with_same_cycle_count(sgpu_mod):
 
 
 def test_tolerance_mode_mixed(sgpu_mod):
+    """Mixed precision in tolerance mode: FP32 V-cycles on corrections inside FP64 defect correction,
+    so the FP64 operator's residual of the FP64 p' meets the tolerance (no FP32 rounding floor)."""
     tol = 1e-5
     cfg = cavity(128, mg_mode="tolerance", pressure_tolerance=tol, pressure_maxit=100,
                  precision="mixed")
@@ -117,14 +119,27 @@ def test_tolerance_mode_mixed(sgpu_mod):
         for it in range(3):
             s.outer_iteration()
             st = s.last_solve_stats()
-            rn32, bn32 = p_residual(s, p, b_minus_mean=True, fp32_operator=True)
             rn, bn = p_residual(s, p, b_minus_mean=True)
             print(f"it {it}: {st['mg_vcycles']} V-cycles, reported {st['rel_residual']:.3e}, "
-                  f"numpy FP32 operator {rn32 / bn32:.3e}, FP64 operator {rn / bn:.3e}")
+                  f"numpy FP64 operator {rn / bn:.3e}")
             assert 1 <= st["mg_vcycles"] <= 100
             assert st["rel_residual"] <= tol
-            # the FP32 operator's residual, recomputed in FP64 from the stored p' (its FP64 mean
-            # removed, which that operator's rows do not sum away exactly)
-            assert rn32 / bn32 <= 1.5 * tol
-            # against the FP64 operator the FP32 rounding of the coefficients shows as well
-            assert rn / bn <= 1e-2
+            assert rn / bn <= 1.01 * tol
+
+
+@pytest.mark.parametrize("n,tol", [(1024, 1e-5), (1024, 1e-8), (2048, 1e-5), (2048, 1e-8)])
+def test_tolerance_mode_mixed_reaches_tight_tolerances_at_scale(sgpu_mod, n, tol):
+    """At 1024^2 and 2048^2 the FP32-only V-cycle stalls above 1e-6; with the FP64 defect correction
+    the mixed solve reaches 1e-5 and 1e-8, checked on the downloaded FP64 system in numpy."""
+    cfg = cavity(n, mg_mode="tolerance", pressure_tolerance=tol, pressure_maxit=60, precision="mixed")
+    p = sgpu_mod.params_from_config(config_text(cfg))
+    with sgpu_mod.Solver(p) as s:
+        for it in range(2):
+            s.outer_iteration()
+            st = s.last_solve_stats()
+            rn, bn = p_residual(s, p, b_minus_mean=True)
+            print(f"{n}^2 it {it}: {st['mg_vcycles']} V-cycles, reported {st['rel_residual']:.3e}, "
+                  f"numpy FP64 operator {rn / bn:.3e}")
+            assert st["mg_vcycles"] < 60
+            assert st["rel_residual"] <= tol
+            assert rn / bn <= 1.01 * tol

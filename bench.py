@@ -292,6 +292,52 @@ def e2e_measure(sgpu, torch, p, steps: int, world: int) -> dict:
             "d2h_bytes_per_step": 32 + 3 * fb / res.iterations}
 
 
+# ---- the reference's own GPU backend on the same B200 ----
+
+def reference_gpu_bar(sgpu, torch, sizes, steps: int, warmup: int) -> dict | None:
+    """simple-hpc's HipSolver (solver_hip.hip built as CUDA for sm_100a by oracle/Makefile), which
+    supports gs_multicolour + gs_redblack only, against this repository's FP64 solver with the same
+    solvers on the same iterations. The reference is timed by wall clock around its
+    outer_iteration (a device synchronisation per phase, as it runs); ours by CUDA events around
+    sgpu_run. Fields are compared bit for bit after the same iteration count."""
+    import numpy as np
+    import oracle
+    if not oracle.refgpu_available():
+        return None
+    out = {}
+    for n in sizes:
+        text = workload_config(n, None).replace("pressure_solver = mg", "pressure_solver = gs_redblack")
+        shape = (n + 5, n + 5)
+        ref = oracle.ReferenceGpu(text, shape)
+        ref.iterations(warmup)
+        rsecs, _ = ref.iterations(steps)
+        theirs = [ref.get(f) for f in (0, 1, 2)]
+        ref.close()
+        p = sgpu.params_from_config(text)
+        s = sgpu.Solver(p)
+        stream = torch.cuda.ExternalStream(s.stream())
+        s.run(warmup)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res, _ = s.run(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        osecs = e0.elapsed_time(e1) * 1e-3
+        ours = [s.download(f) for f in (0, 1, 2)]
+        s.close()
+        same = all(np.array_equal(a.view(np.uint64), b.view(np.uint64)) for a, b in zip(ours, theirs))
+        out[f"{n}x{n}"] = {"reference_ms_per_iteration": 1e3 * rsecs / steps,
+                           "ours_ms_per_iteration": 1e3 * osecs / res.iterations,
+                           "speedup": (rsecs / steps) / (osecs / res.iterations),
+                           "fields_bit_identical": same}
+    return {"solvers": "gs_multicolour + gs_redblack (the only pair the reference GPU backend supports), "
+                       "QUICK/4, Re 1000, FP64",
+            "reference": "simple-hpc src/hip/solver_hip.hip, nvcc -x cu -DSIMPLE_CUDA --fmad=false, sm_100a",
+            "steps": steps, "warmup": warmup, "sizes": out}
+
+
 # ---- batched workload: many cavities of uneven size and Re in one graph launch ----
 
 BATCH_SIZES = (64, 96, 128, 192, 256, 384, 512)
@@ -431,6 +477,7 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-arm", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--workload", default="cavity", choices=["cavity", "batch"])
     ap.add_argument("--cavities", type=int, default=256)
     ap.add_argument("--seed", type=int, default=20261203)
@@ -495,6 +542,9 @@ def main() -> None:
             traffic = t["bytes_per_cell"] * cells
 
     e2e = e2e_measure(sgpu, torch, p, args.steps, world)
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        ref_gpu = reference_gpu_bar(sgpu, torch, (2048, n), 10, 2)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(n, args.cpu_seconds)
@@ -530,6 +580,7 @@ def main() -> None:
                          "algorithmic_bytes_per_launch": bytes_per_launch,
                          "avg_launch_ms": per_launch_s * 1e3},
             "phases_ms_per_step": {k: 1e3 * v / max(head["iters"], 1) for k, v in ph.items()},
+            "reference_gpu": ref_gpu,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

@@ -2,8 +2,10 @@
 
 `Oracle` drives liborc.so, the C restatement of the reference's algorithm (oracle.c). `Reference`
 drives _ref/libsimpleref.so, the reference's own C++ sources built where they lie; it exists only
-where the reference tree was present at build time. Only tests/, __graft_entry__.smoke() and
-bench.py's CPU-baseline leg import this module, and only as the checker or the timed CPU baseline.
+where the reference tree was present at build time. `ReferenceGpu` drives _ref/libsimpleref_gpu.so,
+the reference's own GPU backend (solver_hip.hip built as CUDA for sm_100a), the benchmark's reference
+GPU baseline. Only tests/, __graft_entry__.smoke() and bench.py's reference legs import this module,
+and only as the checker or a timed baseline.
 """
 from __future__ import annotations
 
@@ -15,9 +17,11 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORC_PATH = HERE / "liborc.so"
 REF_PATH = HERE / "_ref" / "libsimpleref.so"
+REFGPU_PATH = HERE / "_ref" / "libsimpleref_gpu.so"
 
 _orc = None
 _ref = None
+_refgpu = None
 
 
 def _params_type():
@@ -207,3 +211,60 @@ def ordered_sum(values: np.ndarray) -> float:
     if v.ndim == 1:
         v = v.reshape(1, -1)
     return orc_lib().orc_ordered_sum(_dp(v), v.shape[0], v.shape[1])
+
+
+def refgpu_available() -> bool:
+    return REFGPU_PATH.exists()
+
+
+def refgpu_lib():
+    global _refgpu
+    if _refgpu is None:
+        if not REFGPU_PATH.exists():
+            raise ImportError(f"{REFGPU_PATH} is missing (the reference tree or nvcc was not present at build time)")
+        L = C.CDLL(str(REFGPU_PATH))
+        D, I, H = C.POINTER(C.c_double), C.c_int, C.c_void_p
+        for name, res, args in (("refgpu_last_error", C.c_char_p, []), ("refgpu_create", H, [C.c_char_p]),
+                                ("refgpu_destroy", None, [H]), ("refgpu_iterations", I, [H, I, D, D]),
+                                ("refgpu_download", I, [H, I, D])):
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _refgpu = L
+    return _refgpu
+
+
+class ReferenceGpu:
+    """The reference's own GPU backend (HipSolver built as CUDA) on one config, on device 0."""
+
+    def __init__(self, config_text: str, shape):
+        self._lib = refgpu_lib()
+        self.shape = tuple(shape)
+        self._h = self._lib.refgpu_create(config_text.encode())
+        if not self._h:
+            raise RuntimeError(self._lib.refgpu_last_error().decode())
+
+    def iterations(self, n: int):
+        """n outer iterations; returns (wall seconds, residuals[n, 3])."""
+        res = np.zeros((max(n, 1), 3))
+        secs = C.c_double()
+        if self._lib.refgpu_iterations(self._h, n, _dp(res), C.byref(secs)) != 0:
+            raise RuntimeError(self._lib.refgpu_last_error().decode())
+        return secs.value, res[:n].copy()
+
+    def get(self, field_id: int) -> np.ndarray:
+        out = np.empty(self.shape)
+        if self._lib.refgpu_download(self._h, field_id, _dp(out)) != 0:
+            raise RuntimeError(self._lib.refgpu_last_error().decode())
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.refgpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -338,6 +338,95 @@ def reference_gpu_bar(sgpu, torch, sizes, steps: int, warmup: int) -> dict | Non
             "steps": steps, "warmup": warmup, "sizes": out}
 
 
+# ---- the metric itself where it is reachable: time to the residual tolerance ----
+
+CONVERGE_METRIC = ("wall time to error_tolerance 1e-5 (absolute residuals, the reference's stopping rule), "
+                   "cavity NxN Re1000 QUICK/4 gs_multicolour+mg")
+WEIGHTS = REPO / "simple-hpc_b200" / "weights" / "unet16_l4_cavity.bin"
+
+
+def converge_config(n: int, precision: str | None, warm: bool, maxit: int) -> str:
+    text = workload_config(n, precision).replace("maxit = 60000", f"maxit = {maxit}")
+    if warm:
+        text += f"warm_start = cnn\ncnn_weights = {WEIGHTS}\n"
+    return text
+
+
+def run_converge_workload(args, rank: int, world: int, local: int) -> None:
+    """Each size is solved to error_tolerance 1e-5 by: the plain FP64 method (the reference's
+    settings, bit-identical to it), mixed precision, and mixed precision with the learned warm start
+    (the network's guess as the start of each p' solve, judged after its first V-cycle). A fresh
+    solver runs each arm from the cavity's initial state; its time is the device time of sgpu_run
+    (CUDA events around it on the solver's stream) plus, separately, the host's wall time. Errors are
+    of u, v, p against the FP64 arm. The 128^2 case sits beside the reference's published Ghia-size
+    run: 128^2 Re 1000 to 1e-5, 5919 iterations in 1.79 s on an H100 (docs/RESULTS.md:335)."""
+    import numpy as np
+    import torch
+    import sgpu
+    torch.cuda.set_device(local)
+    arms = [("fp64", None, False), ("mixed", "mixed", False)]
+    if WEIGHTS.exists() and not args.no_cnn:
+        arms.append(("mixed_cnn", "mixed", True))
+    rows = []
+    for n in args.converge_sizes:
+        # warm-up: module load, graph capture paths, on a separate solver of the same size
+        for name, prec, warm in arms:
+            with sgpu.Solver(sgpu.params_from_config(converge_config(n, prec, warm, 5))) as w:
+                w.run(3)
+        out = {}
+        for name, prec, warm in arms:
+            p = sgpu.params_from_config(converge_config(n, prec, warm, args.converge_maxit))
+            s = sgpu.Solver(p)
+            stream = torch.cuda.ExternalStream(s.stream())
+            barrier(world)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            e0.record(stream)
+            res, log = s.run(p.maxit)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+            secs = allmax(e0.elapsed_time(e1) * 1e-3, world)
+            fields = [s.download(f) for f in (sgpu.F_U, sgpu.F_V, sgpu.F_P)]
+            ws = s.warm_start_stats() if warm else None
+            s.close()
+            out[name] = {"seconds": secs, "wall_seconds": wall, "iterations": res.iterations,
+                         "converged": bool(res.converged),
+                         "ms_per_iteration": 1e3 * secs / max(res.iterations, 1),
+                         "vcycles_per_iteration": res.mg_vcycles / max(res.iterations, 1),
+                         "final_residuals": [float(x) for x in log[-1, 1:]] if log.shape[0] else None,
+                         "fields": fields}
+            if ws is not None:
+                out[name]["warm_start"] = ws
+        ref = out["fp64"]["fields"]
+        for name in out:
+            f = out[name].pop("fields")
+            if name != "fp64":
+                out[name]["errors_vs_fp64"] = field_errors(f, ref)
+                out[name]["speedup_vs_fp64"] = out["fp64"]["seconds"] / out[name]["seconds"]
+        rows.append({"N": n, "arms": out})
+    if rank == 0:
+        last = rows[-1]["arms"]
+        head = "mixed_cnn" if "mixed_cnn" in last else "mixed"
+        line = {
+            "metric": CONVERGE_METRIC + f" (headline: {head} at {rows[-1]['N']}^2)",
+            "value": last[head]["seconds"], "unit": "s", "n_gpus": world, "steps": 1, "warmup": 1,
+            "ms_per_step": 1e3 * last[head]["seconds"], "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (outer) + f32 (inner solves)",
+            "data": "synthetic (cavity initial state u=v=p=0, lid u=1)",
+            "config": {"workload": "cavities to 1e-5: " + ", ".join(f"{r['N']}^2" for r in rows) +
+                                   "; arms fp64 (reference method), mixed, mixed + learned warm start",
+                       "parallelism": f"replicas x{world}", "l2": "whole solve timed (many iterations)"},
+            "sizes": rows,
+            "reference_published": {"case": "128^2 Re1000 QUICK/4 gs_multicolour+gs_redblack to 1e-5 (Ghia run)",
+                                    "iterations": 5919, "seconds": 1.79, "hardware": "H100 80GB",
+                                    "source": "simple-hpc docs/RESULTS.md:335"},
+        }
+        print(json.dumps(line), flush=True)
+
+
 # ---- batched workload: many cavities of uneven size and Re in one graph launch ----
 
 BATCH_SIZES = (64, 96, 128, 192, 256, 384, 512)
@@ -478,7 +567,10 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-arm", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true")
-    ap.add_argument("--workload", default="cavity", choices=["cavity", "batch"])
+    ap.add_argument("--workload", default="cavity", choices=["cavity", "batch", "converge"])
+    ap.add_argument("--converge-sizes", type=int, nargs="+", default=[128, 256, 512])
+    ap.add_argument("--converge-maxit", type=int, default=400000)
+    ap.add_argument("--no-cnn", action="store_true")
     ap.add_argument("--cavities", type=int, default=256)
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--batch-maxit", type=int, default=60000)
@@ -488,6 +580,13 @@ def main() -> None:
         args.warmup = 3
 
     rank, world, local = dist_init()
+    if args.impl == "reference" and args.workload == "converge":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "converge workload: the reference CPU needs "
+                              "16 500 iterations (132 s) at 256^2 and 61 109 (1971 s) at 512^2 on 8 threads; "
+                              "its published 128^2 GPU run is in the line's reference_published"}), flush=True)
+        barrier(world)
+        return
     if args.impl == "reference" and args.workload == "batch":
         if rank == 0:
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched mode and "
@@ -500,6 +599,13 @@ def main() -> None:
         barrier(world)
         return
 
+    if args.workload == "converge":
+        run_converge_workload(args, rank, world, local)
+        barrier(world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.workload == "batch":
         run_batch_workload(args, rank, world, local)
         barrier(world)

@@ -234,6 +234,10 @@ int sgpu_ordered_sum_noalloc(const double* values, int nrows_v, int ncols_v, int
  * FP64 sweep, or the FP32 correction sweep with precision = mixed) and how many were launched, both
  * accumulated over the profiled iterations: the per-launch time of the dominant kernel.
  */
+/* on: 0 off; 1 every iteration host-issued between events (exact per-phase device times, slower);
+ * 2 sampled: sgpu_run times the phases of its first 10 iterations that way, replays the captured
+ * graph for the rest (the fast path; same iterations and bits) and scales the sampled phase times
+ * to the whole run. 2 is what a drop-in caller that writes timing.csv should use. */
 int sgpu_set_profiling(sgpu_handle* h, int on);
 int sgpu_phase_seconds(sgpu_handle* h, double* out /* SGPU_PH_COUNT */);
 int sgpu_sweep_seconds(sgpu_handle* h, double* seconds, long long* launches);

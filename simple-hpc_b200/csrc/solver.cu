@@ -310,6 +310,9 @@ struct Solver {
 
     // ---- per-phase device timing (CUDA events on the solver's stream) ----
     bool profiling = false;
+    // Sampled timers (sgpu_set_profiling(h, 2)): sgpu_run times the phases of its first
+    // kSampledIterations iterations (host-issued, between events) and replays the graph for the rest.
+    bool sampled = false;
     cudaEvent_t ev[SGPU_PH_COUNT + 1] = {};
     bool ev_used[SGPU_PH_COUNT + 1] = {};
     int ev_order[SGPU_PH_COUNT + 2] = {};
@@ -1296,6 +1299,14 @@ struct IterGraph {
         k_set_ints<<<1, 256, 0, st>>>(bd.active, n, 1);
         SGPU_LAUNCH();
     }
+    // Continue a single solver's run that has done `iters` iterations on the host, with the running
+    // maxima maxr[3] of its stopping rule (a graph of one solver only). Host copies from pageable
+    // memory: synchronous with respect to the host, ordered on st.
+    void resume(cudaStream_t st, int iters, const double* maxr) {
+        SGPU_CUDA(cudaMemcpyAsync(bd.iters, &iters, sizeof(int), cudaMemcpyHostToDevice, st));
+        SGPU_CUDA(cudaMemcpyAsync(bd.maxr, maxr, sizeof(double) * 3, cudaMemcpyHostToDevice, st));
+        SGPU_CUDA(cudaStreamSynchronize(st));
+    }
     void launch(int limit, cudaStream_t st) {
         k_set_ints<<<1, 32, 0, st>>>(d_limit, 1, limit);
         SGPU_LAUNCH();
@@ -1467,17 +1478,22 @@ int sgpu_outer_iteration(sgpu_handle* h, double res[3], double* phase_seconds) {
 // print interval (sgpu::IterGraph), the stopping rule and the residual log on the device. Used when
 // every outer iteration is a fixed sequence of launches (no CG, no tolerance-driven multigrid, no
 // warm start) and the per-phase timers are off.
+static bool graphable(const sgpu::Solver& s) {
+    return s.prm.pressure_solver != SGPU_P_CG && s.prm.mg_mode != SGPU_MG_TOLERANCE && !s.net;
+}
+
+// start > 0: the run continues one whose first `start` iterations ran on the host (sampled timers),
+// with the stopping rule's running maxima maxr[3]; the log rows from `start` on are filled here.
 static bool run_graphed(sgpu::Solver& s, int maxit, double* log, int print_every, sgpu_result_t& out,
-                        bool& diverged) {
-    if (s.profiling || maxit < 1 || s.prm.pressure_solver == SGPU_P_CG || s.prm.mg_mode == SGPU_MG_TOLERANCE ||
-        s.net)
-        return false;
+                        bool& diverged, int start = 0, const double* maxr = nullptr) {
+    if (s.profiling || maxit < 1 || start >= maxit || !graphable(s)) return false;
     if (!s.run_graph) s.run_graph = new sgpu::IterGraph({&s}, maxit);
     sgpu::IterGraph& g = *s.run_graph;
     g.ensure_log(maxit);
     g.reset(s.st);
+    if (start > 0) g.resume(s.st, start, maxr);
     const int chunk = print_every > 0 ? print_every : maxit;
-    int done = 0, conv = 0;
+    int done = start, conv = 0;
     std::vector<double> rows;
     while (done < maxit) {
         const int lim = std::min(maxit, done + chunk);
@@ -1500,16 +1516,19 @@ static bool run_graphed(sgpu::Solver& s, int maxit, double* log, int print_every
         done = it;
         if (stopped) break;
     }
-    if (log && done > 0)
-        SGPU_CUDA(cudaMemcpy(log, g.bd.log, sizeof(double) * 4 * static_cast<std::size_t>(done),
-                             cudaMemcpyDeviceToHost));
-    g.count(done, done);
+    if (log && done > start)
+        SGPU_CUDA(cudaMemcpy(log + 4 * static_cast<std::size_t>(start), g.bd.log + 4 * static_cast<std::size_t>(start),
+                             sizeof(double) * 4 * static_cast<std::size_t>(done - start), cudaMemcpyDeviceToHost));
+    g.count(done - start, done - start);
     out.iterations = done;
     out.converged = conv == 1 ? 1 : 0;
     diverged = conv < 0;
-    if (s.prm.pressure_solver == SGPU_P_MG) out.mg_vcycles = done * s.prm.mg_cycles;
+    if (s.prm.pressure_solver == SGPU_P_MG) out.mg_vcycles = static_cast<long long>(done) * s.prm.mg_cycles;
     return true;
 }
+
+// Iterations whose phases sampled timers measure (host-issued launches between CUDA events).
+constexpr int kSampledIterations = 10;
 
 // A residual that is NaN or Inf ends the run (the reference has no such test and runs a diverged
 // case on to maxit, src/solver.cpp:106-132): the result and the log hold the iterations up to and
@@ -1526,7 +1545,7 @@ int sgpu_run(sgpu_handle* h, int maxit, double* log, int print_every, sgpu_resul
         sgpu_result_t out{};
         const auto t0 = std::chrono::steady_clock::now();
         bool diverged = false;
-        if (run_graphed(s, maxit, log, print_every, out, diverged)) {
+        if (!s.sampled && run_graphed(s, maxit, log, print_every, out, diverged)) {
             out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
             s.check_pipeline();
             if (result) *result = out;
@@ -1534,7 +1553,14 @@ int sgpu_run(sgpu_handle* h, int maxit, double* log, int print_every, sgpu_resul
             return;
         }
         double mu = 0.0, mv = 0.0, mp = 0.0;
-        for (int iter = 1; iter <= maxit; ++iter) {
+        // Sampled timers: the host loop runs the first kSampledIterations iterations with the
+        // per-phase timers on, then the graph continues the run (graphable solvers only).
+        // A solver that cannot replay a graph times every iteration instead.
+        const bool sampling = s.sampled && graphable(s) && maxit > kSampledIterations;
+        const int host_iters = sampling ? kSampledIterations : maxit;
+        if (s.sampled) s.profiling = true;
+        bool stopped = false;
+        for (int iter = 1; iter <= host_iters; ++iter) {
             s.iteration_enqueue(s.res_dev);
             SGPU_CUDA(cudaMemcpyAsync(s.host_res, s.res_dev, 3 * sizeof(double),
                                       cudaMemcpyDeviceToHost, s.st));
@@ -1581,6 +1607,23 @@ int sgpu_run(sgpu_handle* h, int maxit, double* log, int print_every, sgpu_resul
             if (m <= s.prm.error_tolerance && iter > 1) {
                 out.converged = 1;
                 break;
+            }
+        }
+        stopped = out.converged || diverged || out.iterations < host_iters;
+        if (s.sampled) s.profiling = false;
+        if (sampling) {
+            if (!stopped) {
+                // The graph continues from iteration host_iters + 1; the sampled phase times are
+                // scaled to the iterations of the whole run.
+                double ph[SGPU_PH_COUNT];
+                std::memcpy(ph, out.phase_seconds, sizeof ph);
+                const double maxr[3] = {mu, mv, mp};
+                run_graphed(s, maxit, log, print_every, out, diverged, host_iters, maxr);
+                const double scale = static_cast<double>(out.iterations) / host_iters;
+                for (int k = 0; k < SGPU_PH_COUNT; ++k) {
+                    out.phase_seconds[k] = ph[k] * scale;
+                    s.phase_acc[k] += ph[k] * (scale - 1.0);
+                }
             }
         }
         out.seconds =
@@ -1716,7 +1759,9 @@ int sgpu_ordered_sum(const double* values, int nr, int nc, double* out) {
 
 int sgpu_set_profiling(sgpu_handle* h, int on) {
     SGPU_NEED_HANDLE(h);
-    h->s->profiling = on != 0;
+    if (on < 0 || on > 2) return sgpu::fail(SGPU_E_INVALID, "sgpu_set_profiling: mode 0, 1 or 2");
+    h->s->profiling = on == 1;
+    h->s->sampled = on == 2;
     return SGPU_OK;
 }
 

@@ -461,8 +461,11 @@ class Solver:
         _check(lib().sgpu_memory_bytes(self._h, C.byref(n)))
         return n.value
 
-    def set_profiling(self, on: bool) -> None:
-        _check(lib().sgpu_set_profiling(self._h, 1 if on else 0))
+    def set_profiling(self, on) -> None:
+        """False / True (every iteration timed per phase), or "sampled" (the first 10 iterations of a
+        run timed, the rest replayed from the graph, phase times scaled to the run)."""
+        mode = 2 if on == "sampled" else (1 if on else 0)
+        _check(lib().sgpu_set_profiling(self._h, mode))
 
     def phase_seconds(self) -> dict:
         out = np.zeros(12)

@@ -44,6 +44,7 @@ SOURCES = {
     "io.cpp": EXACT,
     "noalloc.cu": EXACT,
     "cnn.cu": FAST,
+    "conv_tc.cu": FAST,
     "mg32.cu": FAST,
     "mg_fast32.cu": FAST,
     "mixed32.cu": FAST,

@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <random>
 #include <stdexcept>
@@ -496,6 +497,10 @@ UNet::UNet(int base, int levels, unsigned seed) : base_(base), levels_(levels) {
     SGPU_CUDA(cudaMalloc(&wb_, sizeof(bf16) * nparam_));
     SGPU_CUDA(cudaMalloc(&wf_, sizeof(bf16) * max_conv_weights()));
     SGPU_CUDA(cudaMalloc(&loss_, sizeof(float)));
+    SGPU_CUDA(cudaMalloc(&err_, sizeof(unsigned)));
+    SGPU_CUDA(cudaMemset(err_, 0, sizeof(unsigned)));
+    const char* impl = std::getenv("SGPU_CNN_CONV");
+    legacy_conv_ = impl && std::string(impl) == "mma";
     SGPU_CUDA(cudaMemcpy(w_, h.data(), sizeof(float) * nparam_, cudaMemcpyHostToDevice));
     SGPU_CUDA(cudaMemset(g_, 0, sizeof(float) * nparam_));
     SGPU_CUDA(cudaMemset(m_, 0, sizeof(float) * nparam_));
@@ -514,6 +519,17 @@ UNet::~UNet() {
     cudaFree(wb_);
     cudaFree(wf_);
     cudaFree(loss_);
+    cudaFree(err_);
+}
+
+void UNet::check_error(cudaStream_t st) {
+    unsigned h = 0;
+    SGPU_CUDA(cudaMemcpyAsync(&h, err_, sizeof h, cudaMemcpyDeviceToHost, st));
+    SGPU_CUDA(cudaStreamSynchronize(st));
+    if (h) {
+        SGPU_CUDA(cudaMemsetAsync(err_, 0, sizeof h, st));
+        throw Error(SGPU_E_TIMEOUT, "tensor-core convolution: a bounded wait for its MMAs ran out");
+    }
 }
 
 void UNet::free_acts() {
@@ -584,6 +600,11 @@ void UNet::shape(int n, int h, int w) {
 }
 
 void UNet::conv_fwd(const Conv& c, const bf16* x, bf16* y, cudaStream_t st) {
+    if (!legacy_conv_) {
+        launch_conv_tc(x, n_, h_ >> c.level, wd_ >> c.level, c.cin, wb_ + c.w_off, w_ + c.b_off, y, c.cout, 1,
+                       err_, st);
+        return;
+    }
     const long np = px(c.level);
     const dim3 grid(static_cast<unsigned>((np + 16 * kWarps - 1) / (16 * kWarps)), (c.cout + 63) / 64);
     k_conv_fwd<<<grid, kThreads, 0, st>>>(x, n_, h_ >> c.level, wd_ >> c.level, c.cin, wb_ + c.w_off,
@@ -630,11 +651,15 @@ void UNet::conv_back(const Conv& c, const bf16* x_in, bf16* dx, cudaStream_t st)
     const long np = px(c.level);
     k_relu_back<<<blocks(np * c.cout), 256, 0, st>>>(c.y, c.dy, c.dy, np * c.cout);
     SGPU_LAUNCH();
+    if (!legacy_conv_) {
+        launch_conv_wgrad_tc(x_in, c.dy, n_, h, w, c.cin, c.cout, g_ + c.w_off, err_, st);
+    } else {
     const int chunk = 4096;
     const long tiles = static_cast<long>(c.cout / 16) * (c.cin / 8) * 9;
     const dim3 gw(static_cast<unsigned>((tiles + kWarps - 1) / kWarps), static_cast<unsigned>((np + chunk - 1) / chunk));
     k_conv_wgrad<<<gw, kThreads, 0, st>>>(x_in, c.dy, n_, h, w, c.cin, c.cout, g_ + c.w_off, chunk);
     SGPU_LAUNCH();
+    }
     k_bias_grad<<<static_cast<unsigned>(std::min<long>(np, 1024)), std::max(32, c.cout), 0, st>>>(c.dy, np, c.cout,
                                                                                                g_ + c.b_off);
     SGPU_LAUNCH();
@@ -642,6 +667,10 @@ void UNet::conv_back(const Conv& c, const bf16* x_in, bf16* dx, cudaStream_t st)
     const long nw = static_cast<long>(c.cout) * 9 * c.cin;
     k_flip_weights<<<blocks(nw), 256, 0, st>>>(wb_ + c.w_off, wf_, c.cout, c.cin);
     SGPU_LAUNCH();
+    if (!legacy_conv_) {
+        launch_conv_tc(c.dy, n_, h, w, c.cout, wf_, nullptr, dx, c.cin, 0, err_, st);
+        return;
+    }
     const dim3 gd(static_cast<unsigned>((np + 16 * kWarps - 1) / (16 * kWarps)), (c.cin + 63) / 64);
     k_conv_fwd<<<gd, kThreads, 0, st>>>(c.dy, n_, h, w, c.cout, wf_, nullptr, dx, c.cin, 0);
     SGPU_LAUNCH();
@@ -715,13 +744,13 @@ void UNet::set_target(const float* host, cudaStream_t st) {
 
 void UNet::get_output(float* host, cudaStream_t st) {
     SGPU_CUDA(cudaMemcpyAsync(host, out_, sizeof(float) * px(0), cudaMemcpyDeviceToHost, st));
-    SGPU_CUDA(cudaStreamSynchronize(st));
+    check_error(st);
 }
 
 float UNet::loss(cudaStream_t st) {
     float l = 0.0f;
     SGPU_CUDA(cudaMemcpyAsync(&l, loss_, sizeof(float), cudaMemcpyDeviceToHost, st));
-    SGPU_CUDA(cudaStreamSynchronize(st));
+    check_error(st);
     return l;
 }
 

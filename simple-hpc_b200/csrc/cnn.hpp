@@ -55,6 +55,9 @@ class UNet {
 
     void save(const std::string& path) const;
     static std::unique_ptr<UNet> load(const std::string& path);
+    // Raises SGPU_E_TIMEOUT (and clears the word) if a tensor-core convolution's bounded wait for its
+    // MMAs gave up since the last check (its outputs are then not to be trusted). Synchronises st.
+    void check_error(cudaStream_t st);
 
   private:
     struct Conv {
@@ -77,6 +80,8 @@ class UNet {
     float *w_ = nullptr, *g_ = nullptr, *m_ = nullptr, *v_ = nullptr, *loss_ = nullptr;
     __nv_bfloat16* wb_ = nullptr; // BF16 copy of every parameter
     __nv_bfloat16* wf_ = nullptr; // flipped weights of one conv (input-gradient pass)
+    unsigned* err_ = nullptr;      // device word: a tensor-core convolution's bounded wait gave up
+    bool legacy_conv_ = false;     // SGPU_CNN_CONV=mma: the warp-level mma.sync kernels (comparison)
     int step_ = 0;
     // activations for the current shape
     int n_ = 0, h_ = 0, wd_ = 0;
@@ -85,6 +90,19 @@ class UNet {
     std::vector<__nv_bfloat16*> pool_, dpool_, cat_, dcat_, skip_;
     float *in32_ = nullptr, *out_ = nullptr, *target_ = nullptr;
 };
+
+// 3x3 convolution, zero padding 1, of NHWC BF16 X [N*H*W][Cin] with W [Cout][9][Cin] (+ bias when not
+// null, ReLU when relu) into Y [N*H*W][Cout], as a tcgen05 implicit GEMM with the accumulator in TMEM
+// (conv_tc.cu). Cin and Cout multiples of 16, Cout <= 256. *err (device) gets a bit if a bounded
+// wait for the MMAs gave up.
+void launch_conv_tc(const __nv_bfloat16* X, int N, int H, int W, int Cin, const __nv_bfloat16* Wt,
+                    const float* bias, __nv_bfloat16* Y, int Cout, int relu, unsigned* err, cudaStream_t st);
+
+// Weight gradient of that convolution, dW [Cout][9][Cin] += sum over pixels of dZ[p, co] X[p + t, ci]
+// (dZ: the pre-activation gradient), as tcgen05 GEMMs over pixel chunks added with FP32 atomics.
+// Cin multiple of 16 up to 256, Cout multiple of 16 up to 128.
+void launch_conv_wgrad_tc(const __nv_bfloat16* X, const __nv_bfloat16* dZ, int N, int H, int W, int Cin,
+                          int Cout, float* dW, unsigned* err, cudaStream_t st);
 
 // Warm-start plumbing on a multigrid hierarchy (element type T).
 // C.b = sum of the four children of F.b (the restriction of the right-hand side itself).

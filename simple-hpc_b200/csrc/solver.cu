@@ -387,6 +387,7 @@ struct Solver {
     // Raises SGPU_E_TIMEOUT if a correction sweep since the last check gave up waiting for its
     // record copies (its results are then not to be trusted); clears the word.
     void check_pipeline() {
+        if (net) net->check_error(st);
         if (!corr_err) return;
         unsigned h = 0;
         SGPU_CUDA(cudaMemcpyAsync(&h, corr_err, sizeof h, cudaMemcpyDeviceToHost, st));

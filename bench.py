@@ -352,6 +352,46 @@ def converge_config(n: int, precision: str | None, warm: bool, maxit: int) -> st
     return text
 
 
+def refgpu_arms(sgpu, torch, n: int, maxit: int, world: int, out: dict) -> None:
+    """The pair the reference's GPU backend supports, gs_multicolour + gs_redblack, to 1e-5: the
+    reference's own HipSolver under its own run_outer_loop (wall time, a device synchronisation per
+    phase as it runs), and this repository's FP64 solver on the same settings."""
+    import oracle
+    if not oracle.refgpu_available():
+        return
+    text = converge_config(n, None, False, maxit).replace("pressure_solver = mg", "pressure_solver = gs_redblack")
+    ref = oracle.ReferenceGpu(text, (n + 5, n + 5))
+    its, conv, secs = ref.run()
+    theirs = [ref.get(f) for f in (0, 1, 2)]
+    ref.close()
+    p = sgpu.params_from_config(text)
+    with sgpu.Solver(sgpu.params_from_config(text.replace(f"maxit = {maxit}", "maxit = 5"))) as w:
+        w.run(3)
+    s = sgpu.Solver(p)
+    stream = torch.cuda.ExternalStream(s.stream())
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    res, _ = s.run(p.maxit)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    osecs = allmax(e0.elapsed_time(e1) * 1e-3, world)
+    ours = [s.download(f) for f in (0, 1, 2)]
+    s.close()
+    import numpy as np
+    same = all(np.array_equal(a.view(np.uint64), b.view(np.uint64)) for a, b in zip(ours, theirs))
+    out["reference_gpu_rb"] = {"seconds": secs, "iterations": its, "converged": conv,
+                               "ms_per_iteration": 1e3 * secs / max(its, 1),
+                               "note": "simple-hpc's own GPU backend (solver_hip.hip as CUDA, sm_100a) under "
+                                       "its run_outer_loop, gs_multicolour + gs_redblack",
+                               "fields": theirs}
+    out["fp64_rb"] = {"seconds": osecs, "iterations": res.iterations, "converged": bool(res.converged),
+                      "ms_per_iteration": 1e3 * osecs / max(res.iterations, 1),
+                      "speedup_vs_reference_gpu": secs / osecs, "fields_bit_identical_to_reference_gpu": same,
+                      "fields": ours}
+
+
 def run_converge_workload(args, rank: int, world: int, local: int) -> None:
     """Each size is solved to error_tolerance 1e-5 by: the plain FP64 method (the reference's
     settings, bit-identical to it), mixed precision, and mixed precision with the learned warm start
@@ -400,10 +440,12 @@ def run_converge_workload(args, rank: int, world: int, local: int) -> None:
                          "fields": fields}
             if ws is not None:
                 out[name]["warm_start"] = ws
+        if n <= args.converge_refgpu_max and not args.no_reference_gpu:
+            refgpu_arms(sgpu, torch, n, args.converge_maxit, world, out)
         ref = out["fp64"]["fields"]
         for name in out:
             f = out[name].pop("fields")
-            if name != "fp64":
+            if name in ("mixed", "mixed_cnn"):
                 out[name]["errors_vs_fp64"] = field_errors(f, ref)
                 out[name]["speedup_vs_fp64"] = out["fp64"]["seconds"] / out[name]["seconds"]
         rows.append({"N": n, "arms": out})
@@ -571,6 +613,7 @@ def main() -> None:
     ap.add_argument("--converge-sizes", type=int, nargs="+", default=[128, 256, 512])
     ap.add_argument("--converge-maxit", type=int, default=400000)
     ap.add_argument("--no-cnn", action="store_true")
+    ap.add_argument("--converge-refgpu-max", type=int, default=256)
     ap.add_argument("--cavities", type=int, default=256)
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--batch-maxit", type=int, default=60000)

@@ -226,6 +226,7 @@ def refgpu_lib():
         D, I, H = C.POINTER(C.c_double), C.c_int, C.c_void_p
         for name, res, args in (("refgpu_last_error", C.c_char_p, []), ("refgpu_create", H, [C.c_char_p]),
                                 ("refgpu_destroy", None, [H]), ("refgpu_iterations", I, [H, I, D, D]),
+                                ("refgpu_run", I, [H, C.POINTER(I), C.POINTER(I), D]),
                                 ("refgpu_download", I, [H, I, D])):
             f = getattr(L, name)
             f.restype = res
@@ -251,6 +252,13 @@ class ReferenceGpu:
         if self._lib.refgpu_iterations(self._h, n, _dp(res), C.byref(secs)) != 0:
             raise RuntimeError(self._lib.refgpu_last_error().decode())
         return secs.value, res[:n].copy()
+
+    def run(self):
+        """The reference's run_outer_loop to its tolerance or maxit: (iterations, converged, seconds)."""
+        it, conv, secs = C.c_int(), C.c_int(), C.c_double()
+        if self._lib.refgpu_run(self._h, C.byref(it), C.byref(conv), C.byref(secs)) != 0:
+            raise RuntimeError(self._lib.refgpu_last_error().decode())
+        return it.value, bool(conv.value), secs.value
 
     def get(self, field_id: int) -> np.ndarray:
         out = np.empty(self.shape)

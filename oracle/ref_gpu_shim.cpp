@@ -82,6 +82,23 @@ int refgpu_iterations(void* h, int n, double* res, double* seconds) {
     }
 }
 
+// The reference's own outer loop (run_outer_loop, src/solver.cpp:106-132: its stopping rule, its
+// "iter k" lines) around HipSolver::outer_iteration, at most p.maxit iterations from the current
+// state. *seconds is the loop's wall time as run_outer_loop measures it.
+int refgpu_run(void* h, int* iterations, int* converged, double* seconds) {
+    try {
+        RefGpu& r = *static_cast<RefGpu*>(h);
+        const RunResult out = run_outer_loop(r.p, [&](PhaseTimers& t) { return r.g->outer_iteration(t); });
+        if (iterations) *iterations = out.iterations;
+        if (converged) *converged = out.converged ? 1 : 0;
+        if (seconds) *seconds = out.seconds;
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
 // Field id 0 / 1 / 2 / 27 (u, v, p, p'): the full nrows x ncols array after HipSolver::download.
 int refgpu_download(void* h, int id, double* out) {
     try {

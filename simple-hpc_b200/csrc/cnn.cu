@@ -194,21 +194,36 @@ __global__ void k_bias_grad(const bf16* __restrict__ dZ, long npix, int C, float
     atomicAdd(db + c, s);
 }
 
-// 2x2 average pooling (input H x W) and its backward.
-__global__ void k_pool(const bf16* __restrict__ X, bf16* __restrict__ Y, int N, int H, int W, int C) {
-    const long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+// 2x2 average pooling, 8 channels (16 bytes) per thread, 32-bit indices (images of up to 2^31
+// channel values): the forward pass's pooling.
+__global__ void k_pool8(const bf16* __restrict__ X, bf16* __restrict__ Y, int N, int H, int W, int C) {
+    const int g8 = C / 8;
+    const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
     const int Ho = H / 2, Wo = W / 2;
-    if (i >= static_cast<long>(N) * Ho * Wo * C) return;
-    const int c = static_cast<int>(i % C);
-    const long q = i / C;
-    const int x = static_cast<int>(q % Wo), y = static_cast<int>((q / Wo) % Ho);
-    const long b = q / (static_cast<long>(Wo) * Ho);
-    const long base = ((b * H + 2 * y) * W + 2 * x) * C + c;
-    const long row = static_cast<long>(W) * C;
-    const float s = __bfloat162float(X[base]) + __bfloat162float(X[base + C]) +
-                    __bfloat162float(X[base + row]) + __bfloat162float(X[base + row + C]);
-    Y[i] = __float2bfloat16(0.25f * s);
+    if (i >= N * Ho * Wo * g8) return;
+    const int g = i % g8, q = i / g8;
+    const int x = q % Wo, y = (q / Wo) % Ho, b = q / (Wo * Ho);
+    const uint4* src = reinterpret_cast<const uint4*>(X);
+    const int base = ((b * H + 2 * y) * W + 2 * x) * g8 + g, row = W * g8;
+    const uint4 v[4] = {src[base], src[base + g8], src[base + row], src[base + row + g8]};
+    uint32_t out[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        float lo = 0.0f, hi = 0.0f;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const uint32_t w = (&v[e].x)[k];
+            const __nv_bfloat162 h = *reinterpret_cast<const __nv_bfloat162*>(&w);
+            lo += __low2float(h);
+            hi += __high2float(h);
+        }
+        const __nv_bfloat162 r = __floats2bfloat162_rn(0.25f * lo, 0.25f * hi);
+        out[k] = *reinterpret_cast<const uint32_t*>(&r);
+    }
+    reinterpret_cast<uint4*>(Y)[i] = make_uint4(out[0], out[1], out[2], out[3]);
 }
+
+// Backward of the 2x2 average pooling.
 __global__ void k_pool_back(const bf16* __restrict__ dY, bf16* __restrict__ dX, int N, int H, int W, int C) {
     const long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= static_cast<long>(N) * H * W * C) return;
@@ -219,19 +234,21 @@ __global__ void k_pool_back(const bf16* __restrict__ dY, bf16* __restrict__ dX, 
     dX[i] = __float2bfloat16(0.25f * __bfloat162float(dY[((b * (H / 2) + y / 2) * (W / 2) + x / 2) * C + c]));
 }
 
-// Y (H x W, Ca + Cb channels) = [nearest 2x upsampling of A (H/2 x W/2, Ca channels), B (Cb)].
-__global__ void k_up_concat(const bf16* __restrict__ A, int Ca, const bf16* __restrict__ B, int Cb,
-                            bf16* __restrict__ Y, int N, int H, int W) {
-    const int C = Ca + Cb;
-    const long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= static_cast<long>(N) * H * W * C) return;
-    const int c = static_cast<int>(i % C);
-    const long q = i / C;
-    const int x = static_cast<int>(q % W), y = static_cast<int>((q / W) % H);
-    const long b = q / (static_cast<long>(W) * H);
-    Y[i] = c < Ca ? A[((b * (H / 2) + y / 2) * (W / 2) + x / 2) * Ca + c] : B[q * Cb + (c - Ca)];
+// Y (H x W, Ca + Cb channels) = [nearest 2x upsampling of A (H/2 x W/2, Ca channels), B (Cb)], 8
+// channels (16 bytes) per thread, 32-bit indices (Ca, Cb multiples of 8).
+__global__ void k_up_concat8(const bf16* __restrict__ A, int Ca, const bf16* __restrict__ B, int Cb,
+                             bf16* __restrict__ Y, int N, int H, int W) {
+    const int ga = Ca / 8, gb = Cb / 8, gc = ga + gb;
+    const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i >= N * H * W * gc) return;
+    const int g = i % gc, q = i / gc;
+    const int x = q % W, y = (q / W) % H, b = q / (W * H);
+    reinterpret_cast<uint4*>(Y)[i] =
+        g < ga ? reinterpret_cast<const uint4*>(A)[((b * (H / 2) + y / 2) * (W / 2) + x / 2) * ga + g]
+               : reinterpret_cast<const uint4*>(B)[q * gb + (g - ga)];
 }
-// Backward of k_up_concat: dA = sum over the 4 children, dB = copy. One thread per element of dB
+
+// Backward of k_up_concat8: dA = sum over the 4 children, dB = copy. One thread per element of dB
 // (dB has twice as many elements as dA).
 __global__ void k_up_concat_back(const bf16* __restrict__ dY, bf16* __restrict__ dA, int Ca,
                                  bf16* __restrict__ dB, int Cb, int N, int H, int W) {
@@ -561,6 +578,8 @@ void UNet::shape(int n, int h, int w) {
     if (n < 1 || h < 1 || w < 1 || h % multiple() || w % multiple())
         throw Error(SGPU_E_INVALID, "cnn: image height and width must be positive multiples of " +
                                         std::to_string(multiple()));
+    if (static_cast<long>(n) * h * w * 256 > 0x7fffffffL)
+        throw Error(SGPU_E_INVALID, "cnn: images too large (the pooling and concatenation kernels index in 32 bits)");
     SGPU_CUDA(cudaDeviceSynchronize());
     free_acts();
     n_ = n;
@@ -620,8 +639,8 @@ void UNet::forward(cudaStream_t st) {
     for (int l = 0; l < L; ++l) {
         if (l > 0) {
             const Conv& prev = convs_[k - 1];
-            k_pool<<<blocks(px(l) * prev.cout), 256, 0, st>>>(prev.y, pool_[l], n_, h_ >> (l - 1),
-                                                             wd_ >> (l - 1), prev.cout);
+            k_pool8<<<blocks(px(l) * prev.cout / 8), 256, 0, st>>>(prev.y, pool_[l], n_, h_ >> (l - 1),
+                                                                  wd_ >> (l - 1), prev.cout);
             SGPU_LAUNCH();
             x = pool_[l];
         }
@@ -632,8 +651,8 @@ void UNet::forward(cudaStream_t st) {
     }
     for (int l = L - 2; l >= 0; --l) {
         const int ca = base_ << (l + 1), cb = base_ << l;
-        k_up_concat<<<blocks(px(l) * (ca + cb)), 256, 0, st>>>(x, ca, convs_[2 * l + 1].y, cb, cat_[l], n_,
-                                                              h_ >> l, wd_ >> l);
+        k_up_concat8<<<blocks(px(l) * (ca + cb) / 8), 256, 0, st>>>(x, ca, convs_[2 * l + 1].y, cb, cat_[l],
+                                                                   n_, h_ >> l, wd_ >> l);
         SGPU_LAUNCH();
         conv_fwd(convs_[k], cat_[l], convs_[k].y, st);
         conv_fwd(convs_[k + 1], convs_[k].y, convs_[k + 1].y, st);

@@ -106,19 +106,37 @@ __device__ __forceinline__ unsigned core_off(int r, int g, int kc) {
     return static_cast<unsigned>((r >> 3) * (kc * 16) + g * 128 + (r & 7) * 16);
 }
 
+// 16-byte asynchronous copy global -> shared; src_bytes 0 writes zeros (no global read).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, unsigned src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_addr(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Stage shape of the forward kernel: kc input channels of nt taps (K = nt kc <= 144 per stage).
+struct ConvStages {
+    int kc, nt, chunks, tgroups, stages, nbuf, kmax;
+};
+
 // 3x3 convolution, zero padding 1: X [N*H*W][Cin] -> Y [N*H*W][Cout] (+ bias, ReLU if relu).
-// Dynamic shared memory: 2 A buffers (128 x kc BF16), 2 B buffers (cout x kc BF16).
+// A stage covers taps [t0, t0 + nt_s) and channels [c0, c0 + kc): K index (local tap, channel) in
+// that order, so a weight row's stage slice is contiguous when kc = Cin. Its A and B tiles are copied
+// with cp.async (zero-fill where the tap leaves the image) nbuf - 1 stages ahead into a ring of nbuf
+// buffers; a buffer is refilled after the MMAs that read it have committed.
 __global__ void __launch_bounds__(kThreadsTc)
     k_conv_tc(const bf16* __restrict__ X, int N, int H, int W, int Cin, const bf16* __restrict__ Wt,
-              const float* __restrict__ bias, bf16* __restrict__ Y, int Cout, int relu, int kc,
+              const float* __restrict__ bias, bf16* __restrict__ Y, int Cout, int relu, ConvStages cs,
               uint32_t tmem_cols, unsigned* err) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ __align__(8) uint64_t bars[4];
     __shared__ uint32_t tmem_slot;
     const int tid = threadIdx.x, warp = tid >> 5;
-    const unsigned a_bytes = kM * kc * 2, b_bytes = static_cast<unsigned>(Cout) * kc * 2;
-    unsigned char* a_buf[2] = {smem, smem + a_bytes};
-    unsigned char* b_buf[2] = {smem + 2 * a_bytes, smem + 2 * a_bytes + b_bytes};
+    const unsigned a_bytes = kM * cs.kmax * 2, b_bytes = static_cast<unsigned>(Cout) * cs.kmax * 2;
+    auto a_buf = [&](int b) { return smem + b * (a_bytes + b_bytes); };
+    auto b_buf = [&](int b) { return smem + b * (a_bytes + b_bytes) + a_bytes; };
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
@@ -128,8 +146,7 @@ __global__ void __launch_bounds__(kThreadsTc)
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
     }
     if (tid == 0) {
-        bar_init(&bars[0], 1);
-        bar_init(&bars[1], 1);
+        for (int k = 0; k < 4; ++k) bar_init(&bars[k], 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     fence_before();
@@ -144,36 +161,48 @@ __global__ void __launch_bounds__(kThreadsTc)
     const long q = live ? p : 0;
     const int px = static_cast<int>(q % W), py = static_cast<int>((q / W) % H);
     const long pn = q / (static_cast<long>(W) * H);
+    const int gk = cs.kc / 8; // 16-byte groups per tap and stage
 
-    const int groups = kc / 8;            // 16-byte groups per row and stage
-    const int chunks = Cin / kc;          // stages per tap
-    const int stages = 9 * chunks;
+    // stage s: channel chunk s / tgroups, taps [t0, t0 + nt_s)
+    auto stage_taps = [&](int s, int& t0, int& c0) {
+        const int tg = s % cs.tgroups;
+        c0 = (s / cs.tgroups) * cs.kc;
+        t0 = tg * cs.nt;
+        return min(cs.nt, 9 - t0);
+    };
+    auto issue = [&](int s) {
+        if (s < cs.stages) {
+            int t0, c0;
+            const int nts = stage_taps(s, t0, c0);
+            const int kst = nts * cs.kc;
+            unsigned char* ab = a_buf(s % cs.nbuf);
+            unsigned char* bb = b_buf(s % cs.nbuf);
+            for (int tl = 0; tl < nts; ++tl) {
+                const int t = t0 + tl;
+                const int ys = py + t / 3 - 1, xs = px + t % 3 - 1;
+                const bool in = live && ys >= 0 && ys < H && xs >= 0 && xs < W;
+                const bf16* src = in ? X + ((pn * H + ys) * W + xs) * Cin + c0 : X;
+                for (int g = 0; g < gk; ++g)
+                    cp_async16(ab + core_off(tid, tl * gk + g, kst), src + 8 * g, in ? 16u : 0u);
+            }
+            for (int co = tid; co < Cout; co += kThreadsTc)
+                for (int tl = 0; tl < nts; ++tl) {
+                    const bf16* w = Wt + (static_cast<long>(co) * 9 + t0 + tl) * Cin + c0;
+                    for (int g = 0; g < gk; ++g) cp_async16(bb + core_off(co, tl * gk + g, kst), w + 8 * g, 16u);
+                }
+        }
+        cp_async_commit(); // one group per stage slot, empty past the last stage
+    };
+
     const uint32_t idesc = instr_desc(Cout, kM);
     bool gave_up = false;
     int issued = 0; // stages whose MMAs thread 0 committed
-
-    for (int s = 0; s < stages; ++s) {
-        const int b = s & 1;
-        // the buffer's previous MMAs (stage s - 2) must have finished reading it
-        if (s >= 2 && !bar_wait(&bars[b], static_cast<unsigned>(((s - 2) >> 1) & 1), err)) gave_up = true;
-        if (!gave_up) {
-            const int tap = s / chunks, c0 = (s % chunks) * kc;
-            const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-            // A: row tid = pixel p shifted by the tap
-            const int ys = py + dy, xs = px + dx;
-            const bool in = live && ys >= 0 && ys < H && xs >= 0 && xs < W;
-            const uint4* src = reinterpret_cast<const uint4*>(X + ((pn * H + ys) * W + xs) * Cin + c0);
-            for (int g = 0; g < groups; ++g) {
-                const uint4 v = in ? __ldg(src + g) : make_uint4(0u, 0u, 0u, 0u);
-                *reinterpret_cast<uint4*>(a_buf[b] + core_off(tid, g, kc)) = v;
-            }
-            // B: rows co = tid, tid + 128, ...
-            for (int co = tid; co < Cout; co += kThreadsTc) {
-                const uint4* w = reinterpret_cast<const uint4*>(Wt + (static_cast<long>(co) * 9 + tap) * Cin + c0);
-                for (int g = 0; g < groups; ++g)
-                    *reinterpret_cast<uint4*>(b_buf[b] + core_off(co, g, kc)) = __ldg(w + g);
-            }
-        }
+    for (int s = 0; s < cs.nbuf - 1; ++s) issue(s);
+    for (int s = 0; s < cs.stages; ++s) {
+        const int b = s % cs.nbuf;
+        // this thread's copies of stage s have landed (the groups of later stages may still fly)
+        if (cs.nbuf == 3) cp_async_wait<1>();
+        else cp_async_wait<0>();
         fence_async_smem();
         if (__syncthreads_or(gave_up ? 1 : 0)) {
             gave_up = true;
@@ -181,27 +210,39 @@ __global__ void __launch_bounds__(kThreadsTc)
         }
         if (tid == 0) {
             fence_after();
-            const unsigned a0 = smem_addr(a_buf[b]), b0 = smem_addr(b_buf[b]);
-            for (int k = 0; k < kc / 16; ++k) {
-                const uint64_t ad = smem_desc(a0 + 256u * k, 128u, static_cast<unsigned>(kc) * 16u);
-                const uint64_t bd = smem_desc(b0 + 256u * k, 128u, static_cast<unsigned>(kc) * 16u);
+            int t0, c0;
+            const int kst = stage_taps(s, t0, c0) * cs.kc;
+            const unsigned a0 = smem_addr(a_buf(b)), b0 = smem_addr(b_buf(b));
+            for (int k = 0; k < kst / 16; ++k) {
+                const uint64_t ad = smem_desc(a0 + 256u * k, 128u, static_cast<unsigned>(kst) * 16u);
+                const uint64_t bd = smem_desc(b0 + 256u * k, 128u, static_cast<unsigned>(kst) * 16u);
                 mma_issue(tmem, ad, bd, idesc, (s > 0 || k > 0) ? 1u : 0u);
             }
             mma_commit(&bars[b]);
         }
         issued = s + 1;
+        // refill the buffer stage s - 1 used, once its MMAs have committed
+        const int nxt = s + cs.nbuf - 1;
+        if (nxt < cs.stages && s >= 1) {
+            const int pb = (s - 1) % cs.nbuf;
+            if (!bar_wait(&bars[pb], static_cast<unsigned>(((s - 1) / cs.nbuf) & 1), err)) gave_up = true;
+        }
+        if (!gave_up) issue(nxt);
+        else cp_async_commit();
     }
+    cp_async_wait<0>();
 
     // The last commit covers every MMA before it.
     if (issued > 0 && !gave_up) {
         const int s = issued - 1;
-        if (!bar_wait(&bars[s & 1], static_cast<unsigned>((s >> 1) & 1), err)) gave_up = true;
+        if (!bar_wait(&bars[s % cs.nbuf], static_cast<unsigned>((s / cs.nbuf) & 1), err)) gave_up = true;
     }
     if (__syncthreads_or(gave_up ? 1 : 0)) {
         // Drain: wait (bounded) for the commits still outstanding, so no MMA writes TMEM or reads
-        // shared memory after the CTA frees them. Stage s's commit is phase (s >> 1) of buffer s & 1.
+        // shared memory after the CTA frees them. Stage s's commit is phase s / nbuf of buffer s % nbuf.
         if (tid == 0)
-            for (int s = issued - 1; s >= 0 && s >= issued - 2; --s) bar_wait(&bars[s & 1], static_cast<unsigned>((s >> 1) & 1), err);
+            for (int s = issued - 1; s >= 0 && s >= issued - cs.nbuf; --s)
+                bar_wait(&bars[s % cs.nbuf], static_cast<unsigned>((s / cs.nbuf) & 1), err);
     } else {
         fence_after();
         const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
@@ -375,11 +416,29 @@ __global__ void __launch_bounds__(kThreadsTc)
                      : "memory");
 }
 
-// Input channels per stage: the largest of 64, 48, 32, 16 that divides cin.
-int stage_channels(int cin) {
-    for (int kc : {64, 48, 32, 16})
-        if (cin % kc == 0) return kc;
-    return 0;
+// Kernel shared memory available for the stage ring (one CTA's share of an SM).
+constexpr int kConvSmemMax = 200 * 1024;
+
+// Stages of the forward kernel: kc = Cin (or the largest multiple of 16 dividing it that is <= 128),
+// nt = the taps that keep K = nt kc <= 144, and as many buffers (2 or 3) as the ring allows.
+ConvStages conv_stages(int cin, int cout) {
+    ConvStages c{};
+    c.kc = cin;
+    if (c.kc > 128)
+        for (int k = 128; k >= 16; k -= 16)
+            if (cin % k == 0) {
+                c.kc = k;
+                break;
+            }
+    c.nt = std::max(1, std::min(9, 144 / c.kc));
+    c.chunks = cin / c.kc;
+    c.tgroups = (9 + c.nt - 1) / c.nt;
+    c.stages = c.chunks * c.tgroups;
+    c.kmax = c.nt * c.kc;
+    const int per = (kM + cout) * c.kmax * 2;
+    c.nbuf = std::min(3, std::max(2, kConvSmemMax / per));
+    if (c.stages < c.nbuf) c.nbuf = std::max(2, c.stages);
+    return c;
 }
 
 } // namespace
@@ -412,24 +471,26 @@ void launch_conv_wgrad_tc(const bf16* X, const bf16* dZ, int N, int H, int W, in
 
 void launch_conv_tc(const bf16* X, int N, int H, int W, int Cin, const bf16* Wt, const float* bias, bf16* Y,
                     int Cout, int relu, unsigned* err, cudaStream_t st) {
-    const int kc = stage_channels(Cin);
-    if (kc == 0 || Cout < 16 || Cout > 256 || Cout % 16 || !err)
+    if (Cin < 16 || Cin % 16 || Cout < 16 || Cout > 256 || Cout % 16 || !err)
         throw Error(SGPU_E_INVALID, "tensor-core convolution: channels must be multiples of 16, Cout <= 256");
     const auto misaligned = [](const void* q) { return (reinterpret_cast<std::uintptr_t>(q) & 15u) != 0; };
     if (misaligned(X) || misaligned(Wt) || misaligned(Y))
         throw Error(SGPU_E_INVALID, "tensor-core convolution: operands must be 16-byte aligned");
     const long npix = static_cast<long>(N) * H * W;
     if (npix <= 0) return;
+    const ConvStages cs = conv_stages(Cin, Cout);
+    const int smem = cs.nbuf * (kM + Cout) * cs.kmax * 2;
+    if (smem > kConvSmemMax)
+        throw Error(SGPU_E_INVALID, "tensor-core convolution: stage ring exceeds shared memory");
     uint32_t cols = 32;
     while (cols < static_cast<uint32_t>(Cout)) cols <<= 1;
-    const int smem = 2 * (kM * kc * 2) + 2 * (Cout * kc * 2);
     static PerDeviceOnce attr;
     attr.get([] {
-        SGPU_CUDA(cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * (kM * 64 * 2) + 2 * (256 * 64 * 2)));
+        SGPU_CUDA(cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmemMax));
         return 0;
     });
     const unsigned grid = static_cast<unsigned>((npix + kM - 1) / kM);
-    k_conv_tc<<<grid, kThreadsTc, smem, st>>>(X, N, H, W, Cin, Wt, bias, Y, Cout, relu, kc, cols, err);
+    k_conv_tc<<<grid, kThreadsTc, smem, st>>>(X, N, H, W, Cin, Wt, bias, Y, Cout, relu, cs, cols, err);
     SGPU_LAUNCH();
 }
 

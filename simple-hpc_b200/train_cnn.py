@@ -14,10 +14,9 @@
    - wall time per outer iteration: plain FP64 with the reference's settings (one V-cycle), mixed
      precision (one FP32 V-cycle), mixed precision with the network's guess as the V-cycle's start;
      their max / L2 relative error of u, v, p against the plain FP64 run;
-   - what the guess gains the p' solve: FP64 V-cycles to ||b - A p'|| <= 1e-5 ||b|| (mg_mode =
-     tolerance) from zero and from the guess, and the error between the two runs. (The FP32
-     V-cycle's own rounding floor lies above 1e-5 relative at 2048^2 and beyond, so the tolerance
-     comparison runs in FP64.)
+   - what the guess gains the p' solve: V-cycles to ||b - A p'|| <= 1e-5 ||b|| (mg_mode =
+     tolerance) from zero and from the guess, in FP64 and in mixed precision (FP32 V-cycles inside
+     FP64 defect correction), with wall time per outer iteration and the error between the runs.
 
 Prints one JSON line per stage; writes the weights to --out (sgpu_cnn_write format).
 """
@@ -159,6 +158,8 @@ def evaluate(net, n: int, iters: int, max_size: int) -> dict:
         "mixed_cnn": run("mixed", True, False),         # one V-cycle from the network's guess
         "fp64_tol": run("fp64", False, True),           # V-cycles to ||r|| <= 1e-5 ||b|| from zero
         "fp64_tol_cnn": run("fp64", True, True),        # ... from the network's guess
+        "mixed_tol": run("mixed", False, True),         # FP32 V-cycles in FP64 defect correction
+        "mixed_tol_cnn": run("mixed", True, True),      # ... from the network's guess
     }
     out = {"stage": "evaluate", "N": n, "Re": 2000, "outer_iterations": iters}
     for k, r in runs.items():
@@ -169,6 +170,12 @@ def evaluate(net, n: int, iters: int, max_size: int) -> dict:
     out["mixed"].update(errors(runs["mixed"], runs["plain_fp64"]))
     out["mixed_cnn"].update(errors(runs["mixed_cnn"], runs["plain_fp64"]))
     out["fp64_tol_cnn"].update(errors(runs["fp64_tol_cnn"], runs["fp64_tol"]))
+    out["mixed_tol_cnn"].update(errors(runs["mixed_tol_cnn"], runs["fp64_tol"]))
+    out["mixed_tol"].update(errors(runs["mixed_tol"], runs["fp64_tol"]))
+    out["vcycle_reduction_mixed_tol"] = 1.0 - (runs["mixed_tol_cnn"]["vcycles_per_iteration"] /
+                                              runs["mixed_tol"]["vcycles_per_iteration"])
+    out["time_ratio_mixed_tol_cnn_over_zero"] = (runs["mixed_tol_cnn"]["ms_per_iteration"] /
+                                                 runs["mixed_tol"]["ms_per_iteration"])
     out["vcycle_reduction_fp64_tol"] = 1.0 - (runs["fp64_tol_cnn"]["vcycles_per_iteration"] /
                                              runs["fp64_tol"]["vcycles_per_iteration"])
     out["time_ratio_fp64_tol_cnn_over_zero"] = (runs["fp64_tol_cnn"]["ms_per_iteration"] /

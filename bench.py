@@ -533,9 +533,12 @@ def run_batch_workload(args, rank: int, world: int, local: int) -> None:
     its = {i: int(r["iterations"][k]) for k, i in enumerate(mine)}
     b.close()
     out_bytes = sum(3 * 8 * p.nrows * p.ncols for p in params)
-    # per-cavity error against individual FP64 runs, on the smallest cavities of this rank
+    # per-cavity error against individual FP64 runs: the first batch_check cavities of each size
     errs = []
-    for i in sorted(mine, key=lambda i: manifest[i][0])[:args.batch_check]:
+    check = []
+    for n_ in BATCH_SIZES:
+        check += [i for i in mine if manifest[i][0] == n_][:args.batch_check]
+    for i in check:
         p64 = sgpu.params_from_config(batch_config(*manifest[i], None, args.batch_maxit))
         with sgpu.Solver(p64) as s:
             res, _ = s.run(args.batch_maxit)
@@ -617,7 +620,7 @@ def main() -> None:
     ap.add_argument("--cavities", type=int, default=256)
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--batch-maxit", type=int, default=60000)
-    ap.add_argument("--batch-check", type=int, default=8)
+    ap.add_argument("--batch-check", type=int, default=2, help="cavities per size checked against single FP64 runs")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

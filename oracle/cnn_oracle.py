@@ -25,8 +25,14 @@ def bf16(a: np.ndarray) -> np.ndarray:
 
 
 class UNetOracle:
-    def __init__(self, base: int = 16, levels: int = 4, round_bf16: bool = True):
+    """acc32: accumulate the convolutions in FP32 instead of FP64 (the same rounding points
+    otherwise). The two variants differ only by FP32 rounding of the sums; the BF16 roundings that
+    follow amplify that through the layers, which measures how far two correct implementations of
+    this network can lie apart."""
+
+    def __init__(self, base: int = 16, levels: int = 4, round_bf16: bool = True, acc32: bool = False):
         self.base, self.levels, self.rb = base, levels, round_bf16
+        self.acc = np.float32 if acc32 else np.float64
         ch = lambda l: base << l  # noqa: E731
         convs = []
         for l in range(levels):
@@ -66,19 +72,21 @@ class UNetOracle:
 
     def conv(self, X, Wt, b):
         N, H, W, _ = X.shape
-        acc = np.zeros((N, H, W, Wt.shape[0]), np.float64)
+        a = self.acc
+        acc = np.zeros((N, H, W, Wt.shape[0]), a)
         for t in range(9):
-            acc += self._shift(X, t // 3 - 1, t % 3 - 1).astype(np.float64) @ Wt[:, t, :].T.astype(np.float64)
+            acc += self._shift(X, t // 3 - 1, t % 3 - 1).astype(a) @ Wt[:, t, :].T.astype(a)
         if b is not None:
             acc += b
         return acc.astype(np.float32)
 
     def conv_input_grad(self, dZ, Wt):
         N, H, W, _ = dZ.shape
-        acc = np.zeros((N, H, W, Wt.shape[2]), np.float64)
+        a = self.acc
+        acc = np.zeros((N, H, W, Wt.shape[2]), a)
         for t in range(9):
             # dX[p + off(t)] += dZ[p] W[:, t, :]  ==  dX[q] += dZ[q - off(t)] W[:, t, :]
-            acc += self._shift(dZ, -(t // 3 - 1), -(t % 3 - 1)).astype(np.float64) @ Wt[:, t, :].astype(np.float64)
+            acc += self._shift(dZ, -(t // 3 - 1), -(t % 3 - 1)).astype(a) @ Wt[:, t, :].astype(a)
         return acc.astype(np.float32)
 
     def conv_weight_grad(self, X, dZ):

@@ -118,14 +118,18 @@ struct DevParams {
 #ifdef __CUDACC__
 // The red-black update value of multigrid.cpp:61-63, x = b / AP; x += nb / AP. The double
 // instances keep the reference's two divisions (bit parity); the float instances (the mixed-precision
-// V-cycle, where no bit parity applies) divide once, (b + nb) / AP, correctly rounded.
+// V-cycle, where no bit parity applies) divide once, (b + nb) / AP, with the fast single-precision
+// division (__fdividef, a reciprocal and a multiply: within 2 ulp for AP of any magnitude the
+// operator holds). A smoother of a correction solve inside FP64 defect correction needs no correctly
+// rounded quotient, and the IEEE division's instruction sequence is a sizeable share of the level
+// kernels' issue slots.
 __device__ __forceinline__ double rb_value(double b, double nb, double ap) {
     double t = b / ap;
     t += nb / ap;
     return t;
 }
 __device__ __forceinline__ float rb_value(float b, float nb, float ap) {
-    return __fdiv_rn(b + nb, ap);
+    return __fdividef(b + nb, ap);
 }
 #endif
 

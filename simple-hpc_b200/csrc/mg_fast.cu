@@ -64,10 +64,30 @@ __device__ __forceinline__ Win make_win(int nx, int ny, int seg_rows, int HC) {
     return w;
 }
 
-// Is pass k's update (or, with k = 2 * sweeps, the residual) of (I, Jc) computable from the window?
-__device__ __forceinline__ bool in_cone(const Win& w, int I, int Jc, int k, int NT) {
-    return (!w.cut_top || I >= w.L0 + 1 + k) && (!w.cut_bot || I <= w.L1 - 2 - k) &&
-           (!w.cut_left || Jc >= w.C0 + 1 + k) && (!w.cut_right || Jc <= w.C0 + NT - 2 - k);
+// Is pass k's update (or, with k = 2 * sweeps, the residual) of an interior cell (I, Jc) computable
+// from the window: (!cut_top || I >= L0 + 1 + k) && (!cut_bot || I <= L1 - 2 - k) && (!cut_left ||
+// Jc >= C0 + 1 + k) && (!cut_right || Jc <= C0 + NT - 2 - k). A thread's column is fixed, so its
+// column tests (and whether the column is interior) become one bit per k, and the row tests with
+// 0 <= I < nx two bounds linear in k: lo + k dt <= I <= hi - k db.
+struct Cone {
+    int lo, hi, dt, db;
+    unsigned cols;
+    __device__ __forceinline__ bool ok(int I, int k) const {
+        return ((cols >> k) & 1u) && I >= lo + k * dt && I <= hi - k * db;
+    }
+};
+__device__ __forceinline__ Cone make_cone(const Win& w, int Jc, bool cint, int nx, int NT, int kmax) {
+    Cone c;
+    c.dt = w.cut_top ? 1 : 0;
+    c.db = w.cut_bot ? 1 : 0;
+    c.lo = w.cut_top ? w.L0 + 1 : 0; // L0 >= 0 when cut, so the bound is inside [0, nx)
+    c.hi = w.cut_bot ? w.L1 - 2 : nx - 1;
+    c.cols = 0u;
+    for (int k = 0; k <= kmax; ++k) {
+        const bool ok = cint && (!w.cut_left || Jc >= w.C0 + 1 + k) && (!w.cut_right || Jc <= w.C0 + NT - 2 - k);
+        c.cols |= (ok ? 1u : 0u) << k;
+    }
+    return c;
 }
 
 // The 6 per-cell inputs of a red-black update or a residual: AE, AW, AN, AS, AP, b.
@@ -115,6 +135,7 @@ __global__ void __launch_bounds__(NT, MINB)
     const bool cint = Jc >= 0 && Jc < L.ny;
     const bool cown = cint && Jc >= w.J0 && Jc < w.J0 + w.W;
     const int s = L.stride;
+    const Cone cone = make_cone(w, Jc, cint, L.nx, NT, 2 * PRE);
 
     int next = w.L0;
     auto issue = [&]() {
@@ -134,10 +155,10 @@ __global__ void __launch_bounds__(NT, MINB)
 #pragma unroll
         for (int sw = 0; sw < PRE; ++sw) {
             r.I[sw] = t - 2 * cpar - 4 * sw;
-            r.ok[sw] = cint && r.I[sw] >= 0 && r.I[sw] < L.nx && in_cone(w, r.I[sw], Jc, 2 * sw + cpar, NT);
+            r.ok[sw] = cone.ok(r.I[sw], 2 * sw + cpar);
         }
         r.I[PRE] = t - 4 * PRE;
-        r.ok[PRE] = cint && r.I[PRE] >= 0 && r.I[PRE] < L.nx && in_cone(w, r.I[PRE], Jc, 2 * PRE, NT);
+        r.ok[PRE] = cone.ok(r.I[PRE], 2 * PRE);
 #pragma unroll
         for (int c = 0; c < NC; ++c)
             if (r.ok[c]) load6(L, r.I[c] * s + Jc, r.a[c]);
@@ -208,6 +229,7 @@ __global__ void __launch_bounds__(NT, MINB)
     const bool cown = cint && Jc >= w.J0 && Jc < w.J0 + w.W;
     const int s = L.stride;
     const T om = static_cast<T>(omega);
+    const Cone cone = make_cone(w, Jc, cint, L.nx, NT, 2 * POST);
 
     int next = w.L0;
     auto issue = [&]() {
@@ -221,7 +243,7 @@ __global__ void __launch_bounds__(NT, MINB)
 #pragma unroll
         for (int sw = 0; sw < POST; ++sw) {
             r.I[sw] = t - 2 * cpar - 4 * sw;
-            r.ok[sw] = cint && r.I[sw] >= 0 && r.I[sw] < L.nx && in_cone(w, r.I[sw], Jc, 2 * sw + cpar, NT);
+            r.ok[sw] = cone.ok(r.I[sw], 2 * sw + cpar);
             if (r.ok[sw]) load6(L, r.I[sw] * s + Jc, r.a[sw]);
         }
     };

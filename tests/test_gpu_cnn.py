@@ -74,6 +74,11 @@ def test_tensor_core_convolutions_match_warp_mma(sgpu_mod, cnn_oracle, monkeypat
 
 
 def test_loss_and_gradients_match_oracle(sgpu_mod, cnn_oracle):
+    """The 4-level network's loss and gradients against the oracle. The GPU accumulates in FP32 and
+    the oracle in FP64, with BF16 rounding at the same points; a rounding that flips in one layer
+    perturbs every layer after it, so over 28 BF16-rounded layers the gradients of two correct
+    implementations lie a few percent apart. The bound is therefore the oracle's own spread: the
+    oracle with FP32 accumulation against the oracle with FP64 accumulation, per convolution."""
     params = cnn_oracle.init_params(16, 4, seed=12)
     rng = np.random.default_rng(2)
     x = rng.normal(size=(2, 32, 32, 2)).astype(np.float32)
@@ -83,17 +88,44 @@ def test_loss_and_gradients_match_oracle(sgpu_mod, cnn_oracle):
         loss, g = net.loss_grad(x, t)
     o = cnn_oracle.UNetOracle(16, 4)
     rloss, rg, _ = o.loss_grad(params, x, t)
+    _, sg, _ = cnn_oracle.UNetOracle(16, 4, acc32=True).loss_grad(params, x, t)
     print(f"loss {loss:.6f} vs oracle {rloss:.6f}")
     assert abs(loss - rloss) <= 1e-2 * abs(rloss)
-    worst = 0.0
     for k, ((cin, cout, _), (wo, bo)) in enumerate(zip(o.convs, o.offs)):
         e = rel_l2(g[wo:bo + cout], rg[wo:bo + cout])
-        worst = max(worst, e)
-        print(f"conv {k:2d} ({cin:3d} -> {cout:3d}): gradient relative L2 error {e:.2e}")
-        assert e < 5e-2
+        spread = rel_l2(sg[wo:bo + cout], rg[wo:bo + cout])
+        print(f"conv {k:2d} ({cin:3d} -> {cout:3d}): gradient relative L2 error {e:.2e}, "
+              f"oracle FP32-vs-FP64 spread {spread:.2e}")
+        assert e <= 2.0 * spread + 2e-3
     eh = rel_l2(g[o.head_w:], rg[o.head_w:])
-    print(f"head: {eh:.2e}; whole vector: {rel_l2(g, rg):.2e}")
-    assert eh < 2e-2 and rel_l2(g, rg) < 2e-2
+    whole, whole_spread = rel_l2(g, rg), rel_l2(sg, rg)
+    print(f"head: {eh:.2e}; whole vector: {whole:.2e} (oracle spread {whole_spread:.2e})")
+    assert eh < 2e-2 and whole <= 2.0 * whole_spread + 2e-3
+
+
+@pytest.mark.parametrize("base,levels", [(16, 1), (32, 1), (16, 2)])
+def test_shallow_network_gradients_within_one_percent(sgpu_mod, cnn_oracle, base, levels):
+    """Networks of 1 and 2 levels (2 and 6 convolutions): too shallow for rounding flips to cascade,
+    so the tcgen05 forward, input-gradient and weight-gradient kernels must match the oracle's
+    gradients to 1% per convolution (and the forward to 0.5%)."""
+    params = cnn_oracle.init_params(base, levels, seed=31 + base + levels)
+    rng = np.random.default_rng(7)
+    x = rng.normal(size=(2, 24, 40, 2)).astype(np.float32)
+    t = rng.normal(size=(2, 24, 40)).astype(np.float32)
+    with sgpu_mod.Cnn(base, levels) as net:
+        net.set_params(params)
+        out = net.forward(x)
+        loss, g = net.loss_grad(x, t)
+    o = cnn_oracle.UNetOracle(base, levels)
+    ref, _ = o.forward(params, x)
+    rloss, rg, _ = o.loss_grad(params, x, t)
+    ef = rel_l2(out, ref)
+    print(f"base {base} levels {levels}: forward {ef:.2e}, loss {loss:.6f} vs {rloss:.6f}")
+    assert ef < 5e-3
+    for k, ((cin, cout, _), (wo, bo)) in enumerate(zip(o.convs, o.offs)):
+        e = rel_l2(g[wo:bo + cout], rg[wo:bo + cout])
+        print(f"conv {k} ({cin} -> {cout}): {e:.2e}")
+        assert e < 1e-2
 
 
 def test_training_lowers_loss_and_weights_round_trip(sgpu_mod, tmp_path):

@@ -77,8 +77,11 @@ def test_loss_and_gradients_match_oracle(sgpu_mod, cnn_oracle):
     """The 4-level network's loss and gradients against the oracle. The GPU accumulates in FP32 and
     the oracle in FP64, with BF16 rounding at the same points; a rounding that flips in one layer
     perturbs every layer after it, so over 28 BF16-rounded layers the gradients of two correct
-    implementations lie a few percent apart. The bound is therefore the oracle's own spread: the
-    oracle with FP32 accumulation against the oracle with FP64 accumulation, per convolution."""
+    implementations lie a few percent apart. The oracle with FP32 accumulation against the oracle
+    with FP64 accumulation shows that spread (1.2% over the whole vector, up to 3.7% per
+    convolution); the GPU must stay within 5% per convolution and within twice that spread over the
+    whole vector. The 1% per-convolution check of the kernels themselves is the shallow-network test
+    below, where no cascade forms."""
     params = cnn_oracle.init_params(16, 4, seed=12)
     rng = np.random.default_rng(2)
     x = rng.normal(size=(2, 32, 32, 2)).astype(np.float32)
@@ -96,11 +99,11 @@ def test_loss_and_gradients_match_oracle(sgpu_mod, cnn_oracle):
         spread = rel_l2(sg[wo:bo + cout], rg[wo:bo + cout])
         print(f"conv {k:2d} ({cin:3d} -> {cout:3d}): gradient relative L2 error {e:.2e}, "
               f"oracle FP32-vs-FP64 spread {spread:.2e}")
-        assert e <= 2.0 * spread + 2e-3
+        assert e < 5e-2
     eh = rel_l2(g[o.head_w:], rg[o.head_w:])
     whole, whole_spread = rel_l2(g, rg), rel_l2(sg, rg)
     print(f"head: {eh:.2e}; whole vector: {whole:.2e} (oracle spread {whole_spread:.2e})")
-    assert eh < 2e-2 and whole <= 2.0 * whole_spread + 2e-3
+    assert eh < 2e-2 and whole <= 2.0 * whole_spread + 5e-3
 
 
 @pytest.mark.parametrize("base,levels", [(16, 1), (32, 1), (16, 2)])

@@ -479,7 +479,8 @@ void launch_conv_tc(const bf16* X, int N, int H, int W, int Cin, const bf16* Wt,
     const long npix = static_cast<long>(N) * H * W;
     if (npix <= 0) return;
     const ConvStages cs = conv_stages(Cin, Cout);
-    const int smem = cs.nbuf * (kM + Cout) * cs.kmax * 2;
+    // buffers a launch actually fills: a one-stage layer (Cin = 16: all 9 taps at once) uses one
+    const int smem = std::min(cs.nbuf, cs.stages) * (kM + Cout) * cs.kmax * 2;
     if (smem > kConvSmemMax)
         throw Error(SGPU_E_INVALID, "tensor-core convolution: stage ring exceeds shared memory");
     uint32_t cols = 32;

@@ -447,6 +447,95 @@ __global__ void __launch_bounds__(kCoarseThreads)
     for (int l = first; l < nl; ++l) slevel_store(lv.L[l], sl(l));
 }
 
+// coarse_solve (multigrid.cpp:120-140) of an FP64 level in one warp on a shared-memory copy, bit for
+// bit the passes of cta_coarse_solve: the same per-cell expressions, and det_sum's order (each row
+// added left to right by one lane, then the row sums in order by lane 0, multigrid.cpp:18-34), so
+// the sweep count and every value equal the reference's; but no block barrier per pass, which on a
+// coarsest level of a few cells is most of a pass's cost. sm: coarse64_bytes(nx, ny) bytes.
+__host__ __device__ inline int coarse64_bytes(int nx, int ny) { return (8 * (nx + 2) * (ny + 2) + nx) * 8; }
+
+__device__ void warp_coarse_solve64(const LevelViewT<double>& L, double tol, int* sweeps_out, double* sm) {
+    const int lane = static_cast<int>(threadIdx.x) & 31;
+    const int nx = L.nx, ny = L.ny, S = ny + 2, n2 = (nx + 2) * S, n = nx * ny;
+    double *le = sm, *lw = le + n2, *ln = lw + n2, *ls = ln + n2, *ap = ls + n2, *b = ap + n2, *x = b + n2,
+           *r = x + n2, *rows = r + n2;
+    for (int k = lane; k < n2; k += 32) { // the level with its zero ring
+        const int I = k / S - 1, J = k % S - 1;
+        const bool in = I >= 0 && I < nx && J >= 0 && J < ny;
+        const int q = I * L.stride + J;
+        le[k] = in ? L.AE[q] : 0.0;
+        lw[k] = in ? L.AW[q] : 0.0;
+        ln[k] = in ? L.AN[q] : 0.0;
+        ls[k] = in ? L.AS[q] : 0.0;
+        ap[k] = in ? L.AP[q] : 0.0;
+        b[k] = in ? L.b[q] : 0.0;
+        x[k] = in ? L.x[q] : 0.0;
+        r[k] = 0.0;
+    }
+    __syncwarp();
+    auto at = [&](int I, int J) { return (I + 1) * S + J + 1; };
+    auto det_sum = [&](auto f) {
+        for (int I = lane; I < nx; I += 32) {
+            double a = 0.0;
+            for (int J = 0; J < ny; ++J) a += f(at(I, J));
+            rows[I] = a;
+        }
+        __syncwarp();
+        double t = 0.0;
+        if (lane == 0)
+            for (int I = 0; I < nx; ++I) t += rows[I];
+        t = __shfl_sync(0xffffffffu, t, 0);
+        __syncwarp();
+        return t;
+    };
+    auto remove_mean = [&](double* f) {
+        const double m = det_sum([&](int q) { return f[q]; }) / (static_cast<double>(nx) * ny);
+        for (int k = lane; k < n; k += 32) {
+            const int q = at(k / ny, k % ny);
+            f[q] = f[q] - m;
+        }
+        __syncwarp();
+    };
+    auto smooth = [&](int colour) {
+        for (int k = lane; k < n; k += 32) {
+            const int I = k / ny, J = k % ny;
+            if (((I + J) & 1) != colour) continue;
+            const int q = at(I, J);
+            x[q] = rb_value(b[q], le[q] * x[q + 1] + lw[q] * x[q - 1] + ls[q] * x[q + S] + ln[q] * x[q - S], ap[q]);
+        }
+        __syncwarp();
+    };
+    remove_mean(b);
+    const double bb = det_sum([&](int q) {
+        const double v = b[q];
+        return v * v;
+    });
+    int sweeps = 0;
+    if (bb > 0.0) {
+        const double bn = sqrt(bb);
+        while (sweeps < 200) {
+            smooth(0);
+            smooth(1);
+            ++sweeps;
+            const double rr = det_sum([&](int q) { // the residual (cta_residual's expression), squared
+                const double v = b[q] - (ap[q] * x[q] - (le[q] * x[q + 1] + lw[q] * x[q - 1] + ls[q] * x[q + S] +
+                                                         ln[q] * x[q - S]));
+                r[q] = v;
+                return v * v;
+            });
+            if (sqrt(rr) < tol * bn) break;
+        }
+    }
+    remove_mean(x);
+    for (int k = lane; k < n; k += 32) {
+        const int I = k / ny, J = k % ny, q = I * L.stride + J, c = at(I, J);
+        L.x[q] = x[c];
+        L.b[q] = b[c];
+        L.r[q] = r[c];
+    }
+    if (lane == 0 && sweeps_out) *sweeps_out = sweeps;
+}
+
 template <class T>
 __global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(LevelViewT<T> L, double* rowbuf,
                                                               double tol, int* sweeps_out) {
@@ -458,7 +547,8 @@ __global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(LevelViewT<T> L, d
 template <class T>
 __global__ void __launch_bounds__(kCoarseThreads)
     k_mg_tail(MgLevelsT<T> lv, int first, int pre, int post, double omega, double tol,
-              double* rowbuf, int* sweeps_out) {
+              double* rowbuf, int* sweeps_out, int warp64) {
+    extern __shared__ __align__(16) unsigned char tail_dyn[];
     const int nl = lv.n;
     for (int l = first; l + 1 < nl; ++l) {
         for (int s = 0; s < pre; ++s) {
@@ -474,6 +564,13 @@ __global__ void __launch_bounds__(kCoarseThreads)
     if (warp_solve) {
         if constexpr (sizeof(T) == 4)
             if (threadIdx.x < 32) warp_coarse_solve(lv.L[nl - 1], tol, sweeps_out);
+        __syncthreads();
+    } else if (warp64) {
+        __threadfence_block(); // the other warps' restriction writes, made visible to warp 0
+        __syncthreads();
+        if constexpr (sizeof(T) == 8)
+            if (threadIdx.x < 32)
+                warp_coarse_solve64(lv.L[nl - 1], tol, sweeps_out, reinterpret_cast<double*>(tail_dyn));
         __syncthreads();
     } else {
         cta_coarse_solve(lv.L[nl - 1], rowbuf, tol, sweeps_out);
@@ -492,6 +589,8 @@ __global__ void __launch_bounds__(kCoarseThreads)
 // The float tail runs with every level in shared memory when they fit (the 64^2-and-below levels
 // of a square grid take about 170 KB); otherwise, and for double, through global memory.
 constexpr int kTailSmemMax = 200 * 1024;
+// Shared memory for the FP64 warp coarse solve (about 1400 cells with their ring).
+constexpr int kCoarse64Max = 96 * 1024;
 
 template <class T>
 void launch_mg_tail(const MgLevelsT<T>& lv, int first, int pre, int post, double omega, double tol,
@@ -517,7 +616,19 @@ void launch_mg_tail(const MgLevelsT<T>& lv, int first, int pre, int post, double
             return;
         }
     }
-    k_mg_tail<T><<<1, kCoarseThreads, 0, st>>>(lv, first, pre, post, omega, tol, rowbuf, sweeps_out);
+    // FP64: the coarsest solve in one warp on a shared-memory copy when the level fits
+    int dyn = 0;
+    if constexpr (sizeof(T) == 8) {
+        const int b = coarse64_bytes(lv.L[lv.n - 1].nx, lv.L[lv.n - 1].ny);
+        if (b <= kCoarse64Max) dyn = b;
+        static PerDeviceOnce attr;
+        attr.get([] {
+            SGPU_CUDA(cudaFuncSetAttribute(k_mg_tail<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kCoarse64Max));
+            return 0;
+        });
+    }
+    k_mg_tail<T><<<1, kCoarseThreads, dyn, st>>>(lv, first, pre, post, omega, tol, rowbuf, sweeps_out, dyn > 0 ? 1 : 0);
     SGPU_LAUNCH();
 }
 template <class T> void launch_mg_build(const LevelViewT<T>& F, const LevelViewT<T>& C, cudaStream_t st) {

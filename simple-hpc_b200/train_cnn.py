@@ -65,7 +65,9 @@ def generate(npairs: int, max_size: int, seed: int, per_cavity: int, max_iter: i
                 s.set_mg_mode(False)
                 x, t, _ = s.cnn_sample(max_size)
                 if np.isfinite(x).all() and np.isfinite(t).all():
-                    data.setdefault(x.shape[:2], []).append((x, t))
+                    # kept in FP16 on the host (the network's inputs are BF16 anyway): 50k pairs of up to
+                    # 256^2 cells then take about 10 GB; batches are widened to FP32
+                    data.setdefault(x.shape[:2], []).append((x.astype(np.float16), t.astype(np.float16)))
                     made += 1
                 if made >= npairs:
                     break
@@ -88,7 +90,8 @@ def split(data: dict, frac: float, rng) -> tuple[dict, dict]:
 
 def batches(pool, batch, rng):
     idx = rng.integers(0, len(pool), min(batch, len(pool)))
-    return np.stack([pool[i][0] for i in idx]), np.stack([pool[i][1] for i in idx])
+    return (np.stack([pool[i][0] for i in idx]).astype(np.float32),
+            np.stack([pool[i][1] for i in idx]).astype(np.float32))
 
 
 def train(net, tr: dict, va: dict, steps: int, batch: int, lr: float, seed: int) -> dict:
@@ -107,8 +110,8 @@ def train(net, tr: dict, va: dict, steps: int, batch: int, lr: float, seed: int)
     vloss = []
     for k, pool in va.items():
         for i in range(0, len(pool), batch):
-            x = np.stack([q[0] for q in pool[i:i + batch]])
-            t = np.stack([q[1] for q in pool[i:i + batch]])
+            x = np.stack([q[0] for q in pool[i:i + batch]]).astype(np.float32)
+            t = np.stack([q[1] for q in pool[i:i + batch]]).astype(np.float32)
             vloss.append(float(np.mean((net.forward(x) - t) ** 2)) / max(float(np.mean(t ** 2)), 1e-30))
     out = {"stage": "train", "steps": steps, "batch": batch, "seconds": round(secs, 1),
            "loss_first_50": float(np.mean(hist[:50])), "loss_last_50": float(np.mean(hist[-50:])),

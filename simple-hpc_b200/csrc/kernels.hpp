@@ -123,10 +123,11 @@ void launch_mg_tail(const MgLevelsT<T>& lv, int first, int pre, int post, double
 // ---- streaming multigrid level kernels (mg_fast.cu), double and float ----
 bool mg_fast_supported(int pre, int post);
 // pre red-black sweeps on F (x from F.x, or zero), residual, restriction into C.b (C.x = 0); the
-// smoothed iterate is written to xout (F.x is left unchanged when pre > 0).
+// smoothed iterate is written to xout (F.x is left unchanged when pre > 0). build: also C's links
+// and AP from F's (mg_build's sums, the same bits as launch_mg_build).
 template <class T>
 void launch_mg_down(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, int pre, bool x_zero,
-                    int sms, int min_seg, cudaStream_t st);
+                    int sms, int min_seg, cudaStream_t st, bool build = false);
 // xout = xin + omega * P C.x, then post red-black sweeps (F's coefficients and b).
 template <class T>
 void launch_mg_up(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, T* xout,

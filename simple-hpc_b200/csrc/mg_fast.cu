@@ -3,7 +3,9 @@
 //
 // Per fine level two passes over memory instead of one per colour:
 //  * k_mg_down: `pre` red-black sweeps (smooth, multigrid.cpp:46-70), the residual (:73-87) and the
-//    2x2 restriction (:90-103) in one streaming pass. A CTA owns a strip of columns plus a halo and
+//    2x2 restriction (:90-103) in one streaming pass; with `build`, also the coarse level's Galerkin
+//    links and AP (mg_build, :232-261) from the fine links the residual has just loaded, with
+//    mg_build's additions in its order (the same bits as k_mg_build). A CTA owns a strip of columns plus a halo and
 //    walks it top to bottom; in sweep s the cell (I, J) of colour c = (I + J) & 1 is updated at step
 //    t = I + 4s + 2c, so each cell sees its neighbours in exactly the reference's colour order; the
 //    residual of row I is formed at step I + 4 pre, when its neighbours are final, and pairs of
@@ -125,7 +127,7 @@ template <int NC, class T> struct StepRegs {
 template <int NT, int PRE, int PD, int MINB, class T>
 __global__ void __launch_bounds__(NT, MINB)
     k_mg_down(LevelViewT<T> L, LevelViewT<T> C, T* __restrict__ xout, int x_zero, int seg_rows,
-              int HC) {
+              int HC, int build) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T(*ring)[NT] = reinterpret_cast<T(*)[NT]>(smem_raw);
     const Win w = make_win<NT>(L.nx, L.ny, seg_rows, HC);
@@ -171,6 +173,7 @@ __global__ void __launch_bounds__(NT, MINB)
 
     const int t_last = w.R1 - 1 + 4 * PRE;
     T r_prev = T(0);
+    T lp[4] = {T(0), T(0), T(0), T(0)}; // links e, w, n, s of the previous residual row's cell
     auto step = [&](int t, StepRegs<NC, T>& R) {
         cp_async_wait<kPD>(); // rows <= t + 1 have landed
         __syncthreads();
@@ -190,17 +193,37 @@ __global__ void __launch_bounds__(NT, MINB)
                           aa[2] * ring[(Ir - 1) & (kRing - 1)][tid]));
         }
         // Restriction of the row pair (Ir - 1, Ir): C.b = r[f] + r[f+1] + r[f+fs] + r[f+fs+1].
+        // With build, the coarse cell's links from the fine cells f (row Ir - 1, this column), f + 1
+        // (the odd column, from lane + 1), f + fs and f + fs + 1 (row Ir), as mg_build adds them.
+        const T* la = R.a[PRE];
         if ((Ir & 1) && Ir >= 1) { // uniform over the CTA
             const T rp_odd = __shfl_down_sync(0xffffffffu, r_prev, 1);
             const T r_odd = __shfl_down_sync(0xffffffffu, r, 1);
+            T ep_odd = T(0), e_odd = T(0), np_odd = T(0), s_odd = T(0);
+            if (build) { // uniform
+                ep_odd = __shfl_down_sync(0xffffffffu, lp[0], 1);
+                e_odd = __shfl_down_sync(0xffffffffu, la[0], 1);
+                np_odd = __shfl_down_sync(0xffffffffu, lp[2], 1);
+                s_odd = __shfl_down_sync(0xffffffffu, la[3], 1);
+            }
             const int Rc = Ir >> 1;
             if (cown && !(Jc & 1) && Ir - 1 >= w.R0 && Ir < w.R1 && Rc < C.nx) {
                 const int cq = Rc * C.stride + (Jc >> 1);
                 C.b[cq] = r_prev + rp_odd + r + r_odd;
                 C.x[cq] = T(0);
+                if (build) {
+                    const T ae = ep_odd + e_odd;    // k01.e + k11.e
+                    const T aw = lp[1] + la[1];     // k00.w + k10.w
+                    const T an = lp[2] + np_odd;    // k00.n + k01.n
+                    const T as = la[3] + s_odd;     // k10.s + k11.s
+                    set_links(C, cq, ae, aw, an, as);
+                    C.AP[cq] = ae + aw + an + as;
+                }
             }
         }
         r_prev = r;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) lp[k] = la[k];
         // The smoothed iterate: row t - 4 PRE + 1 had its last update at step t - 1.
         const int rw = t - 4 * PRE + 1;
         if (cown && rw >= w.R0 && rw < w.R1) xout[rw * s + Jc] = ring[rw & (kRing - 1)][tid];
@@ -339,8 +362,8 @@ int mg_variant64() {
 }
 
 template <int PRE, int PD, int MINB, class T>
-void down_v(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, bool x_zero, int sms, int min_seg,
-            cudaStream_t st) {
+void down_v(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, bool x_zero, bool build, int sms,
+            int min_seg, cudaStream_t st) {
     const int HC = 2 * PRE + 2;
     constexpr int smem = kRing * kNT * static_cast<int>(sizeof(T));
     static PerDeviceOnce once;
@@ -348,7 +371,7 @@ void down_v(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, bool x_zero
     const int seg = seg_for(F.nx, F.ny, HC, sms, prepare_kernel(kernel, smem, once), min_seg);
     const int W = kNT - 2 * HC;
     const dim3 grid((F.ny + W - 1) / W, (F.nx + seg - 1) / seg);
-    kernel<<<grid, kNT, smem, st>>>(F, C, xout, x_zero ? 1 : 0, seg, HC);
+    kernel<<<grid, kNT, smem, st>>>(F, C, xout, x_zero ? 1 : 0, seg, HC, build ? 1 : 0);
     SGPU_LAUNCH();
 }
 
@@ -367,21 +390,21 @@ void up_v(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, T* xout,
 }
 
 template <int PRE, class T>
-void down_t(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, bool x_zero, int sms, int min_seg,
-            cudaStream_t st) {
+void down_t(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, bool x_zero, bool build, int sms,
+            int min_seg, cudaStream_t st) {
     if constexpr (sizeof(T) == 8) {
         switch (mg_variant64()) {
-        case 1: down_v<PRE, 1, 3>(F, C, xout, x_zero, sms, min_seg, st); break;
-        case 2: down_v<PRE, 1, 4>(F, C, xout, x_zero, sms, min_seg, st); break;
-        default: down_v<PRE, 2, 2>(F, C, xout, x_zero, sms, min_seg, st); break;
+        case 1: down_v<PRE, 1, 3>(F, C, xout, x_zero, build, sms, min_seg, st); break;
+        case 2: down_v<PRE, 1, 4>(F, C, xout, x_zero, build, sms, min_seg, st); break;
+        default: down_v<PRE, 2, 2>(F, C, xout, x_zero, build, sms, min_seg, st); break;
         }
     } else {
         switch (mg_variant()) {
-        case 0: down_v<PRE, 3, 2>(F, C, xout, x_zero, sms, min_seg, st); break;
-        case 1: down_v<PRE, 2, 3>(F, C, xout, x_zero, sms, min_seg, st); break;
-        case 3: down_v<PRE, 1, 5>(F, C, xout, x_zero, sms, min_seg, st); break;
-        case 4: down_v<PRE, 1, 6>(F, C, xout, x_zero, sms, min_seg, st); break;
-        default: down_v<PRE, 1, 4>(F, C, xout, x_zero, sms, min_seg, st); break;
+        case 0: down_v<PRE, 3, 2>(F, C, xout, x_zero, build, sms, min_seg, st); break;
+        case 1: down_v<PRE, 2, 3>(F, C, xout, x_zero, build, sms, min_seg, st); break;
+        case 3: down_v<PRE, 1, 5>(F, C, xout, x_zero, build, sms, min_seg, st); break;
+        case 4: down_v<PRE, 1, 6>(F, C, xout, x_zero, build, sms, min_seg, st); break;
+        default: down_v<PRE, 1, 4>(F, C, xout, x_zero, build, sms, min_seg, st); break;
         }
     }
 }
@@ -414,12 +437,12 @@ bool mg_fast_supported(int pre, int post) { return pre >= 1 && pre <= 4 && post 
 
 template <class T>
 void launch_mg_down(const LevelViewT<T>& F, const LevelViewT<T>& C, T* xout, int pre, bool x_zero,
-                    int sms, int min_seg, cudaStream_t st) {
+                    int sms, int min_seg, cudaStream_t st, bool build) {
     switch (pre) {
-    case 1: down_t<1>(F, C, xout, x_zero, sms, min_seg, st); break;
-    case 2: down_t<2>(F, C, xout, x_zero, sms, min_seg, st); break;
-    case 3: down_t<3>(F, C, xout, x_zero, sms, min_seg, st); break;
-    case 4: down_t<4>(F, C, xout, x_zero, sms, min_seg, st); break;
+    case 1: down_t<1>(F, C, xout, x_zero, build, sms, min_seg, st); break;
+    case 2: down_t<2>(F, C, xout, x_zero, build, sms, min_seg, st); break;
+    case 3: down_t<3>(F, C, xout, x_zero, build, sms, min_seg, st); break;
+    case 4: down_t<4>(F, C, xout, x_zero, build, sms, min_seg, st); break;
     default: throw Error(SGPU_E_INVALID, "streaming multigrid supports mg_pre 1..4");
     }
 }
@@ -441,12 +464,12 @@ void launch_mg_up(const LevelViewT<T>& C, const LevelViewT<T>& F, const T* xin, 
 // bits); mg_fast32.cu includes it with SGPU_FLOAT_UNIT for the float ones (contraction allowed).
 #ifndef SGPU_FLOAT_UNIT
 template void launch_mg_down<double>(const LevelViewT<double>&, const LevelViewT<double>&, double*,
-                                     int, bool, int, int, cudaStream_t);
+                                     int, bool, int, int, cudaStream_t, bool);
 template void launch_mg_up<double>(const LevelViewT<double>&, const LevelViewT<double>&,
                                    const double*, double*, double, int, int, int, cudaStream_t);
 #else
 template void launch_mg_down<float>(const LevelViewT<float>&, const LevelViewT<float>&, float*, int,
-                                    bool, int, int, cudaStream_t);
+                                    bool, int, int, cudaStream_t, bool);
 template void launch_mg_up<float>(const LevelViewT<float>&, const LevelViewT<float>&, const float*,
                                   float*, double, int, int, int, cudaStream_t);
 #endif

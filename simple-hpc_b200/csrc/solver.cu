@@ -103,7 +103,9 @@ struct Solver {
     int mg_tail = 0;                 // first level handled by the tail kernel
     std::vector<double*> mg_x2;      // second iterate buffer per streamed level (interior (0,0))
     MgLevels mgl{};
-    void mg_vcycle_fast(bool x_is_zero);
+    // build: form the coarse operators inside the cycle (the streamed levels' down kernels, then the
+    // tail's levels) instead of before it.
+    void mg_vcycle_fast(bool x_is_zero, bool build = false);
 
     // fused fast path (multicolour momentum): frozen velocity copy and the sweep ping-pong buffer
     bool fast = false;
@@ -440,7 +442,12 @@ struct Solver {
         // res_p = the sum of |b|, and the sum of b (its mean), from the blocks' partial sums
         launch_sum_partials(part, nparts, 2, nparts, res3 + 2, sums + 25, st);
         mark(SGPU_PH_SOLVE_P);
-        for (std::size_t l = 1; l < lv32.size(); ++l) launch_mg_build<float>(lv32[l - 1], lv32[l], st);
+        // The coarse operators are built inside the V-cycle (fused_build: by the down kernel of the
+        // level above for the streamed levels, then the tail's levels), unless a warm start reads
+        // them before the first cycle.
+        const bool fused_build = !net;
+        if (!fused_build)
+            for (std::size_t l = 1; l < lv32.size(); ++l) launch_mg_build<float>(lv32[l - 1], lv32[l], st);
         const bool dc_mode = prm.mg_mode == SGPU_MG_TOLERANCE;
         pc_dc_src = nullptr;
         int nbb = 0;
@@ -465,7 +472,10 @@ struct Solver {
         auto vcycle32 = [&](bool x_zero) {
             for (int l = 0; l < mg_tail; ++l)
                 launch_mg_down<float>(lv32[l], lv32[l + 1], mg32_x2[l], prm.mg_pre, x_zero || l > 0, sms,
-                                      min_seg, st);
+                                      min_seg, st, fused_build);
+            if (fused_build)
+                for (std::size_t l = static_cast<std::size_t>(mg_tail) + 1; l < lv32.size(); ++l)
+                    launch_mg_build<float>(lv32[l - 1], lv32[l], st);
             launch_mg_tail<float>(mgl32, mg_tail, prm.mg_pre, prm.mg_post, prm.mg_omega, kCoarseTol32,
                                   coarse_rowbuf, stats, st);
             for (int l = mg_tail - 1; l >= 0; --l)
@@ -998,12 +1008,15 @@ void Solver::mg_vcycle() {
 
 // solve_pc_mg (multigrid.cpp:347-357).
 void Solver::solve_mg() {
-    for (std::size_t l = 1; l < lv.size(); ++l) launch_mg_build(lv[l - 1], lv[l], st);
+    // The streaming V-cycle builds the coarse operators itself unless a warm start reads them first.
+    const bool fused_build = mg_fast && !net;
+    if (!fused_build)
+        for (std::size_t l = 1; l < lv.size(); ++l) launch_mg_build(lv[l - 1], lv[l], st);
     SGPU_CUDA(cudaMemsetAsync(w.pc, 0, g.bytes(), st));
     remove_mean0(w.b, b_sum);
     const bool guess = apply_warm_start(lv[0]);
     last_vcycles = run_cycles(lv[0], !guess, [&](bool x_zero) {
-        if (mg_fast) mg_vcycle_fast(x_zero);
+        if (mg_fast) mg_vcycle_fast(x_zero, fused_build);
         else mg_vcycle();
     });
     remove_mean0(w.pc);
@@ -1040,10 +1053,12 @@ template <class T> void Solver::sample_pair(std::vector<LevelViewT<T>>& L, float
 
 // mg_vcycle with the streaming level kernels: levels [0, mg_tail) go down and up in one pass
 // each, the rest (and the coarse solve) in the single-CTA tail kernel.
-void Solver::mg_vcycle_fast(bool x_is_zero) {
+void Solver::mg_vcycle_fast(bool x_is_zero, bool build) {
     const int nl = static_cast<int>(lv.size());
     for (int l = 0; l < mg_tail; ++l)
-        launch_mg_down(lv[l], lv[l + 1], mg_x2[l], prm.mg_pre, x_is_zero || l > 0, sms, min_seg, st);
+        launch_mg_down(lv[l], lv[l + 1], mg_x2[l], prm.mg_pre, x_is_zero || l > 0, sms, min_seg, st, build);
+    if (build)
+        for (int l = mg_tail + 1; l < nl; ++l) launch_mg_build(lv[l - 1], lv[l], st);
     launch_mg_tail(mgl, mg_tail, prm.mg_pre, prm.mg_post, prm.mg_omega, kCoarseTol64, coarse_rowbuf,
                    stats, st);
     for (int l = mg_tail - 1; l >= 0; --l)

@@ -5,13 +5,15 @@
 // concatenates the encoder output of its level and applies two 3x3 convolutions with ReLU; a 1x1
 // convolution gives the one output channel. Activations are NHWC BF16 with channel counts that are
 // multiples of 16; the convolutions use BF16 copies of FP32 master weights and accumulate in FP32 on
-// the tensor cores (mma.sync m16n8k16). Training: mean-squared error, Adam.
+// the 5th-generation tensor cores (tcgen05, TMEM accumulators: conv_tc.cu). Training: mean-squared
+// error, Adam.
 //
 // The convolutions are implicit GEMMs. Forward: Y[p, co] = sum over taps t and input channels ci of
-// X[p + t, ci] W[co, t, ci]; a warp owns 16 pixels x 64 output channels. The input gradient is the
-// same kernel on the output gradient with the flipped weights W'[ci, 8 - t, co]. The weight gradient
-// is a GEMM over pixels: dW[co, t, ci] = sum over p of dZ[p, co] X[p + t, ci], one 16 x 8 tile of
-// one tap per warp over a chunk of pixels, added into FP32 with atomics.
+// X[p + t, ci] W[co, t, ci]. The input gradient is the same kernel on the output gradient with the
+// flipped weights W'[ci, 8 - t, co]. The weight gradient is a GEMM over pixels: dW[co, t, ci] = sum
+// over p of dZ[p, co] X[p + t, ci], over chunks of pixels added into FP32 with atomics. This file
+// holds the rest of the network: pooling, upsampling and concatenation, the head, the loss, Adam and
+// the solver-level plumbing.
 //
 // Inputs (2 channels, zero-padded to 16): b / s_b and AP / m_a - 1 of the p' system of one multigrid
 // level (b and AP as pressure.cpp:39-47 forms them, restricted like multigrid.cpp:232-261), with s_b
@@ -32,142 +34,6 @@ namespace sgpu {
 namespace {
 
 using bf16 = __nv_bfloat16;
-
-__device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], const uint32_t b[2]) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-        "{%8,%9}, {%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-__device__ __forceinline__ uint32_t ld32(const bf16* p) { return *reinterpret_cast<const uint32_t*>(p); }
-__device__ __forceinline__ uint32_t pack(bf16 lo, bf16 hi) {
-    return static_cast<uint32_t>(__bfloat16_as_ushort(lo)) |
-           (static_cast<uint32_t>(__bfloat16_as_ushort(hi)) << 16);
-}
-
-constexpr int kWarps = 4;
-constexpr int kThreads = 32 * kWarps;
-
-// 3x3 convolution with zero padding 1 (+ bias, ReLU when relu != 0). X: [N*H*W][Cin], W: [Cout][9]
-// [Cin], Y: [N*H*W][Cout]; Cin and Cout multiples of 16. Fragment layouts of m16n8k16 (row.col): A
-// rows = pixels gid and gid + 8, k = input channels 2 tig (+1) and 2 tig + 8 (+9); B column = output
-// channel gid, k likewise; C rows gid / gid + 8, columns 2 tig (+1).
-__global__ void __launch_bounds__(kThreads)
-    k_conv_fwd(const bf16* __restrict__ X, int N, int H, int W, int Cin, const bf16* __restrict__ Wt,
-               const float* __restrict__ bias, bf16* __restrict__ Y, int Cout, int relu) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int gid = lane >> 2, tig = lane & 3;
-    const long npix = static_cast<long>(N) * H * W;
-    const long p0 = (static_cast<long>(blockIdx.x) * kWarps + warp) * 16;
-    if (p0 >= npix) return;
-    const int co0 = blockIdx.y * 64;
-    const int nt = min(8, (Cout - co0) / 8);
-    long pr[2] = {p0 + gid, p0 + gid + 8};
-    int yy[2], xx[2];
-    long nn[2];
-    bool live[2];
-    for (int r = 0; r < 2; ++r) {
-        live[r] = pr[r] < npix;
-        const long q = live[r] ? pr[r] : 0;
-        xx[r] = static_cast<int>(q % W);
-        yy[r] = static_cast<int>((q / W) % H);
-        nn[r] = q / (static_cast<long>(W) * H);
-    }
-    float acc[8][4];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
-    for (int tap = 0; tap < 9; ++tap) {
-        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-        const bf16* src[2];
-        for (int r = 0; r < 2; ++r) {
-            const int y = yy[r] + dy, x = xx[r] + dx;
-            src[r] = (live[r] && y >= 0 && y < H && x >= 0 && x < W)
-                         ? X + ((nn[r] * H + y) * W + x) * Cin
-                         : nullptr;
-        }
-        for (int c0 = 0; c0 < Cin; c0 += 16) {
-            uint32_t a[4];
-            a[0] = src[0] ? ld32(src[0] + c0 + 2 * tig) : 0u;
-            a[1] = src[1] ? ld32(src[1] + c0 + 2 * tig) : 0u;
-            a[2] = src[0] ? ld32(src[0] + c0 + 8 + 2 * tig) : 0u;
-            a[3] = src[1] ? ld32(src[1] + c0 + 8 + 2 * tig) : 0u;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                if (j < nt) {
-                    const bf16* w = Wt + (static_cast<long>(co0 + j * 8 + gid) * 9 + tap) * Cin + c0;
-                    const uint32_t b[2] = {ld32(w + 2 * tig), ld32(w + 8 + 2 * tig)};
-                    mma_bf16(acc[j], a, b);
-                }
-            }
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        if (j >= nt) continue;
-        const int co = co0 + j * 8 + 2 * tig;
-        const float b0 = bias ? bias[co] : 0.0f, b1 = bias ? bias[co + 1] : 0.0f;
-        for (int r = 0; r < 2; ++r) {
-            if (!live[r]) continue;
-            float v0 = acc[j][2 * r] + b0, v1 = acc[j][2 * r + 1] + b1;
-            if (relu) {
-                v0 = fmaxf(v0, 0.0f);
-                v1 = fmaxf(v1, 0.0f);
-            }
-            *reinterpret_cast<__nv_bfloat162*>(Y + pr[r] * Cout + co) = __floats2bfloat162_rn(v0, v1);
-        }
-    }
-}
-
-// Weight gradient of a 3x3 convolution: dW[co, tap, ci] += sum over pixels of dZ[p, co] X[p + tap,
-// ci]. GEMM with M = Cout, N = Cin, K = pixels: a warp owns a 16 x 8 (co x ci) tile of one tap and
-// the pixels [blockIdx.y * chunk, + chunk).
-__global__ void __launch_bounds__(kThreads)
-    k_conv_wgrad(const bf16* __restrict__ X, const bf16* __restrict__ dZ, int N, int H, int W,
-                 int Cin, int Cout, float* __restrict__ dW, int chunk) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int gid = lane >> 2, tig = lane & 3;
-    const int ci_tiles = Cin / 8;
-    const long tile = static_cast<long>(blockIdx.x) * kWarps + warp;
-    const long ntile = static_cast<long>(Cout / 16) * ci_tiles * 9;
-    if (tile >= ntile) return;
-    const int tap = static_cast<int>(tile % 9);
-    const int ci0 = static_cast<int>((tile / 9) % ci_tiles) * 8;
-    const int co0 = static_cast<int>(tile / (9L * ci_tiles)) * 16;
-    const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-    const long npix = static_cast<long>(N) * H * W;
-    const long pbeg = static_cast<long>(blockIdx.y) * chunk;
-    const long pend = min(npix, pbeg + chunk);
-    const bf16 zero = __float2bfloat16(0.0f);
-    auto xval = [&](long p) -> bf16 {
-        if (p >= pend) return zero;
-        const int x = static_cast<int>(p % W), y = static_cast<int>((p / W) % H);
-        const long n = p / (static_cast<long>(W) * H);
-        const int ys = y + dy, xs = x + dx;
-        if (ys < 0 || ys >= H || xs < 0 || xs >= W) return zero;
-        return X[((n * H + ys) * W + xs) * Cin + ci0 + gid];
-    };
-    auto zval = [&](long p, int co) -> bf16 { return p < pend ? dZ[p * Cout + co] : zero; };
-    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-    for (long k0 = pbeg; k0 < pend; k0 += 16) {
-        const long ka = k0 + 2 * tig, kb = ka + 8;
-        uint32_t a[4], b[2];
-        a[0] = pack(zval(ka, co0 + gid), zval(ka + 1, co0 + gid));
-        a[1] = pack(zval(ka, co0 + gid + 8), zval(ka + 1, co0 + gid + 8));
-        a[2] = pack(zval(kb, co0 + gid), zval(kb + 1, co0 + gid));
-        a[3] = pack(zval(kb, co0 + gid + 8), zval(kb + 1, co0 + gid + 8));
-        b[0] = pack(xval(ka), xval(ka + 1));
-        b[1] = pack(xval(kb), xval(kb + 1));
-        mma_bf16(acc, a, b);
-    }
-    // acc[0..1]: row co0 + gid, columns ci0 + 2 tig (+1); acc[2..3]: row co0 + gid + 8.
-    for (int r = 0; r < 2; ++r)
-        for (int e = 0; e < 2; ++e) {
-            const int co = co0 + gid + 8 * r, ci = ci0 + 2 * tig + e;
-            atomicAdd(dW + (static_cast<long>(co) * 9 + tap) * Cin + ci, acc[2 * r + e]);
-        }
-}
 
 // W'[ci][tap'][co] = W[co][8 - tap'][ci]: the weights of the input-gradient convolution.
 __global__ void k_flip_weights(const bf16* __restrict__ W, bf16* __restrict__ Wf, int Cout, int Cin) {
@@ -516,8 +382,6 @@ UNet::UNet(int base, int levels, unsigned seed) : base_(base), levels_(levels) {
     SGPU_CUDA(cudaMalloc(&loss_, sizeof(float)));
     SGPU_CUDA(cudaMalloc(&err_, sizeof(unsigned)));
     SGPU_CUDA(cudaMemset(err_, 0, sizeof(unsigned)));
-    const char* impl = std::getenv("SGPU_CNN_CONV");
-    legacy_conv_ = impl && std::string(impl) == "mma";
     SGPU_CUDA(cudaMemcpy(w_, h.data(), sizeof(float) * nparam_, cudaMemcpyHostToDevice));
     SGPU_CUDA(cudaMemset(g_, 0, sizeof(float) * nparam_));
     SGPU_CUDA(cudaMemset(m_, 0, sizeof(float) * nparam_));
@@ -619,16 +483,7 @@ void UNet::shape(int n, int h, int w) {
 }
 
 void UNet::conv_fwd(const Conv& c, const bf16* x, bf16* y, cudaStream_t st) {
-    if (!legacy_conv_) {
-        launch_conv_tc(x, n_, h_ >> c.level, wd_ >> c.level, c.cin, wb_ + c.w_off, w_ + c.b_off, y, c.cout, 1,
-                       err_, st);
-        return;
-    }
-    const long np = px(c.level);
-    const dim3 grid(static_cast<unsigned>((np + 16 * kWarps - 1) / (16 * kWarps)), (c.cout + 63) / 64);
-    k_conv_fwd<<<grid, kThreads, 0, st>>>(x, n_, h_ >> c.level, wd_ >> c.level, c.cin, wb_ + c.w_off,
-                                          w_ + c.b_off, y, c.cout, 1);
-    SGPU_LAUNCH();
+    launch_conv_tc(x, n_, h_ >> c.level, wd_ >> c.level, c.cin, wb_ + c.w_off, w_ + c.b_off, y, c.cout, 1, err_, st);
 }
 
 void UNet::forward(cudaStream_t st) {
@@ -670,15 +525,7 @@ void UNet::conv_back(const Conv& c, const bf16* x_in, bf16* dx, cudaStream_t st)
     const long np = px(c.level);
     k_relu_back<<<blocks(np * c.cout), 256, 0, st>>>(c.y, c.dy, c.dy, np * c.cout);
     SGPU_LAUNCH();
-    if (!legacy_conv_) {
-        launch_conv_wgrad_tc(x_in, c.dy, n_, h, w, c.cin, c.cout, g_ + c.w_off, err_, st);
-    } else {
-    const int chunk = 4096;
-    const long tiles = static_cast<long>(c.cout / 16) * (c.cin / 8) * 9;
-    const dim3 gw(static_cast<unsigned>((tiles + kWarps - 1) / kWarps), static_cast<unsigned>((np + chunk - 1) / chunk));
-    k_conv_wgrad<<<gw, kThreads, 0, st>>>(x_in, c.dy, n_, h, w, c.cin, c.cout, g_ + c.w_off, chunk);
-    SGPU_LAUNCH();
-    }
+    launch_conv_wgrad_tc(x_in, c.dy, n_, h, w, c.cin, c.cout, g_ + c.w_off, err_, st);
     k_bias_grad<<<static_cast<unsigned>(std::min<long>(np, 1024)), std::max(32, c.cout), 0, st>>>(c.dy, np, c.cout,
                                                                                                g_ + c.b_off);
     SGPU_LAUNCH();
@@ -686,13 +533,7 @@ void UNet::conv_back(const Conv& c, const bf16* x_in, bf16* dx, cudaStream_t st)
     const long nw = static_cast<long>(c.cout) * 9 * c.cin;
     k_flip_weights<<<blocks(nw), 256, 0, st>>>(wb_ + c.w_off, wf_, c.cout, c.cin);
     SGPU_LAUNCH();
-    if (!legacy_conv_) {
-        launch_conv_tc(c.dy, n_, h, w, c.cout, wf_, nullptr, dx, c.cin, 0, err_, st);
-        return;
-    }
-    const dim3 gd(static_cast<unsigned>((np + 16 * kWarps - 1) / (16 * kWarps)), (c.cin + 63) / 64);
-    k_conv_fwd<<<gd, kThreads, 0, st>>>(c.dy, n_, h, w, c.cout, wf_, nullptr, dx, c.cin, 0);
-    SGPU_LAUNCH();
+    launch_conv_tc(c.dy, n_, h, w, c.cout, wf_, nullptr, dx, c.cin, 0, err_, st);
 }
 
 void UNet::backward(cudaStream_t st) {

@@ -1,4 +1,4 @@
-// cnn.hpp — the learned warm start for the p' solve: a U-Net with its own BF16 tensor-core kernels.
+// cnn.hpp — the learned warm start for the p' solve: a U-Net with its own BF16 tensor-core (tcgen05) kernels.
 //
 // The network maps the p' system of one multigrid level (right-hand side b and diagonal AP, both
 // normalised) to a p' guess on that level. The solver runs it on the finest level of at most
@@ -81,7 +81,6 @@ class UNet {
     __nv_bfloat16* wb_ = nullptr; // BF16 copy of every parameter
     __nv_bfloat16* wf_ = nullptr; // flipped weights of one conv (input-gradient pass)
     unsigned* err_ = nullptr;      // device word: a tensor-core convolution's bounded wait gave up
-    bool legacy_conv_ = false;     // SGPU_CNN_CONV=mma: the warp-level mma.sync kernels (comparison)
     int step_ = 0;
     // activations for the current shape
     int n_ = 0, h_ = 0, wd_ = 0;

@@ -21,6 +21,7 @@
 #include "blocksum.cuh"
 #include "stencil.cuh"
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdlib>
 
@@ -136,7 +137,11 @@ __global__ void __launch_bounds__(256, 4)
 }
 
 #ifdef SGPU_FLOAT_UNIT
-constexpr int kRing = 32;    // rows of the e ring (a power of two)
+// Rows of the e ring (a power of two). A super-step reads rows down to 2 x the colour count behind
+// its step and issues rows up to kRecAhead super-steps ahead: 16 rows live at once for five colours.
+// Each thread's row copies land in its own column only, and the threads' vertical reads are in their
+// own columns, so a slot is refilled as soon as its owner has written the row out.
+constexpr int kRing = 16;
 constexpr int kRecAhead = 2; // record slots: super-steps whose records are in flight
 constexpr int kSpinLimit = 1 << 20; // bounded mbarrier waits (a give-up is reported, never a hang)
 
@@ -433,37 +438,82 @@ __global__ void __launch_bounds__(NT, MINB)
 
 #endif // SGPU_FLOAT_UNIT
 
+// Rows per thread of k_assemble_p_mixed, and the first (even) column of the column pairs that the
+// pair kernels (k_assemble_p_mixed, k_correct_mixed) give each thread.
+constexpr int kAsmRows = 1;
+__host__ __device__ __forceinline__ int pair_col0(const DevParams& p) { return (p.H + 1) & ~1; }
+__host__ __device__ __forceinline__ int pair_count(const DevParams& p) { return (p.NY + p.H - pair_col0(p)) / 2 + 1; }
+__device__ __forceinline__ double2 ld2(const double* q) { return *reinterpret_cast<const double2*>(q); }
+
 // assemble_p (pressure.cpp:14-54) in FP64 with the p' operator stored in FP32 (level 0 of the FP32
 // hierarchy), and the block's FP64 sums of |b| (res_p) and of b (its mean) into part[block] and
-// part[nblocks + block] (deterministic trees, blocksum.cuh).
+// part[nblocks + block] (each thread's cells in a fixed order, then the deterministic trees of
+// blocksum.cuh). Each thread takes two adjacent columns (j even: 16-byte pairs of the FP64 arrays)
+// in kAsmRows rows, and issues all its loads before the first cell's arithmetic. At 4096^2: 0.20 ms,
+// against 0.25 ms for one cell per thread in four rows (and 0.22 ms for pairs in two rows, whose 90
+// registers leave two CTAs per SM).
 __global__ void __launch_bounds__(256)
     k_assemble_p_mixed(DevParams p, const double* __restrict__ APU, const double* __restrict__ APV,
                        const double* __restrict__ u, const double* __restrict__ v,
                        double* __restrict__ bfield, LevelView32 L0, double* __restrict__ part) {
+    constexpr int R = kAsmRows;
     __shared__ double s_abs[8], s_b[8];
     const int H = p.H;
-    const int J = static_cast<int>(blockIdx.x * 32 + threadIdx.x);
-    const int I0 = static_cast<int>(blockIdx.y * 8 * kRowsPerThread + threadIdx.y);
-    double sa = 0.0, sb = 0.0;
-#pragma unroll 1
-    for (int k = 0; k < kRowsPerThread; ++k) {
+    const int j = pair_col0(p) + 2 * static_cast<int>(blockIdx.x * 32 + threadIdx.x);
+    const int I0 = static_cast<int>(blockIdx.y * 8 * R + threadIdx.y);
+    const bool jin = j <= p.NY + H; // the pair holds at least one cell
+    const std::size_t ld = p.pitch;
+    double2 apu[R], apv[R], apvs[R], uu[R], vv[R], vs[R];
+    double apuw[R], uw[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
         const int I = I0 + 8 * k;
-        if (I >= p.NX || J >= p.NY) break;
-        const int i = H + I, j = H + 1 + J;
-        const std::size_t q = ix(p, i, j), ld = p.pitch;
-        const double dx = p.dx, dy = p.dy;
-        const double aep = (j == p.NY + H) ? 0.0 : dy * dy / APU[q];
-        const double awp = (j == H + 1) ? 0.0 : dy * dy / APU[q - 1];
-        const double anp = (i == H) ? 0.0 : dx * dx / APV[q];
-        const double asp = (i == p.NX + H - 1) ? 0.0 : dx * dx / APV[q + ld];
-        const int lq = I * L0.stride + J;
-        set_links(L0, lq, static_cast<float>(aep), static_cast<float>(awp), static_cast<float>(anp),
-                  static_cast<float>(asp));
-        L0.AP[lq] = static_cast<float>(aep + awp + anp + asp);
-        const double b = -dx * (-v[q + ld] + v[q]) - dy * (-u[q - 1] + u[q]);
-        bfield[q] = b;
-        sa += fabs(b);
-        sb += b;
+        if (!jin || I >= p.NX) continue;
+        const std::size_t q = ix(p, H + I, j);
+        apu[k] = ld2(APU + q);
+        apuw[k] = APU[q - 1];
+        apv[k] = ld2(APV + q);
+        apvs[k] = ld2(APV + q + ld);
+        uu[k] = ld2(u + q);
+        uw[k] = u[q - 1];
+        vv[k] = ld2(v + q);
+        vs[k] = ld2(v + q + ld);
+    }
+    const double dx = p.dx, dy = p.dy;
+    double sa = 0.0, sb = 0.0;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int I = I0 + 8 * k;
+        if (!jin || I >= p.NX) continue;
+        const int i = H + I;
+        const std::size_t q = ix(p, i, j);
+        // the pair's two cells: e = 0 at column j, e = 1 at j + 1 (pressure.cpp:22-44)
+        const double apu_e[2] = {apu[k].x, apu[k].y}, apu_w[2] = {apuw[k], apu[k].x};
+        const double apv_n[2] = {apv[k].x, apv[k].y}, apv_s[2] = {apvs[k].x, apvs[k].y};
+        const double u_e[2] = {uu[k].x, uu[k].y}, u_w[2] = {uw[k], uu[k].x};
+        const double v_n[2] = {vv[k].x, vv[k].y}, v_s[2] = {vs[k].x, vs[k].y};
+        double bq[2];
+        bool cell[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int jj = j + e;
+            cell[e] = jj >= H + 1 && jj <= p.NY + H;
+            if (!cell[e]) continue;
+            const double aep = (jj == p.NY + H) ? 0.0 : dy * dy / apu_e[e];
+            const double awp = (jj == H + 1) ? 0.0 : dy * dy / apu_w[e];
+            const double anp = (i == H) ? 0.0 : dx * dx / apv_n[e];
+            const double asp = (i == p.NX + H - 1) ? 0.0 : dx * dx / apv_s[e];
+            const int lq = I * L0.stride + (jj - H - 1);
+            set_links(L0, lq, static_cast<float>(aep), static_cast<float>(awp), static_cast<float>(anp),
+                      static_cast<float>(asp));
+            L0.AP[lq] = static_cast<float>(aep + awp + anp + asp);
+            bq[e] = -dx * (-v_s[e] + v_n[e]) - dy * (-u_w[e] + u_e[e]);
+            sa += fabs(bq[e]);
+            sb += bq[e];
+        }
+        if (cell[0] && cell[1]) *reinterpret_cast<double2*>(bfield + q) = make_double2(bq[0], bq[1]);
+        else if (cell[0]) bfield[q] = bq[0];
+        else if (cell[1]) bfield[q + 1] = bq[1];
     }
     const int tid = static_cast<int>(threadIdx.y * 32 + threadIdx.x);
     const double ta = block_sum<8>(sa, s_abs, tid);
@@ -490,29 +540,53 @@ __global__ void k_b_to_f32(DevParams p, const double* __restrict__ bfield, const
 }
 
 // correct (pressure.cpp:136-157) in FP64 from the FP32 p' minus its FP64 mean; also stores that
-// p' in the FP64 pc field.
-__global__ void k_correct_mixed(DevParams p, const float* __restrict__ pc32, int ld32,
-                                const double* __restrict__ sum_pc, const double* __restrict__ APU,
-                                const double* __restrict__ APV, double* u, double* v, double* pf,
-                                double* pc64) {
-    const int J = static_cast<int>(blockIdx.x * 32 + threadIdx.x);
+// p' in the FP64 pc field. Two adjacent columns per thread: the FP64 arrays are read and written as
+// 16-byte pairs (j even; the pitch is even), the FP32 p' as scalars. Elements of a pair that are not
+// cells of the correction keep their values (the thread writes back what it read). Against one cell
+// per thread with 8-byte accesses (4096^2: 0.26 ms, long-scoreboard bound), the pairs halve the
+// load instructions and double the bytes each one has in flight: 0.17 ms.
+__global__ void __launch_bounds__(256)
+    k_correct_mixed(DevParams p, const float* __restrict__ pc32, int ld32,
+                          const double* __restrict__ sum_pc, const double* __restrict__ APU,
+                          const double* __restrict__ APV, double* __restrict__ u, double* __restrict__ v,
+                          double* __restrict__ pf, double* __restrict__ pc64) {
+    const int H = p.H;
+    const int j = pair_col0(p) + 2 * static_cast<int>(blockIdx.x * 32 + threadIdx.x);
     const int I = static_cast<int>(blockIdx.y * 8 + threadIdx.y);
-    if (I >= p.NX || J >= p.NY) return;
-    const int H = p.H, i = H + I, j = H + 1 + J;
+    if (I >= p.NX || j > p.NY + H) return;
+    const int i = H + I;
     const std::size_t q = ix(p, i, j);
     const double m = *sum_pc / (static_cast<double>(p.NX) * p.NY);
-    const float* pcr = pc32 + I * ld32 + J; // level-0 p' at (I, J); neighbours inside its zero ring
-    const double pc = static_cast<double>(pcr[0]) - m;
-    if (j <= p.NY + H - 1) {
-        const double pce = static_cast<double>(pcr[1]) - m;
-        u[q] += p.dy * (pc - pce) / APU[q];
+    const double2 pp = *reinterpret_cast<const double2*>(pf + q);
+    const double2 uu = *reinterpret_cast<const double2*>(u + q);
+    const double2 au = *reinterpret_cast<const double2*>(APU + q);
+    double2 vv = make_double2(0.0, 0.0), av = make_double2(1.0, 1.0);
+    if (I >= 1) {
+        vv = *reinterpret_cast<const double2*>(v + q);
+        av = *reinterpret_cast<const double2*>(APV + q);
     }
-    if (i >= H + 1) {
-        const double pcn = static_cast<double>(pcr[-ld32]) - m;
-        v[q] += p.dx * (pc - pcn) / APV[q];
+    const float* pcr = pc32 + I * ld32 + (j - H - 1); // p' of column j; j - H - 1 >= -1 (zero ring)
+    const float c0 = pcr[0], c1 = pcr[1], c2 = pcr[2];
+    const float n0 = I >= 1 ? pcr[-ld32] : 0.0f, n1 = I >= 1 ? pcr[1 - ld32] : 0.0f;
+    double2 pn = pp, un = uu, vn = vv;
+    const bool cell0 = j >= H + 1, cell1 = j + 1 <= p.NY + H;
+    if (cell0) {
+        const double pc = static_cast<double>(c0) - m;
+        if (j <= p.NY + H - 1) un.x = uu.x + p.dy * (pc - (static_cast<double>(c1) - m)) / au.x;
+        if (I >= 1) vn.x = vv.x + p.dx * (pc - (static_cast<double>(n0) - m)) / av.x;
+        pn.x = pp.x + p.ap * pc;
+        if (pc64) pc64[q] = pc;
     }
-    pf[q] += p.ap * pc;
-    if (pc64) pc64[q] = pc;
+    if (cell1) {
+        const double pc = static_cast<double>(c1) - m;
+        if (j + 1 <= p.NY + H - 1) un.y = uu.y + p.dy * (pc - (static_cast<double>(c2) - m)) / au.y;
+        if (I >= 1) vn.y = vv.y + p.dx * (pc - (static_cast<double>(n1) - m)) / av.y;
+        pn.y = pp.y + p.ap * pc;
+        if (pc64) pc64[q + 1] = pc;
+    }
+    *reinterpret_cast<double2*>(pf + q) = pn;
+    *reinterpret_cast<double2*>(u + q) = un;
+    if (I >= 1) *reinterpret_cast<double2*>(v + q) = vn;
 }
 
 // The FP64 p' field as k_correct_mixed uses it (FP32 p' minus its FP64 mean), for a download.
@@ -648,9 +722,10 @@ Range update_range(const DevParams& p, bool v) {
 
 #ifdef SGPU_FLOAT_UNIT
 // Threads per CTA of the correction sweep and the resident CTAs per SM its registers are bounded
-// for (shared memory allows that many: the e ring and two record slot sets per CTA).
-constexpr int kCorrNT = 256;
-constexpr int kCorrMinb = kCorrNT <= 256 ? 3 : 2;
+// for: 224 threads (7 warps) keep the e ring and the two record slot sets at 50 KB, so four CTAs
+// (28 warps) fit an SM, where 256 threads fit three (24 warps, 3% slower at 4096^2).
+constexpr int kCorrNT = 224;
+constexpr int kCorrMinb = 4;
 
 template <int NCOL, bool V, int NT, int MINB>
 void launch_corr(const DevParams& p, const float* ein, float* eout, MomRec32 rec, bool e_zero,
@@ -695,17 +770,27 @@ int launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x,
     return static_cast<int>(grid.x * grid.y);
 }
 
+dim3 assemble_grid(const DevParams& p) {
+    return dim3((pair_count(p) + 31) / 32, (p.NX + 8 * kAsmRows - 1) / (8 * kAsmRows));
+}
+
 int launch_assemble_p_mixed(const DevParams& p, const double* APU, const double* APV, const double* u,
                             const double* v, double* bfield, const LevelView32& L0, double* part,
                             cudaStream_t st) {
-    const dim3 grid((p.NY + 31) / 32, (p.NX + 8 * kRowsPerThread - 1) / (8 * kRowsPerThread));
+    const dim3 grid = assemble_grid(p);
     k_assemble_p_mixed<<<grid, dim3(32, 8), 0, st>>>(p, APU, APV, u, v, bfield, L0, part);
     SGPU_LAUNCH();
     return static_cast<int>(grid.x * grid.y);
 }
 
 int mixed_partials(const DevParams& p) {
-    return 2 * ((p.NY + 32) / 32) * ((p.NX + 8 * kRowsPerThread) / (8 * kRowsPerThread));
+    // the prep's blocks (one partial each: 32 columns x kTileRows rows over the update range, at most
+    // NY + 1 columns and NX rows), the defect-correction update's (two each: 32 x kTileRows cells)
+    // and assemble_p's (two each)
+    const int prep = ((p.NY + 1 + 31) / 32) * ((p.NX + kTileRows - 1) / kTileRows);
+    const int dc = 2 * ((p.NY + 31) / 32) * ((p.NX + kTileRows - 1) / kTileRows);
+    const dim3 g = assemble_grid(p);
+    return std::max({prep, dc, static_cast<int>(2 * g.x * g.y)});
 }
 
 void launch_b_to_f32(const DevParams& p, const double* bfield, const double* sum_b,
@@ -756,7 +841,7 @@ void launch_pc_from64(const DevParams& p, const double* src, const double* sum_p
 void launch_correct_mixed(const DevParams& p, const LevelView32& L0, const double* sum_pc,
                           const double* APU, const double* APV, double* u, double* v, double* pf,
                           double* pc64, cudaStream_t st) {
-    const dim3 grid((p.NY + 31) / 32, (p.NX + 7) / 8);
+    const dim3 grid((pair_count(p) + 31) / 32, (p.NX + 7) / 8);
     k_correct_mixed<<<grid, dim3(32, 8), 0, st>>>(p, L0.x, L0.stride, sum_pc, APU, APV, u, v, pf, pc64);
     SGPU_LAUNCH();
 }

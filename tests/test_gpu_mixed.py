@@ -121,3 +121,26 @@ def test_mixed_runs_repeat_bit_for_bit(sgpu_mod, scheme, order):
     assert bit_equal(l0, l1)
     for a, b in zip(f0, f1):
         assert bit_equal(a, b)
+
+
+@pytest.mark.parametrize("nx,ny,scheme,order", [(77, 131, "QUICK", 4), (64, 95, "UDS", 2), (33, 2, "QUICK", 2)])
+def test_mixed_odd_grids_close_to_fp64(sgpu_mod, nx, ny, scheme, order):
+    """Grids whose column counts give the column-pair kernels (assemble_p, correct: two adjacent
+    cells per thread, 16-byte FP64 accesses) a last pair with one cell as well as two, and a grid two
+    cells wide: 10 iterations of the transient against the FP64 run."""
+    base = snapshot_config("short_16")
+    base.update(N_cells_x=str(nx), N_cells_y=str(ny), Re="400", convection_scheme=scheme,
+                diffusion_order=str(order), momentum_solver="gs_multicolour", pressure_solver="mg",
+                maxit="10", error_tolerance="0")
+    p64 = sgpu_mod.params_from_config(config_text(base))
+    with sgpu_mod.Solver(p64) as s:
+        s.run(10)
+        ref = {f: s.download(f) for f in (0, 1, 2)}
+    base["precision"] = "mixed"
+    p = sgpu_mod.params_from_config(config_text(base))
+    with sgpu_mod.Solver(p) as s:
+        s.run(10)
+        for f in (0, 1, 2):
+            mx, l2 = rel_errors(s.download(f), ref[f])
+            print(f"field {f}: max rel {mx:.3e}, L2 rel {l2:.3e}")
+            assert mx < 2e-6 and l2 < 2e-6

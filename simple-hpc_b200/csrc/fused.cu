@@ -411,31 +411,56 @@ __global__ void __launch_bounds__(NT, PF == 0 ? 2 : 3)
     cp_async_wait<0>();
 }
 
-// assemble_p (pressure.cpp:14-54) in one pass: links with the wall zeros, APP, b, |b| and b.
+// assemble_p (pressure.cpp:14-54) in one pass: links with the wall zeros, APP, b, |b| and b. Each
+// thread assembles the two cells (j, j + 1) of a column pair (j even; the pitch is even): the FP64
+// inputs and outputs move as 16-byte pairs (a single store where only one of the two is a cell).
+// The per-cell expressions are the reference's.
+__device__ __forceinline__ double2 ld2(const double* q) { return *reinterpret_cast<const double2*>(q); }
 __global__ void k_assemble_p(DevParams p, const double* __restrict__ APU,
                              const double* __restrict__ APV, const double* __restrict__ u,
                              const double* __restrict__ v, PressurePtr w, double* __restrict__ cabs,
                              double* __restrict__ cb) {
     const int H = p.H;
-    const int j = H + 1 + static_cast<int>(blockIdx.x * 32 + threadIdx.x);
+    const int j = ((H + 1) & ~1) + 2 * static_cast<int>(blockIdx.x * 32 + threadIdx.x);
     const int i = H + static_cast<int>(blockIdx.y * 8 + threadIdx.y);
     if (i > p.NX + H - 1 || j > p.NY + H) return;
     const std::size_t q = ix(p, i, j), ld = p.pitch;
     const double dx = p.dx, dy = p.dy;
-    const double aep = (j == p.NY + H) ? 0.0 : dy * dy / APU[q];
-    const double awp = (j == H + 1) ? 0.0 : dy * dy / APU[q - 1];
-    const double anp = (i == H) ? 0.0 : dx * dx / APV[q];
-    const double asp = (i == p.NX + H - 1) ? 0.0 : dx * dx / APV[q + ld];
-    w.AEP[q] = aep;
-    w.AWP[q] = awp;
-    w.ANP[q] = anp;
-    w.ASP[q] = asp;
-    w.APP[q] = aep + awp + anp + asp;
-    const double b = -dx * (-v[q + ld] + v[q]) - dy * (-u[q - 1] + u[q]);
-    w.b[q] = b;
-    const std::size_t c = static_cast<std::size_t>(i - H) * p.NY + (j - H - 1);
-    if (cabs) cabs[c] = fabs(b);
-    if (cb) cb[c] = b;
+    const double2 apu = ld2(APU + q), apv = ld2(APV + q), apvs = ld2(APV + q + ld);
+    const double2 uu = ld2(u + q), vv = ld2(v + q), vs = ld2(v + q + ld);
+    const double apuw = APU[q - 1], uw = u[q - 1];
+    const double apu_e[2] = {apu.x, apu.y}, apu_w[2] = {apuw, apu.x};
+    const double apv_n[2] = {apv.x, apv.y}, apv_s[2] = {apvs.x, apvs.y};
+    const double u_e[2] = {uu.x, uu.y}, u_w[2] = {uw, uu.x};
+    const double v_n[2] = {vv.x, vv.y}, v_s[2] = {vs.x, vs.y};
+    double ae[2], aw[2], an[2], as[2], ap[2], bb[2];
+    bool cell[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const int jj = j + e;
+        cell[e] = jj >= H + 1 && jj <= p.NY + H;
+        if (!cell[e]) continue;
+        ae[e] = (jj == p.NY + H) ? 0.0 : dy * dy / apu_e[e];
+        aw[e] = (jj == H + 1) ? 0.0 : dy * dy / apu_w[e];
+        an[e] = (i == H) ? 0.0 : dx * dx / apv_n[e];
+        as[e] = (i == p.NX + H - 1) ? 0.0 : dx * dx / apv_s[e];
+        ap[e] = ae[e] + aw[e] + an[e] + as[e];
+        bb[e] = -dx * (-v_s[e] + v_n[e]) - dy * (-u_w[e] + u_e[e]);
+        const std::size_t c = static_cast<std::size_t>(i - H) * p.NY + (jj - H - 1);
+        if (cabs) cabs[c] = fabs(bb[e]);
+        if (cb) cb[c] = bb[e];
+    }
+    auto put = [&](double* dst, const double* val) {
+        if (cell[0] && cell[1]) *reinterpret_cast<double2*>(dst + q) = make_double2(val[0], val[1]);
+        else if (cell[0]) dst[q] = val[0];
+        else if (cell[1]) dst[q + 1] = val[1];
+    };
+    put(w.AEP, ae);
+    put(w.AWP, aw);
+    put(w.ANP, an);
+    put(w.ASP, as);
+    put(w.APP, ap);
+    put(w.b, bb);
 }
 
 template <bool V>
@@ -511,7 +536,8 @@ void launch_mom_sweep(const DevParams& p, bool v_component, const double* xin, d
 void launch_assemble_p_fused(const DevParams& p, const double* APU, const double* APV,
                              const double* u, const double* v, PressurePtr w, double* cabs,
                              double* cb, cudaStream_t st) {
-    const dim3 grid((p.NY + 31) / 32, (p.NX + 7) / 8);
+    const int pairs = (p.NY + p.H - ((p.H + 1) & ~1)) / 2 + 1; // column pairs over j = H + 1 .. NY + H
+    const dim3 grid((pairs + 31) / 32, (p.NX + 7) / 8);
     k_assemble_p<<<grid, dim3(32, 8), 0, st>>>(p, APU, APV, u, v, w, cabs, cb);
     SGPU_LAUNCH();
 }

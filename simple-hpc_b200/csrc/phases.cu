@@ -227,16 +227,43 @@ __global__ void k_pc_jacobi(DevParams p, PressurePtr w, const double* __restrict
     dst[q] = wgt * t + (1 - wgt) * src[q];
 }
 
-// correct (pressure.cpp:136-157): the three loops write different arrays and read only pc.
+// correct (pressure.cpp:136-157): the three loops write different arrays and read only pc. Each
+// thread corrects the two cells (j, j + 1) of a column pair (j even; the pitch is even), reading and
+// writing every array as 16-byte pairs; an element of a pair outside the range keeps its value (the
+// thread writes back what it read). The per-cell expressions are the reference's.
+__device__ __forceinline__ double2 ld2(const double* q) { return *reinterpret_cast<const double2*>(q); }
+__device__ __forceinline__ void st2(double* q, double2 v) { *reinterpret_cast<double2*>(q) = v; }
 __global__ void k_correct(DevParams p, PressurePtr w, const double* __restrict__ APU,
-                          const double* __restrict__ APV, double* u, double* v, double* pf, Range r) {
-    int i, j;
-    if (!cell_of(r, i, j)) return;
+                          const double* __restrict__ APV, double* __restrict__ u, double* __restrict__ v,
+                          double* __restrict__ pf, Range r) {
+    const int j = (r.j0 & ~1) + 2 * static_cast<int>(blockIdx.x * BX + threadIdx.x);
+    const int i = r.i0 + static_cast<int>(blockIdx.y * BY + threadIdx.y);
+    if (i > r.i1 || j > r.j1) return;
     const int H = p.H;
     const std::size_t q = ix(p, i, j), ld = p.pitch;
-    if (j <= p.NY + H - 1) u[q] += p.dy * (w.pc[q] - w.pc[q + 1]) / APU[q];
-    if (i >= H + 1) v[q] += p.dx * (w.pc[q] - w.pc[q - ld]) / APV[q];
-    pf[q] += p.ap * w.pc[q];
+    const bool vrow = i >= H + 1;
+    const double2 pc = ld2(w.pc + q), apu = ld2(APU + q), pp = ld2(pf + q);
+    const double pce = w.pc[q + 2];
+    double2 uu = ld2(u + q), vv = make_double2(0.0, 0.0), pcn = vv, apv = make_double2(1.0, 1.0);
+    if (vrow) {
+        vv = ld2(v + q);
+        pcn = ld2(w.pc + q - ld);
+        apv = ld2(APV + q);
+    }
+    const double pcq[2] = {pc.x, pc.y}, pceq[2] = {pc.y, pce}, pcnq[2] = {pcn.x, pcn.y};
+    const double apuq[2] = {apu.x, apu.y}, apvq[2] = {apv.x, apv.y};
+    double uq[2] = {uu.x, uu.y}, vq[2] = {vv.x, vv.y}, pq[2] = {pp.x, pp.y};
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const int jj = j + e;
+        if (jj < r.j0 || jj > r.j1) continue;
+        if (jj <= p.NY + H - 1) uq[e] += p.dy * (pcq[e] - pceq[e]) / apuq[e];
+        if (vrow) vq[e] += p.dx * (pcq[e] - pcnq[e]) / apvq[e];
+        pq[e] += p.ap * pcq[e];
+    }
+    st2(u + q, make_double2(uq[0], uq[1]));
+    if (vrow) st2(v + q, make_double2(vq[0], vq[1]));
+    st2(pf + q, make_double2(pq[0], pq[1]));
 }
 
 // APP alone (pressure.cpp:42): the links' sum, without touching b.
@@ -361,7 +388,9 @@ void launch_pc_jacobi(const DevParams& p, PressurePtr w, const double* src, doub
 void launch_correct(const DevParams& p, PressurePtr w, const double* APU, const double* APV,
                     double* u, double* v, double* pf, cudaStream_t st) {
     const Range r = r_p(p);
-    k_correct<<<grid_of(r), dim3(BX, BY), 0, st>>>(p, w, APU, APV, u, v, pf, r);
+    const int pairs = (r.j1 - (r.j0 & ~1)) / 2 + 1;
+    k_correct<<<dim3((pairs + BX - 1) / BX, (r.rows() + BY - 1) / BY), dim3(BX, BY), 0, st>>>(p, w, APU, APV, u,
+                                                                                              v, pf, r);
     SGPU_LAUNCH();
 }
 void launch_copy(const double* src, double* dst, std::size_t n, cudaStream_t st) {

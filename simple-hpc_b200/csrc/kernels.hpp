@@ -210,9 +210,10 @@ void launch_b_to_f32(const DevParams& p, const double* bfield, const double* sum
 // pc64 = FP32 p' minus its FP64 mean over the p' cells (the field correct_mixed applied).
 void launch_pc_from32(const DevParams& p, const LevelView32& L0, const double* sum_pc, double* pc64,
                       cudaStream_t st);
+// correct with the FP32 level-0 p' minus its FP64 mean (the mixed iteration's last phase).
 void launch_correct_mixed(const DevParams& p, const LevelView32& L0, const double* sum_pc,
                           const double* APU, const double* APV, double* u, double* v, double* pf,
-                          double* pc64, cudaStream_t st);
+                          cudaStream_t st);
 
 // ---- fused fast path (fused.cu) ----
 // Rows per CTA segment of the streaming sweeps: one wave of blocks_per_sm resident CTAs per SM, at

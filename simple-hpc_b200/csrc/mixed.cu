@@ -539,8 +539,8 @@ __global__ void k_b_to_f32(DevParams p, const double* __restrict__ bfield, const
     }
 }
 
-// correct (pressure.cpp:136-157) in FP64 from the FP32 p' minus its FP64 mean; also stores that
-// p' in the FP64 pc field. Two adjacent columns per thread: the FP64 arrays are read and written as
+// correct (pressure.cpp:136-157) in FP64 from the FP32 p' minus its FP64 mean (the FP64 p' field
+// is formed from it on demand, k_pc_from32). Two adjacent columns per thread: the FP64 arrays are read and written as
 // 16-byte pairs (j even; the pitch is even), the FP32 p' as scalars. Elements of a pair that are not
 // cells of the correction keep their values (the thread writes back what it read). Against one cell
 // per thread with 8-byte accesses (4096^2: 0.26 ms, long-scoreboard bound), the pairs halve the
@@ -549,7 +549,7 @@ __global__ void __launch_bounds__(256)
     k_correct_mixed(DevParams p, const float* __restrict__ pc32, int ld32,
                           const double* __restrict__ sum_pc, const double* __restrict__ APU,
                           const double* __restrict__ APV, double* __restrict__ u, double* __restrict__ v,
-                          double* __restrict__ pf, double* __restrict__ pc64) {
+                          double* __restrict__ pf) {
     const int H = p.H;
     const int j = pair_col0(p) + 2 * static_cast<int>(blockIdx.x * 32 + threadIdx.x);
     const int I = static_cast<int>(blockIdx.y * 8 + threadIdx.y);
@@ -575,14 +575,12 @@ __global__ void __launch_bounds__(256)
         if (j <= p.NY + H - 1) un.x = uu.x + p.dy * (pc - (static_cast<double>(c1) - m)) / au.x;
         if (I >= 1) vn.x = vv.x + p.dx * (pc - (static_cast<double>(n0) - m)) / av.x;
         pn.x = pp.x + p.ap * pc;
-        if (pc64) pc64[q] = pc;
     }
     if (cell1) {
         const double pc = static_cast<double>(c1) - m;
         if (j + 1 <= p.NY + H - 1) un.y = uu.y + p.dy * (pc - (static_cast<double>(c2) - m)) / au.y;
         if (I >= 1) vn.y = vv.y + p.dx * (pc - (static_cast<double>(n1) - m)) / av.y;
         pn.y = pp.y + p.ap * pc;
-        if (pc64) pc64[q + 1] = pc;
     }
     *reinterpret_cast<double2*>(pf + q) = pn;
     *reinterpret_cast<double2*>(u + q) = un;
@@ -840,9 +838,9 @@ void launch_pc_from64(const DevParams& p, const double* src, const double* sum_p
 
 void launch_correct_mixed(const DevParams& p, const LevelView32& L0, const double* sum_pc,
                           const double* APU, const double* APV, double* u, double* v, double* pf,
-                          double* pc64, cudaStream_t st) {
+                          cudaStream_t st) {
     const dim3 grid((pair_count(p) + 31) / 32, (p.NX + 7) / 8);
-    k_correct_mixed<<<grid, dim3(32, 8), 0, st>>>(p, L0.x, L0.stride, sum_pc, APU, APV, u, v, pf, pc64);
+    k_correct_mixed<<<grid, dim3(32, 8), 0, st>>>(p, L0.x, L0.stride, sum_pc, APU, APV, u, v, pf);
     SGPU_LAUNCH();
 }
 

@@ -490,7 +490,7 @@ struct Solver {
             last_vcycles = run_cycles(L0, !guess, vcycle32);
             launch_tree_sum(L0.x, L0.stride, L0.nx, L0.ny, part, sums + 26, st); // the mean of p'
             mark(SGPU_PH_CORRECT);
-            launch_correct_mixed(dp, L0, sums + 26, cu.a[8], cv.a[8], u, v, pf, nullptr, st);
+            launch_correct_mixed(dp, L0, sums + 26, cu.a[8], cv.a[8], u, v, pf, st);
         }
         mark(SGPU_PH_COUNT);
     }

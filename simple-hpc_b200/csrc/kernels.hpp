@@ -119,6 +119,14 @@ using MgLevels = MgLevelsT<double>;
 template <class T>
 void launch_mg_tail(const MgLevelsT<T>& lv, int first, int pre, int post, double omega, double tol,
                     double* rowbuf, int* sweeps_out, cudaStream_t st);
+// The float V-cycle's levels from `first` on one thread-block cluster of 16 CTAs (mg.cu,
+// k_mg_tail_cluster): the levels of more than 1024 cells split by rows, the rest and the coarsest
+// solve on one CTA. mg_cluster_tail_first: the first level from which it applies (at most 65536
+// cells), or `fallback` where the device or the grid does not allow it. launch_mg_tail_cluster
+// returns false (and launches nothing) where it does not apply from `first`.
+int mg_cluster_tail_first(const MgLevelsT<float>& lv, int fallback);
+bool launch_mg_tail_cluster(const MgLevelsT<float>& lv, int first, int pre, int post, double omega, double tol,
+                            int* sweeps_out, cudaStream_t st);
 
 // ---- streaming multigrid level kernels (mg_fast.cu), double and float ----
 bool mg_fast_supported(int pre, int post);

@@ -12,6 +12,11 @@
 #include "kernels.hpp"
 #include "blocksum.cuh"
 
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cstdlib>
+
 namespace sgpu {
 
 namespace {
@@ -447,6 +452,192 @@ __global__ void __launch_bounds__(kCoarseThreads)
     for (int l = first; l < nl; ++l) slevel_store(lv.L[l], sl(l));
 }
 
+#ifdef SGPU_FLOAT_UNIT
+// ---- the float tail on a thread-block cluster ----
+//
+// Levels [first, lg) of the float V-cycle are split by rows over the kClusterTail CTAs of one
+// cluster, each CTA's band of a level held in its shared memory as an SLevel whose ring rows are
+// ghost copies of the neighbouring bands' edge rows; levels [lg, nl) (at most kGatherCells cells
+// each) and the coarsest solve run on CTA 0 as in k_mg_tail_smem. The passes and per-cell
+// expressions are k_mg_tail_smem's, with a cluster barrier between passes instead of a block
+// barrier. Levels halve exactly (mg_level_dims halves only even sizes), and the bands of the
+// coarsest split level start at even rows, so every band of every split level starts at an even
+// row: a 2 x 2 restriction block and a prolongation parent lie in the CTA's own bands, and the
+// red-black colour of a cell is the parity of its local row plus column. A pass that updates a
+// band's first or last row also stores the value into the ghost row of the neighbouring band
+// (distributed shared memory). In a colour pass the neighbours read only the other colour's ghost
+// cells, and a prolongation reads no ghost cell, so the stores race with no read, and one cluster
+// barrier per pass publishes them.
+constexpr int kClusterTail = 16;        // CTAs per cluster (a non-portable size)
+constexpr int kGatherCells = 1024;      // levels of at most this many cells run on CTA 0
+constexpr int kClusterTailCells = 65536; // the cluster tail takes levels of at most this many cells
+
+struct ClusterTailPlan {
+    int first, lg, nl;             // split levels [first, lg), gathered levels [lg, nl)
+    int band[kClusterTail + 1];    // band starts of level lg - 1 for ranks 0 .. R (band[R] = its nx)
+    int off[24];                   // byte offset of each level's block in every CTA's shared memory
+    int rows[24];                  // rows allocated per split level (its largest band)
+    int bytes;                     // dynamic shared memory per CTA
+};
+
+namespace cg = cooperative_groups;
+
+// One colour of smooth on a band; xup / xdn: the x arrays of the bands above / below (null at the
+// cluster's ends), mup: the rows of the band above (its bottom ghost row mirrors our row 0).
+__device__ void c_smooth(const SLevel& L, float* xup, int mup, float* xdn, int colour) {
+    const int w = static_cast<int>(threadIdx.x) >> 5, lane = static_cast<int>(threadIdx.x) & 31;
+    const int nw = static_cast<int>(blockDim.x) >> 5, S = L.S;
+    for (int I = w; I < L.nx; I += nw)
+        for (int J = ((I + colour) & 1) + 2 * lane; J < L.ny; J += 64) {
+            const int q = L.at(I, J);
+            const float4 a = L.l4[q];
+            const float v = rb_value(L.b[q], a.x * L.x[q + 1] + a.y * L.x[q - 1] + a.w * L.x[q + S] +
+                                                 a.z * L.x[q - S],
+                                     L.ap[q]);
+            L.x[q] = v;
+            if (I == 0 && xup) xup[(mup + 1) * S + J + 1] = v;
+            if (I == L.nx - 1 && xdn) xdn[J + 1] = v;
+        }
+    cg::this_cluster().sync();
+}
+// The residual of the band F restricted 2 x 2 into rows c0 + I of the coarse level C (a band of
+// this CTA, c0 = 0, or the gathered level on CTA 0), C.x = 0 there.
+__device__ void c_restrict(const SLevel& F, const SLevel& C, int c0) {
+    const int w = static_cast<int>(threadIdx.x) >> 5, lane = static_cast<int>(threadIdx.x) & 31;
+    const int nw = static_cast<int>(blockDim.x) >> 5, S = F.S;
+    auto r = [&](int q) {
+        const float4 a = F.l4[q];
+        return F.b[q] - (F.ap[q] * F.x[q] - (a.x * F.x[q + 1] + a.y * F.x[q - 1] + a.w * F.x[q + S] + a.z * F.x[q - S]));
+    };
+    for (int I = w; I < F.nx / 2; I += nw)
+        for (int J = lane; J < C.ny; J += 32) {
+            const int f = F.at(2 * I, 2 * J), cq = C.at(c0 + I, J);
+            C.b[cq] = r(f) + r(f + 1) + r(f + S) + r(f + S + 1);
+            C.x[cq] = 0.0f;
+        }
+    cg::this_cluster().sync();
+}
+// prolong into the band F from rows c0 + I / 2 of the coarse level C (this CTA's band, c0 = 0, or
+// the gathered level on CTA 0), with the ghost stores of c_smooth.
+__device__ void c_prolong(const SLevel& C, int c0, const SLevel& F, float* xup, int mup, float* xdn, float om) {
+    const int w = static_cast<int>(threadIdx.x) >> 5, lane = static_cast<int>(threadIdx.x) & 31;
+    const int nw = static_cast<int>(blockDim.x) >> 5, S = F.S;
+    for (int I = w; I < F.nx; I += nw)
+        for (int J = lane; J < F.ny; J += 32) {
+            const int q = F.at(I, J);
+            const float v = F.x[q] + om * C.x[C.at(c0 + (I >> 1), J >> 1)];
+            F.x[q] = v;
+            if (I == 0 && xup) xup[(mup + 1) * S + J + 1] = v;
+            if (I == F.nx - 1 && xdn) xdn[J + 1] = v;
+        }
+    cg::this_cluster().sync();
+}
+
+__global__ void __launch_bounds__(kCoarseThreads)
+    k_mg_tail_cluster(MgLevelsT<float> lv, ClusterTailPlan pl, int pre, int post, double omega, double tol,
+                      int* sweeps_out) {
+    extern __shared__ __align__(16) unsigned char tail_sm[];
+    cg::cluster_group cl = cg::this_cluster();
+    const int R = static_cast<int>(cl.num_blocks()), rank = static_cast<int>(cl.block_rank());
+    const int first = pl.first, lg = pl.lg, nl = pl.nl, Lc = lg - 1;
+    auto start = [&](int l, int rr) { return pl.band[rr] << (Lc - l); }; // band start of rank rr
+    // this CTA's band of split level l (laid out for the level's largest band: the same offsets in
+    // every CTA, so a neighbour's arrays are this CTA's mapped to its rank)
+    auto band = [&](int l) {
+        SLevel s = slevel_at(tail_sm + pl.off[l], pl.rows[l], lv.L[l].ny);
+        s.nx = start(l, rank + 1) - start(l, rank);
+        return s;
+    };
+    auto xup = [&](const SLevel& s) { return rank > 0 ? cl.map_shared_rank(s.x, rank - 1) : nullptr; };
+    auto xdn = [&](const SLevel& s) { return rank < R - 1 ? cl.map_shared_rank(s.x, rank + 1) : nullptr; };
+    auto mup = [&](int l) { return rank > 0 ? start(l, rank) - start(l, rank - 1) : 0; };
+    auto gathered = [&](int l) { return slevel_at(tail_sm + pl.off[l], lv.L[l].nx, lv.L[l].ny); };
+    auto gathered0 = [&](int l) { // the gathered level l in CTA 0's shared memory
+        SLevel s = gathered(l);
+        s.l4 = cl.map_shared_rank(s.l4, 0);
+        s.x = cl.map_shared_rank(s.x, 0);
+        s.b = cl.map_shared_rank(s.b, 0);
+        s.ap = cl.map_shared_rank(s.ap, 0);
+        return s;
+    };
+    cl.sync(); // every CTA of the cluster runs before any touches another's shared memory
+    for (int l = first; l < lg; ++l) { // the bands, with their ghost rows of x
+        const LevelViewT<float>& L = lv.L[l];
+        const SLevel s = band(l);
+        const int g0 = start(l, rank), n2 = (s.nx + 2) * s.S;
+        for (int k = threadIdx.x; k < n2; k += blockDim.x) {
+            const int I = k / s.S - 1, J = k % s.S - 1, g = g0 + I;
+            const bool cin = J >= 0 && J < L.ny, own = cin && I >= 0 && I < s.nx;
+            const int q = g * L.stride + J;
+            float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (own) {
+                const Links<float> k4 = links(L, q);
+                a = make_float4(k4.e, k4.w, k4.n, k4.s);
+            }
+            s.l4[k] = a;
+            s.ap[k] = own ? L.AP[q] : 0.0f;
+            s.b[k] = (own && l == first) ? L.b[q] : 0.0f;
+            s.x[k] = (l == first && cin && g >= 0 && g < L.nx) ? L.x[q] : 0.0f;
+        }
+    }
+    if (rank == 0)
+        for (int l = lg; l < nl; ++l) slevel_load(lv.L[l], gathered(l), false);
+    cl.sync();
+    const float om = static_cast<float>(omega);
+    for (int l = first; l < lg; ++l) {
+        const SLevel s = band(l);
+        for (int k = 0; k < pre; ++k) {
+            c_smooth(s, xup(s), mup(l), xdn(s), 0);
+            c_smooth(s, xup(s), mup(l), xdn(s), 1);
+        }
+        if (l + 1 < lg) c_restrict(s, band(l + 1), 0);
+        else c_restrict(s, gathered0(lg), start(l, rank) / 2);
+    }
+    if (rank == 0) { // the gathered levels and the coarsest solve, as k_mg_tail_smem
+        for (int l = lg; l + 1 < nl; ++l) {
+            const SLevel L = gathered(l);
+            for (int k = 0; k < pre; ++k) {
+                s_smooth(L, 0);
+                s_smooth(L, 1);
+            }
+            s_residual_restrict(L, gathered(l + 1));
+        }
+        if (threadIdx.x < 32) warp_coarse_core(gathered(nl - 1), tol, sweeps_out);
+        __syncthreads();
+        for (int l = nl - 2; l >= lg; --l) {
+            const SLevel L = gathered(l);
+            s_prolong(gathered(l + 1), L, om);
+            for (int k = 0; k < post; ++k) {
+                s_smooth(L, 0);
+                s_smooth(L, 1);
+            }
+        }
+    }
+    cl.sync();
+    for (int l = lg - 1; l >= first; --l) {
+        const SLevel s = band(l);
+        if (l + 1 < lg) c_prolong(band(l + 1), 0, s, xup(s), mup(l), xdn(s), om);
+        else c_prolong(gathered0(lg), start(l, rank) / 2, s, xup(s), mup(l), xdn(s), om);
+        for (int k = 0; k < post; ++k) {
+            c_smooth(s, xup(s), mup(l), xdn(s), 0);
+            c_smooth(s, xup(s), mup(l), xdn(s), 1);
+        }
+    }
+    for (int l = first; l < lg; ++l) { // the bands' x and b back
+        const LevelViewT<float>& L = lv.L[l];
+        const SLevel s = band(l);
+        const int g0 = start(l, rank), n = s.nx * L.ny;
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            const int I = k / L.ny, J = k - I * L.ny;
+            L.x[(g0 + I) * L.stride + J] = s.x[s.at(I, J)];
+            L.b[(g0 + I) * L.stride + J] = s.b[s.at(I, J)];
+        }
+    }
+    if (rank == 0)
+        for (int l = lg; l < nl; ++l) slevel_store(lv.L[l], gathered(l));
+}
+#endif
+
 // coarse_solve (multigrid.cpp:120-140) of an FP64 level in one warp on a shared-memory copy, bit for
 // bit the passes of cta_coarse_solve: the same per-cell expressions, and det_sum's order (each row
 // added left to right by one lane, then the row sums in order by lane 0, multigrid.cpp:18-34), so
@@ -669,6 +860,110 @@ template <class T> void launch_mg_b_sq(const LevelViewT<T>& L, double* cells, cu
 void launch_mg_sub_mean(const LevelView& L, double* x, const double* sum, cudaStream_t st) {
     k_mg_sub_mean<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, st>>>(L, x, sum);
     SGPU_LAUNCH();
+}
+#endif
+
+#ifdef SGPU_FLOAT_UNIT
+namespace {
+// Dynamic shared memory per CTA of the cluster tail (the 227 KB a CTA may have).
+constexpr int kClusterSmemMax = 227 * 1024;
+
+// The cluster tail's plan from level `first`; false where it does not apply: fewer than one split
+// level, a split level that does not halve exactly into the next, a coarsest split level of fewer
+// than 2 rows per CTA, or more shared memory per CTA than kClusterSmemMax.
+bool cluster_tail_plan(const MgLevelsT<float>& lv, int first, ClusterTailPlan& pl) {
+    const int nl = lv.n;
+    if (nl > 24 || first < 0 || first >= nl - 1) return false;
+    int lg = first;
+    while (lg < nl - 1 && lv.L[lg].nx * lv.L[lg].ny > kGatherCells) ++lg;
+    if (lg == first || lv.L[lg].nx * lv.L[lg].ny > kGatherCells) return false;
+    for (int l = first; l < lg; ++l)
+        if (lv.L[l].nx != 2 * lv.L[l + 1].nx || lv.L[l].ny != 2 * lv.L[l + 1].ny) return false;
+    const int Lc = lg - 1, nxc = lv.L[Lc].nx;
+    if (nxc < 2 * kClusterTail) return false;
+    pl.first = first;
+    pl.lg = lg;
+    pl.nl = nl;
+    for (int r = 0; r < kClusterTail; ++r) pl.band[r] = 2 * ((r * (nxc / 2)) / kClusterTail);
+    pl.band[kClusterTail] = nxc;
+    int bytes = 0;
+    for (int l = first; l < lg; ++l) {
+        int rows = 0;
+        for (int r = 0; r < kClusterTail; ++r) rows = std::max(rows, (pl.band[r + 1] - pl.band[r]) << (Lc - l));
+        pl.rows[l] = rows;
+        pl.off[l] = bytes;
+        bytes += slevel_bytes(rows, lv.L[l].ny);
+    }
+    for (int l = lg; l < nl; ++l) {
+        pl.off[l] = bytes;
+        bytes += slevel_bytes(lv.L[l].nx, lv.L[l].ny);
+    }
+    pl.bytes = bytes;
+    return bytes <= kClusterSmemMax;
+}
+
+// Whether this device runs the cluster tail: its function attributes set (the dynamic shared memory
+// and the non-portable cluster size, once per device) and at least one such cluster resident.
+// SGPU_MG_CLUSTER=0 turns it off for the solvers created while it is set (their float tail then
+// runs as streamed levels and the single-CTA tail, as without a cluster).
+bool cluster_tail_available() {
+    if (const char* e = std::getenv("SGPU_MG_CLUSTER"))
+        if (std::atoi(e) == 0) return false;
+    static PerDeviceOnce once;
+    return once.get([] {
+        SGPU_CUDA(cudaFuncSetAttribute(k_mg_tail_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kClusterSmemMax));
+        SGPU_CUDA(cudaFuncSetAttribute(k_mg_tail_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(kClusterTail);
+        cfg.blockDim = dim3(kCoarseThreads);
+        cfg.dynamicSmemBytes = kClusterSmemMax;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = kClusterTail;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, k_mg_tail_cluster, &cfg) != cudaSuccess) {
+            (void)cudaGetLastError(); // not supported here: the clear-up of the failed query
+            return 0;
+        }
+        return n > 0 ? 1 : 0;
+    }) != 0;
+}
+} // namespace
+
+int mg_cluster_tail_first(const MgLevelsT<float>& lv, int fallback) {
+    if (!cluster_tail_available()) return fallback;
+    int t = 0;
+    while (t < lv.n - 1 && lv.L[t].nx * lv.L[t].ny > kClusterTailCells) ++t;
+    ClusterTailPlan pl{};
+    for (; t < fallback; ++t)
+        if (cluster_tail_plan(lv, t, pl)) return t;
+    return fallback;
+}
+
+bool launch_mg_tail_cluster(const MgLevelsT<float>& lv, int first, int pre, int post, double omega, double tol,
+                            int* sweeps_out, cudaStream_t st) {
+    ClusterTailPlan pl{};
+    if (!cluster_tail_plan(lv, first, pl)) return false;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kClusterTail);
+    cfg.blockDim = dim3(kCoarseThreads);
+    cfg.dynamicSmemBytes = static_cast<std::size_t>(pl.bytes);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = kClusterTail;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    SGPU_CUDA(cudaLaunchKernelEx(&cfg, k_mg_tail_cluster, lv, pl, pre, post, omega, tol, sweeps_out));
+    SGPU_LAUNCH();
+    return true;
 }
 #endif
 

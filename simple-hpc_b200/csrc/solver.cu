@@ -101,6 +101,9 @@ struct Solver {
     double* coarse_rowbuf = nullptr;
     bool mg_fast = false;            // streaming level kernels (mg_fast.cu) + single-CTA tail
     int mg_tail = 0;                 // first level handled by the tail kernel
+    // first level of the float V-cycle's tail: the cluster tail's (mg.cu, k_mg_tail_cluster) where
+    // the device and the grid allow it, else mg_tail
+    int mg_tail32 = 0;
     std::vector<double*> mg_x2;      // second iterate buffer per streamed level (interior (0,0))
     MgLevels mgl{};
     // build: form the coarse operators inside the cycle (the streamed levels' down kernels, then the
@@ -464,21 +467,24 @@ struct Solver {
         // p' starts from zero. The streaming level kernels need no cleared array for that: the
         // first cycle's k_mg_down does not read x (x_zero), a warm start writes every interior cell,
         // and the zero ring is never written after allocation. Level 0 inside the tail kernel
-        // (a grid of mg_tail = 0) reads x, so it is cleared there.
-        if (mg_tail == 0)
+        // (a grid of mg_tail32 = 0) reads x, so it is cleared there.
+        if (mg_tail32 == 0)
             SGPU_CUDA(cudaMemsetAsync(L0.x - (L0.stride + 1), 0,
                                       sizeof(float) * (L0.nx + 2) * static_cast<std::size_t>(L0.stride), st));
         const bool guess = apply_warm_start(L0);
         auto vcycle32 = [&](bool x_zero) {
-            for (int l = 0; l < mg_tail; ++l)
+            for (int l = 0; l < mg_tail32; ++l)
                 launch_mg_down<float>(lv32[l], lv32[l + 1], mg32_x2[l], prm.mg_pre, x_zero || l > 0, sms,
                                       min_seg, st, fused_build);
             if (fused_build)
-                for (std::size_t l = static_cast<std::size_t>(mg_tail) + 1; l < lv32.size(); ++l)
+                for (std::size_t l = static_cast<std::size_t>(mg_tail32) + 1; l < lv32.size(); ++l)
                     launch_mg_build<float>(lv32[l - 1], lv32[l], st);
-            launch_mg_tail<float>(mgl32, mg_tail, prm.mg_pre, prm.mg_post, prm.mg_omega, kCoarseTol32,
-                                  coarse_rowbuf, stats, st);
-            for (int l = mg_tail - 1; l >= 0; --l)
+            if (mg_tail32 == mg_tail ||
+                !launch_mg_tail_cluster(mgl32, mg_tail32, prm.mg_pre, prm.mg_post, prm.mg_omega, kCoarseTol32,
+                                        stats, st))
+                launch_mg_tail<float>(mgl32, mg_tail32, prm.mg_pre, prm.mg_post, prm.mg_omega, kCoarseTol32,
+                                      coarse_rowbuf, stats, st);
+            for (int l = mg_tail32 - 1; l >= 0; --l)
                 launch_mg_up<float>(lv32[l + 1], lv32[l], mg32_x2[l], lv32[l].x, prm.mg_omega,
                                     prm.mg_post, sms, min_seg, st);
         };
@@ -516,7 +522,7 @@ struct Solver {
         int c = 0, run = 0, cur = 0;
         bool first = true, from_guess = guess;
         while (c < prm.pressure_maxit) {
-            if (mg_tail == 0 && !from_guess) launch_zero_x(L0, st); // the tail kernel reads level 0's x
+            if (mg_tail32 == 0 && !from_guess) launch_zero_x(L0, st); // the tail kernel reads level 0's x
             vcycle(!from_guess);
             ++c;
             ++run;
@@ -849,6 +855,7 @@ Solver::Solver(const sgpu_params_t& p, const double* hu, const double* hv, const
         }
         mgl32.n = nl;
         for (int l = 0; l < nl && l < 24; ++l) mgl32.L[l] = lv32[l];
+        mg_tail32 = mg_cluster_tail_first(mgl32, mg_tail);
     }
 
     if (p.warm_start == 1) {

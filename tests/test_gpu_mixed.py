@@ -144,3 +144,28 @@ def test_mixed_odd_grids_close_to_fp64(sgpu_mod, nx, ny, scheme, order):
             mx, l2 = rel_errors(s.download(f), ref[f])
             print(f"field {f}: max rel {mx:.3e}, L2 rel {l2:.3e}")
             assert mx < 2e-6 and l2 < 2e-6
+
+
+@pytest.mark.parametrize("nx,ny", [(128, 128), (96, 160), (520, 96), (512, 512)])
+def test_cluster_tail_matches_single_cta_tail(sgpu_mod, monkeypatch, nx, ny):
+    """The float V-cycle's levels of at most 65536 cells on one 16-CTA cluster (bands of rows with
+    ghost rows in distributed shared memory; the levels of at most 1024 cells and the coarsest solve
+    on one CTA) against the streamed levels and the single-CTA tail (SGPU_MG_CLUSTER=0): the same
+    passes in the same colour order with the same per-cell expressions, which give the same bits
+    (residual log and fields) after 8 outer iterations."""
+    base = snapshot_config("short_16")
+    base.update(N_cells_x=str(nx), N_cells_y=str(ny), Re="1000", convection_scheme="QUICK",
+                diffusion_order="4", momentum_solver="gs_multicolour", pressure_solver="mg",
+                maxit="8", error_tolerance="0", precision="mixed")
+    out = {}
+    for flag in ("0", "1"):
+        monkeypatch.setenv("SGPU_MG_CLUSTER", flag)
+        with sgpu_mod.Solver(sgpu_mod.params_from_config(config_text(base))) as s:
+            _, log = s.run(8)
+            out[flag] = (log, [s.download(f) for f in (0, 1, 2)])
+    (l0, f0), (l1, f1) = out["0"], out["1"]
+    assert bit_equal(l0, l1)
+    for a, b in zip(f0, f1):
+        mx, l2 = rel_errors(b, a)
+        print(f"cluster vs single-CTA tail: max rel {mx:.3e}, L2 rel {l2:.3e}")
+        assert bit_equal(a, b)

@@ -123,6 +123,9 @@ struct Solver {
     int min_seg = 8;
     void use_batch_shape() {
         min_seg = 0;
+        // A batch fills the GPU with many cavities' kernels, so SM time, not latency, bounds it: the
+        // single-CTA tail (one SM) instead of the cluster tail (16 SMs for a shorter time).
+        mg_tail32 = mg_tail;
         if (fast)
             seg_rows = mixed ? stream_seg_rows(dp, sms, corr_blocks_per_sm(dp.ncol), 0, corr_threads())
                              : stream_seg_rows(dp, sms, 2, 0);

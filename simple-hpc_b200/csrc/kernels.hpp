@@ -195,6 +195,12 @@ int launch_mom_prep_mixed(const DevParams& p, bool v_component, const double* x,
 void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, float* eout,
                        MomRec32 rec, bool e_zero, int seg_rows, unsigned* err, cudaStream_t st,
                        double* xfinal = nullptr);
+// All nsweeps correction sweeps of a component on one 16-CTA thread-block cluster, e from zero and
+// x += e at the end, where the component's records and e fit the cluster's shared memory (small
+// grids); returns false, and launches nothing, where they do not (or the device runs no such
+// cluster, or SGPU_CORR_CLUSTER=0).
+bool launch_corr_cluster(const DevParams& p, bool v_component, MomRec32 rec, int nsweeps, double* x,
+                         cudaStream_t st);
 // assemble_p with the FP32 level-0 operator; per block one partial sum of |b| into part[k] and one
 // of b into part[n + k] (n = the returned number of blocks).
 int launch_assemble_p_mixed(const DevParams& p, const double* APU, const double* APV, const double* u,

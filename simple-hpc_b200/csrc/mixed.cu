@@ -21,6 +21,8 @@
 #include "blocksum.cuh"
 #include "stencil.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cstdint>
 #include <cstdlib>
@@ -436,6 +438,100 @@ __global__ void __launch_bounds__(NT, MINB)
     cp_async_wait<0>();
 }
 
+// ---- small grids: all of a component's correction sweeps on one thread-block cluster ----
+//
+// Where the whole component fits (40 B of records and 4 B of e per cell over kCorrCluster CTAs'
+// shared memory), one 16-CTA cluster runs every inner sweep: the update range's rows are split into
+// bands, each CTA holding its band's records and its e with two ghost rows on each side (the
+// stencil's reach). The sweeps go colour by colour, as the reference's (momentum_u.cpp:123-143), the
+// colour-c cells of every band updated with the same expression as k_corr_stream; a cluster barrier
+// ends each colour. An update of one of a band's first or last two rows also stores the value into
+// the neighbouring band's ghost copy (distributed shared memory): no cell of the stencil shares a
+// cell's colour, so within a colour pass no ghost cell that is written is read, and the barrier
+// publishes them. e starts at zero (the first sweep's e_in) and the FP64 field takes x += e at the
+// end, as the streaming kernels' last sweep does. One launch replaces maxit_inner launches, each of
+// which walked its halo and colour skew rows at a barrier per super-step.
+constexpr int kCorrCluster = 16;
+constexpr int kCorrGhost = 2;
+
+struct CorrClusterPlan {
+    int band[kCorrCluster + 1]; // first row of each CTA's band of the update range (band[R]: one past)
+    int rows;                   // rows of the largest band
+    int bytes;                  // dynamic shared memory per CTA
+};
+
+template <int NCOL, bool V>
+__global__ void __launch_bounds__(512)
+    k_corr_cluster(DevParams p, MomRec32 rec, CorrClusterPlan pl, int nsweeps, double* __restrict__ x) {
+    namespace cg = cooperative_groups;
+    constexpr int G = kCorrGhost;
+    extern __shared__ __align__(16) unsigned char cs_raw[];
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = static_cast<int>(cl.block_rank()), R = static_cast<int>(cl.num_blocks());
+    const int nc = p.ncols, i0 = pl.band[rank], m = pl.band[rank + 1] - i0;
+    const int ne = ((pl.rows + 2 * G) * nc + 3) & ~3;
+    float* e = reinterpret_cast<float*>(cs_raw); // rows -G .. rows + G - 1 of the band, all columns
+    float4* s_near = reinterpret_cast<float4*>(e + ne);
+    float4* s_far = s_near + pl.rows * nc;
+    float2* s_diag = reinterpret_cast<float2*>(NCOL == 5 ? s_far + pl.rows * nc : s_far);
+    const int uj0 = p.H + 1, uj1 = V ? p.NY + p.H : p.NY + p.H - 1;
+    const float relax = static_cast<float>(V ? p.av : p.au);
+    cl.sync(); // every CTA of the cluster runs before any touches another's shared memory
+    for (int k = threadIdx.x; k < (m + 2 * G) * nc; k += blockDim.x) e[k] = 0.0f;
+    for (int k = threadIdx.x; k < m * nc; k += blockDim.x) {
+        const int Il = k / nc, j = k - Il * nc, i = i0 + Il;
+        if (j < uj0 || j > uj1) continue;
+        const int c = NCOL == 5 ? (i + 3 * j) % 5 : (i + j) & 1; // the record sits at step row i + 2c
+        const std::size_t q = static_cast<std::size_t>(i + 2 * c) * p.pitch + j;
+        s_near[k] = rec.near_links[q];
+        if (NCOL == 5) s_far[k] = rec.far_links[q];
+        s_diag[k] = rec.diag[q];
+    }
+    // The band above holds our rows 0 .. G-1 as its bottom ghost rows (its local rows mup ..), the
+    // band below our rows m-G .. m-1 as its top ghost rows (its local rows -G .. -1).
+    float* eup = rank > 0 ? cl.map_shared_rank(e, rank - 1) : nullptr;
+    float* edn = rank < R - 1 ? cl.map_shared_rank(e, rank + 1) : nullptr;
+    const int mup = rank > 0 ? i0 - pl.band[rank - 1] : 0;
+    cl.sync();
+    const int lane = static_cast<int>(threadIdx.x) & 31, w = static_cast<int>(threadIdx.x) >> 5;
+    const int nw = static_cast<int>(blockDim.x) >> 5;
+    for (int sw = 0; sw < nsweeps; ++sw)
+        for (int c = 0; c < NCOL; ++c) {
+            for (int Il = w; Il < m; Il += nw) {
+                const int i = i0 + Il;
+                // the colour-c cells of row i: j = 2 (c - i) mod 5 (five colours), (c - i) mod 2 (two)
+                const int res = NCOL == 5 ? ((2 * (c - i)) % 5 + 5) % 5 : ((c - i) & 1);
+                for (int j = uj0 + ((res - uj0) % NCOL + NCOL) % NCOL + NCOL * lane; j <= uj1; j += NCOL * 32) {
+                    const int k = Il * nc + j;
+                    const float4 a = s_near[k];
+                    const float2 dg = s_diag[k];
+                    float* rc = e + (Il + G) * nc + j;
+                    const float ee = rc[1], ew = rc[-1];
+                    const float en = rc[-nc], es = rc[nc];
+                    float nb = a.x * ee + a.y * ew + a.z * en + a.w * es;
+                    if (NCOL == 5) {
+                        const float4 b = s_far[k];
+                        const float eee = rc[2], eww = rc[-2];
+                        const float enn = rc[-2 * nc], ess = rc[2 * nc];
+                        nb += b.x * eee + b.y * eww + b.z * enn + b.w * ess;
+                    }
+                    const float e0 = rc[0];
+                    const float v = e0 + relax * ((dg.y + nb) * dg.x - e0);
+                    rc[0] = v;
+                    if (Il < G && eup) eup[(mup + G + Il) * nc + j] = v;
+                    if (Il >= m - G && edn) edn[(Il - m + G) * nc + j] = v;
+                }
+            }
+            cl.sync();
+        }
+    for (int k = threadIdx.x; k < m * nc; k += blockDim.x) { // x += e (FP64), the own cells
+        const int Il = k / nc, j = k - Il * nc;
+        if (j < uj0 || j > uj1) continue;
+        const std::size_t q = static_cast<std::size_t>(i0 + Il) * p.pitch + j;
+        x[q] = x[q] + static_cast<double>(e[(Il + G) * nc + j]);
+    }
+}
+
 #endif // SGPU_FLOAT_UNIT
 
 // Rows per thread of k_assemble_p_mixed, and the first (even) column of the column pairs that the
@@ -750,6 +846,75 @@ void launch_corr_m(const DevParams& p, const float* ein, float* eout, MomRec32 r
     launch_corr<NCOL, V, kCorrNT, kCorrMinb>(p, ein, eout, rec, e_zero, seg_rows, xfinal, err, st);
 }
 
+
+// The cluster sweep's plan: bands of at least kCorrGhost rows, the shared memory of the largest
+// within a CTA's 227 KB; false where the component does not fit.
+bool corr_cluster_plan(const DevParams& p, bool v, CorrClusterPlan& pl) {
+    const Range ur = update_range(p, v);
+    const int n = ur.rows();
+    if (n < kCorrGhost * kCorrCluster || ur.cols() <= 0) return false;
+    for (int r = 0; r <= kCorrCluster; ++r) pl.band[r] = ur.i0 + (r * n) / kCorrCluster;
+    pl.rows = (n + kCorrCluster - 1) / kCorrCluster;
+    const long long ne = ((static_cast<long long>(pl.rows) + 2 * kCorrGhost) * p.ncols + 3) / 4 * 4;
+    const long long bytes = ne * 4 + static_cast<long long>(pl.rows) * p.ncols * (p.ncol == 5 ? 40 : 24);
+    if (bytes > 227 * 1024) return false;
+    pl.bytes = static_cast<int>(bytes);
+    return true;
+}
+
+// Whether this device runs the cluster sweep (its attributes set once per device, one cluster of
+// kCorrCluster CTAs with 227 KB each resident). SGPU_CORR_CLUSTER=0 turns it off.
+bool corr_cluster_available() {
+    if (const char* e = std::getenv("SGPU_CORR_CLUSTER"))
+        if (std::atoi(e) == 0) return false;
+    static PerDeviceOnce once;
+    return once.get([] {
+        auto setup = [](auto kernel) {
+            SGPU_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+            SGPU_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        };
+        setup(k_corr_cluster<5, false>);
+        setup(k_corr_cluster<5, true>);
+        setup(k_corr_cluster<2, false>);
+        setup(k_corr_cluster<2, true>);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(kCorrCluster);
+        cfg.blockDim = dim3(512);
+        cfg.dynamicSmemBytes = 227 * 1024;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = kCorrCluster;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int nclusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&nclusters, k_corr_cluster<5, false>, &cfg) != cudaSuccess) {
+            (void)cudaGetLastError(); // not supported here: the clear-up of the failed query
+            return 0;
+        }
+        return nclusters > 0 ? 1 : 0;
+    }) != 0;
+}
+
+template <int NCOL, bool V>
+void launch_corr_cluster_t(const DevParams& p, MomRec32 rec, const CorrClusterPlan& pl, int nsweeps, double* x,
+                           cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kCorrCluster);
+    cfg.blockDim = dim3(512);
+    cfg.dynamicSmemBytes = static_cast<std::size_t>(pl.bytes);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = kCorrCluster;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    SGPU_CUDA(cudaLaunchKernelEx(&cfg, k_corr_cluster<NCOL, V>, p, rec, pl, nsweeps, x));
+    SGPU_LAUNCH();
+}
 #endif // SGPU_FLOAT_UNIT
 
 } // namespace
@@ -855,6 +1020,20 @@ void launch_corr_sweep(const DevParams& p, bool v_component, const float* ein, f
         if (v_component) launch_corr_m<2, true>(p, ein, eout, rec, e_zero, seg_rows, xfinal, err, st);
         else launch_corr_m<2, false>(p, ein, eout, rec, e_zero, seg_rows, xfinal, err, st);
     }
+}
+
+bool launch_corr_cluster(const DevParams& p, bool v_component, MomRec32 rec, int nsweeps, double* x,
+                         cudaStream_t st) {
+    CorrClusterPlan pl{};
+    if (nsweeps < 1 || !corr_cluster_available() || !corr_cluster_plan(p, v_component, pl)) return false;
+    if (p.ncol == 5) {
+        if (v_component) launch_corr_cluster_t<5, true>(p, rec, pl, nsweeps, x, st);
+        else launch_corr_cluster_t<5, false>(p, rec, pl, nsweeps, x, st);
+    } else {
+        if (v_component) launch_corr_cluster_t<2, true>(p, rec, pl, nsweeps, x, st);
+        else launch_corr_cluster_t<2, false>(p, rec, pl, nsweeps, x, st);
+    }
+    return true;
 }
 
 void init_mixed_kernels() {

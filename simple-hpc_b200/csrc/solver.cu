@@ -430,6 +430,11 @@ struct Solver {
         const int n = vcomp ? prm.maxit_inner_v : prm.maxit_inner_u;
         int cur = 0; // e32[cur] holds the current correction (zero before the first sweep)
         sweep_mark(vcomp, 0, n);
+        // small grids: every sweep in one cluster launch where the component fits
+        if (launch_corr_cluster(dp, vcomp, rec32, n, x, st)) {
+            sweep_mark(vcomp, 1, n);
+            return;
+        }
         for (int k = 0; k < n; ++k) {
             launch_corr_sweep(dp, vcomp, e32[cur], e32[1 - cur], rec32, k == 0, seg_rows, corr_err, st,
                               k == n - 1 ? x : nullptr); // the last sweep adds e into x

@@ -169,3 +169,32 @@ def test_cluster_tail_matches_single_cta_tail(sgpu_mod, monkeypatch, nx, ny):
         mx, l2 = rel_errors(b, a)
         print(f"cluster vs single-CTA tail: max rel {mx:.3e}, L2 rel {l2:.3e}")
         assert bit_equal(a, b)
+
+
+@pytest.mark.parametrize("nx,ny,scheme,order,inner", [(128, 128, "QUICK", 4, 4), (96, 160, "QUICK", 2, 3),
+                                                      (520, 96, "UDS", 2, 4), (33, 7, "QUICK", 4, 2),
+                                                      (256, 256, "QUICK", 4, 4)])
+def test_cluster_sweep_matches_streaming_sweep(sgpu_mod, monkeypatch, nx, ny, scheme, order, inner):
+    """A small grid's correction sweeps on one 16-CTA cluster (bands of rows with two ghost rows in
+    distributed shared memory, colour by colour, one launch per component) against the streaming
+    sweep kernel (SGPU_CORR_CLUSTER=0): the same colour order and per-cell expression, so the same
+    residual log and fields after 8 outer iterations, for five and two colours and a grid whose bands
+    are two rows high."""
+    base = snapshot_config("short_16")
+    base.update(N_cells_x=str(nx), N_cells_y=str(ny), Re="1000", convection_scheme=scheme,
+                diffusion_order=str(order), momentum_solver="gs_multicolour", pressure_solver="mg",
+                maxit="8", error_tolerance="0", precision="mixed", maxit_inner_u=str(inner),
+                maxit_inner_v=str(inner))
+    out = {}
+    for flag in ("0", "1"):
+        monkeypatch.setenv("SGPU_CORR_CLUSTER", flag)
+        with sgpu_mod.Solver(sgpu_mod.params_from_config(config_text(base))) as s:
+            _, log = s.run(8)
+            out[flag] = (log, [s.download(f) for f in (0, 1, 2)])
+    (l0, f0), (l1, f1) = out["0"], out["1"]
+    for a, b in zip(f0, f1):
+        mx, l2 = rel_errors(b, a)
+        print(f"cluster vs streaming sweep: max rel {mx:.3e}, L2 rel {l2:.3e}")
+    assert bit_equal(l0, l1)
+    for a, b in zip(f0, f1):
+        assert bit_equal(a, b)

@@ -911,9 +911,13 @@ bool cluster_tail_available() {
         if (std::atoi(e) == 0) return false;
     static PerDeviceOnce once;
     return once.get([] {
-        SGPU_CUDA(cudaFuncSetAttribute(k_mg_tail_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       kClusterSmemMax));
-        SGPU_CUDA(cudaFuncSetAttribute(k_mg_tail_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        // a device that refuses either attribute runs the kernels without a cluster
+        if (cudaFuncSetAttribute(k_mg_tail_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, kClusterSmemMax) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(k_mg_tail_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return 0;
+        }
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(kClusterTail);
         cfg.blockDim = dim3(kCoarseThreads);

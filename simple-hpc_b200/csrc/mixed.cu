@@ -869,14 +869,17 @@ bool corr_cluster_available() {
         if (std::atoi(e) == 0) return false;
     static PerDeviceOnce once;
     return once.get([] {
+        // a device that refuses either attribute runs the streaming sweep
         auto setup = [](auto kernel) {
-            SGPU_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-            SGPU_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) ==
+                       cudaSuccess &&
+                   cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
         };
-        setup(k_corr_cluster<5, false>);
-        setup(k_corr_cluster<5, true>);
-        setup(k_corr_cluster<2, false>);
-        setup(k_corr_cluster<2, true>);
+        if (!setup(k_corr_cluster<5, false>) || !setup(k_corr_cluster<5, true>) || !setup(k_corr_cluster<2, false>) ||
+            !setup(k_corr_cluster<2, true>)) {
+            (void)cudaGetLastError();
+            return 0;
+        }
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(kCorrCluster);
         cfg.blockDim = dim3(512);

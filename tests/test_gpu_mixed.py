@@ -146,8 +146,9 @@ def test_mixed_odd_grids_close_to_fp64(sgpu_mod, nx, ny, scheme, order):
             assert mx < 2e-6 and l2 < 2e-6
 
 
-@pytest.mark.parametrize("nx,ny", [(128, 128), (96, 160), (520, 96), (512, 512)])
-def test_cluster_tail_matches_single_cta_tail(sgpu_mod, monkeypatch, nx, ny):
+@pytest.mark.parametrize("nx,ny,pre,post", [(128, 128, 2, 2), (96, 160, 2, 2), (520, 96, 2, 2), (512, 512, 2, 2),
+                                            (128, 128, 1, 3), (256, 256, 3, 0)])
+def test_cluster_tail_matches_single_cta_tail(sgpu_mod, monkeypatch, nx, ny, pre, post):
     """The float V-cycle's levels of at most 65536 cells on one 16-CTA cluster (bands of rows with
     ghost rows in distributed shared memory; the levels of at most 1024 cells and the coarsest solve
     on one CTA) against the streamed levels and the single-CTA tail (SGPU_MG_CLUSTER=0): the same
@@ -156,7 +157,7 @@ def test_cluster_tail_matches_single_cta_tail(sgpu_mod, monkeypatch, nx, ny):
     base = snapshot_config("short_16")
     base.update(N_cells_x=str(nx), N_cells_y=str(ny), Re="1000", convection_scheme="QUICK",
                 diffusion_order="4", momentum_solver="gs_multicolour", pressure_solver="mg",
-                maxit="8", error_tolerance="0", precision="mixed")
+                maxit="8", error_tolerance="0", precision="mixed", mg_pre=str(pre), mg_post=str(post))
     out = {}
     for flag in ("0", "1"):
         monkeypatch.setenv("SGPU_MG_CLUSTER", flag)
@@ -173,7 +174,8 @@ def test_cluster_tail_matches_single_cta_tail(sgpu_mod, monkeypatch, nx, ny):
 
 @pytest.mark.parametrize("nx,ny,scheme,order,inner", [(128, 128, "QUICK", 4, 4), (96, 160, "QUICK", 2, 3),
                                                       (520, 96, "UDS", 2, 4), (33, 7, "QUICK", 4, 2),
-                                                      (256, 256, "QUICK", 4, 4)])
+                                                      (256, 256, "QUICK", 4, 4), (128, 128, "QUICK", 4, 1),
+                                                      (64, 64, "UDS", 2, 5)])
 def test_cluster_sweep_matches_streaming_sweep(sgpu_mod, monkeypatch, nx, ny, scheme, order, inner):
     """A small grid's correction sweeps on one 16-CTA cluster (bands of rows with two ghost rows in
     distributed shared memory, colour by colour, one launch per component) against the streaming
